@@ -1,0 +1,334 @@
+"""Benchmark: body-steps/s of the Barnes-Hut step on B200.
+
+Default workload: two colliding exponential discs, N = 4,194,304, theta = 0.5,
+FP64 state, softening 0.01, dt = 1e-4 (seeded synthetic input; no dataset).
+One "step" is the whole reference step: bounding box, Morton sort, tree,
+moments, force + kick, drift.  `value` is device-timed (CUDA events on the
+library's stream around K graph-launched steps) with the bodies resident in
+HBM; `e2e` times the same steps through the C ABI with host buffers: every
+step uploads the bodies from pinned host memory and downloads positions and
+velocities back, which is the reference's own per-step contract
+(BarnesHutCuda.cu:632-646) plus an upload.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--mode fp64|split] [--n N]
+
+--impl reference times the reference's CPU Barnes-Hut (compiled from the
+reference sources into oracle/_ref when available, else the CPU oracle's
+restatement of the GPU step) on the host cores, on a bounded sample.
+Under torchrun each rank runs an independent replica ("replicas only": the
+step does not shard); rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parent
+PKG = ROOT / "n-body-2d_b200"
+
+FLOPS_PER_INTERACTION = 14  # dx,dy,d2,+eps,r^-3 (3 mul),m*,2 fma: FP64/FP32 flops, rsqrt as 1
+FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+# Algorithmic HBM bytes per body for each memory-bound phase (FP64 state,
+# u64 codes, u32 payload): bbox 16 + Morton 16 in / 12 out; 8 radix passes of
+# 12 in + 12 out; gather 44 in + 44 out; drift 32 in + 16 out.
+PHASE_BYTES_PER_BODY = {"bbox+morton": 16 + 28, "sort": 8 * 24, "gather": 88, "drift": 48}
+
+
+def _package():
+    if "nbody_b200" in sys.modules:
+        return sys.modules["nbody_b200"]
+    spec = importlib.util.spec_from_file_location(
+        "nbody_b200", PKG / "__init__.py", submodule_search_locations=[str(PKG)])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["nbody_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def _peaks() -> tuple[dict, str]:
+    f = ROOT / "MEASURED_PEAKS.json"
+    if f.exists():
+        return json.loads(f.read_text()), "measured"
+    return dict(FALLBACK_PEAKS), "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.device)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+
+    def summary(self) -> dict:
+        sm, smax, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in getattr(self, "lines", []):
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def _dist():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def _workload(kind: str, n: int, seed: int = 0):
+    nb = _package()
+    return nb.universes.make(kind, n, seed)
+
+
+def cpu_baseline(n: int, theta: float, mass, pos, vel) -> dict:
+    """Bounded CPU sample: one full step of the whole workload on all host
+    cores, with the reference's CPU Barnes-Hut when it was built from the
+    reference sources, else with the CPU oracle's restatement of the GPU step."""
+    ref = ROOT / "oracle" / "_ref"
+    cores = os.cpu_count() or 1
+    if str(ROOT) not in sys.path:
+        sys.path.insert(0, str(ROOT))
+    runner = ref / "ref_cpu_bh"
+    if runner.exists():
+        from oracle import refcpu  # drives the reference CPU backend binary
+
+        t = refcpu.time_steps(mass, pos, vel, theta=theta, steps=1, threads=cores)
+        return {"value": n / t, "unit": "body-steps/s", "cores": cores, "kind": "reference",
+                "sample": f"1 step of the full N={n} workload, reference BarnesHut (CPU), "
+                          f"{cores} threads"}
+    import oracle
+
+    st = oracle.RefState(mass, pos, vel)
+    t0 = time.perf_counter()
+    st.step(theta=theta, eps2=1e-4, dt=1e-4, G=1.0, nthreads=cores)
+    t = time.perf_counter() - t0
+    return {"value": n / t, "unit": "body-steps/s", "cores": cores, "kind": "port",
+            "sample": f"1 step of the full N={n} workload, CPU restatement of the reference "
+                      f"GPU step, {cores} OpenMP threads"}
+
+
+def run_reference(args) -> None:
+    world, rank, _ = _dist()
+    if rank != 0:
+        return
+    m, p, v = _workload(args.kind, args.n)
+    steps_t = []
+    info = None
+    for k in range(args.warmup + args.steps):
+        info = cpu_baseline(args.n, args.theta, m, p, v)
+        if k >= args.warmup:
+            steps_t.append(args.n / info["value"])
+    t = sum(steps_t) / len(steps_t)
+    value = args.n / t
+    line = {
+        "impl": "reference", "metric": "body-steps/s", "value": value, "unit": "body-steps/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": _config(args),
+        "cpu_baseline": {"value": value, "unit": "body-steps/s", "cores": info["cores"],
+                         "kind": info["kind"], "sample": info["sample"]},
+        "e2e": {"value": value, "unit": "body-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def _config(args) -> dict:
+    return {"workload": args.workload, "n": args.n, "theta": args.theta, "mode": args.mode,
+            "softening": 0.01, "dt": 1e-4, "G": 1.0, "state": "f64",
+            "l2": "inputs larger than L2 (state + tree > 126 MB at this N)"}
+
+
+def run_ours(args) -> None:
+    world, rank, local = _dist()
+    nb = _package()
+    import torch
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    m, p, v = _workload(args.kind, args.n, seed=rank)
+    mode = nb.NB_MODE_SPLIT if args.mode == "split" else nb.NB_MODE_FP64
+    cfg = nb.SimConfig(timestep=1e-4, theta=args.theta, epsilon_squared=1e-4, G=1.0, mode=mode,
+                       device=local)
+    ctx = nb.NbContext(cfg, m, p, v)
+    ctx.step(args.warmup)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+            torch.cuda.synchronize()
+
+    barrier()
+    with ClockSampler(local) as clocks:
+        ctx.step(args.steps, sync=False)
+        ctx.sync()
+    barrier()
+    st = ctx.stats()
+    ms = st.ms_last_step
+    phases = ctx.phase_times()
+    if world > 1:
+        import torch.distributed as dist
+
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * args.n / (ms * 1e-3)
+
+    # e2e through the C ABI: host buffers, copies inside the timed region
+    pin = lambda shape: torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy()
+    hm, hp, hv = pin((args.n,)), pin((args.n, 2)), pin((args.n, 2))
+    hm[:], hp[:], hv[:] = m, p, v
+    op, ov = pin((args.n, 2)), pin((args.n, 2))
+    e2e_steps = max(1, min(args.steps, 5))
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        ctx.upload(hm, hp, hv)
+        ctx.step(1, sync=False)
+        ctx.download(op, ov)
+    e2e_t = (time.perf_counter() - t0) / e2e_steps
+    if world > 1:
+        t = torch.tensor([e2e_t], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_t = float(t.item())
+
+    peaks, peak_kind = _peaks()
+    clk = clocks.summary()
+    sm_mhz = clk["sm_mhz"] or peaks.get("sm_max_mhz", 1965.0)
+    interactions = st.cell_interactions + st.body_interactions
+    force_ms = phases.get("force", ms)
+    # FP64: 64 FMA lanes per SM per clock on B200 (37 TF at 1.965 GHz); FP32: 128.
+    lanes = 64 if args.mode == "fp64" else 128
+    fp_peak = 148 * lanes * 2 * sm_mhz * 1e6 / 1e12
+    achieved = FLOPS_PER_INTERACTION * interactions / (force_ms * 1e-3) / 1e12
+    hbm = peaks.get("hbm_gbs", FALLBACK_PEAKS["hbm_gbs"])
+    rooflines = {}
+    for name, bpb in PHASE_BYTES_PER_BODY.items():
+        if phases.get(name, 0) > 0:
+            gbs = bpb * args.n / (phases[name] * 1e-3) / 1e9
+            rooflines[name] = {"bound": "hbm", "achieved": round(gbs, 1), "peak": hbm,
+                               "unit": "GB/s", "frac": round(gbs / hbm, 4),
+                               "ms": round(phases[name], 4)}
+    line = {
+        "metric": "body-steps/s", "value": value, "unit": "body-steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.mode == "fp64" else "f32+f64", "data": "synthetic",
+        "config": _config(args),
+        "roofline": {"kernel": "force", "bound": "fp64" if args.mode == "fp64" else "fp32",
+                     "achieved": round(achieved, 3), "peak": round(fp_peak, 2),
+                     "unit": "TFLOP/s", "frac": round(achieved / fp_peak, 4), "traffic": None,
+                     "peak_source": f"nominal {lanes} FMA/clk/SM x 148 SMs at the sampled "
+                                    f"median SM clock {sm_mhz} MHz",
+                     "interactions_per_s": interactions / (force_ms * 1e-3),
+                     "interactions_per_body": interactions / args.n,
+                     "flops_per_interaction": FLOPS_PER_INTERACTION},
+        "rooflines_hbm": rooflines, "hbm_peak_source": f"{peak_kind} MEASURED_PEAKS.json hbm_gbs"
+        if peak_kind == "measured" else "fallback 6.65 TB/s",
+        "phases_ms": {k: round(v, 4) for k, v in phases.items()},
+        "e2e": {"value": world * args.n / e2e_t, "unit": "body-steps/s",
+                "h2d_bytes_per_step": 40 * args.n, "d2h_bytes_per_step": 32 * args.n,
+                "steps": e2e_steps},
+        "gpu_launches": int(st.kernels_per_step) * args.steps,
+        "clocks": clk,
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(args.n, args.theta, m, p, v)
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+WORKLOADS = {
+    "collision4m": ("collision", 4194304, 0.5),
+    "disc16k": ("disc", 16384, 0.5),
+    "plummer16m": ("plummer", 16777216, 0.5),
+}
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--mode", choices=["fp64", "split"], default="fp64")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="collision4m")
+    ap.add_argument("--n", type=int, default=None, help="override the body count")
+    ap.add_argument("--theta", type=float, default=None)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args(argv)
+    kind, n, theta = WORKLOADS[args.workload]
+    args.kind = kind
+    args.n = args.n or n
+    args.theta = theta if args.theta is None else args.theta
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

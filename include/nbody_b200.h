@@ -1,0 +1,165 @@
+/*
+ * nbody_b200.h -- C ABI of the B200 Barnes-Hut step.
+ *
+ * This is the drop-in boundary for the GPU backend of PhivPap/n-body-2d.  The
+ * reference backend is the C++ class BarnesHutCuda
+ * (src/Simulation/include/Simulation/BarnesHutCuda.hpp:44-112), created by
+ * create_sim() (src/main.cpp:26-38) behind the abstract Simulation interface
+ * (src/Simulation/include/Simulation/Simulation.hpp:13-67).  Its device work
+ * lives in private member functions with no C entry points; each function
+ * below replaces one of them and is cited with the member it stands in for.
+ *
+ * Plain pointers and sizes only.  Host arrays use the reference's Bodies
+ * layout (src/common_lib/Body/include/Body/Body.hpp:26-31): mass is double[n],
+ * positions and velocities are interleaved {x, y} doubles (double[2n]), all in
+ * the caller's original body order.
+ *
+ * Threading: one context per host thread at a time; the library keeps no
+ * global mutable state.  Every call returns an NB_* status; on failure
+ * nb_last_error() describes the cause (the reference calls exit(1) instead,
+ * src/Simulation/src/BarnesHutCuda.cu:12-19).
+ */
+#ifndef NBODY_B200_H
+#define NBODY_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define NB_API __attribute__((visibility("default")))
+#else
+#define NB_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define NB_OK 0
+#define NB_ERR_INVALID 1   /* bad argument, NaN/Inf input, n out of range      */
+#define NB_ERR_CUDA 2      /* a CUDA runtime call failed                       */
+#define NB_ERR_CAPACITY 3  /* a device-side capacity bound was hit             */
+#define NB_ERR_TIMEOUT 4   /* a bounded device-side wait gave up               */
+#define NB_ERR_NOMEM 5     /* device or host allocation failed                 */
+#define NB_ERR_NOTFOUND 6  /* no CUDA device / bad device ordinal              */
+
+/* ---- traversal modes --------------------------------------------------- */
+/* NB_MODE_FP64: the reference's semantics (per-body DFS, per-body opening
+ * test, leaf size 1, FP64 throughout), for parity with
+ * src/Simulation/src/BarnesHutCuda.cu:382-486.
+ * NB_MODE_SPLIT: warp-cooperative group traversal with FP32 cell moments and
+ * interactions; FP64 kept for the bounding box, the tree's centre-of-mass sums
+ * and the integrator's position/velocity accumulation. */
+#define NB_MODE_FP64 0
+#define NB_MODE_SPLIT 1
+
+typedef struct nb_params {
+    double G;               /* gravitational constant (Constants::Simulation::G)    */
+    double timestep;        /* dt (Config::Simulation::timestep)                    */
+    double theta;           /* opening angle (Config::Simulation::theta)            */
+    double epsilon_squared; /* Plummer softening squared (Simulation::epsilon_squared) */
+    int32_t mode;           /* NB_MODE_*                                            */
+    int32_t leaf_size;      /* SPLIT: bodies a cell may hold and still be summed
+                               body by body instead of opened (0 = default)         */
+    int32_t device;         /* CUDA device ordinal                                  */
+    int32_t flags;          /* reserved, must be 0                                  */
+} nb_params;
+
+typedef struct nb_stats {
+    uint64_t steps;              /* steps taken since nb_create                       */
+    uint64_t n;                  /* bodies                                            */
+    uint64_t tree_nodes;         /* internal cells of the last tree built             */
+    uint64_t cell_interactions;  /* body-cell terms of the last force pass            */
+    uint64_t body_interactions;  /* body-body terms of the last force pass            */
+    double ms_last_step;         /* device ms per step of the last synced nb_step batch */
+    double root_width;           /* width of the squared root box of the last step    */
+    uint64_t kernels_per_step;   /* kernel launches one step makes                    */
+} nb_stats;
+
+typedef struct nb_ctx nb_ctx;
+
+/* Fills *p with G=1, dt=1e-4, theta=0.5, epsilon_squared=1e-4, FP64 mode. */
+NB_API int nb_params_default(nb_params* p);
+
+/* Replaces BarnesHutCuda::BarnesHutCuda + init_device_resources
+ * (src/Simulation/src/BarnesHutCuda.cpp:7-11, BarnesHutCuda.cu:550-606):
+ * allocates every device buffer once and uploads the bodies. */
+NB_API int nb_create(const nb_params* p, uint64_t n, const double* mass, const double* pos_xy,
+              const double* vel_xy, nb_ctx** out);
+
+/* Replaces ~BarnesHutCuda + release_device_resources (BarnesHutCuda.cpp:13-18,
+ * BarnesHutCuda.cu:608-630). Accepts NULL. */
+NB_API int nb_destroy(nb_ctx* ctx);
+
+/* Replaces nsteps iterations of the body of BarnesHutCuda::simulate
+ * (src/Simulation/src/BarnesHutCuda.cpp:30-40) minus the per-step download:
+ * bounding box, Morton sort, tree, force + kick, drift.  Enqueued on the
+ * context's stream as captured CUDA graphs; returns once enqueued. */
+NB_API int nb_step(nb_ctx* ctx, uint32_t nsteps);
+
+/* Waits for enqueued work and reports any device-side error flag. */
+NB_API int nb_sync(nb_ctx* ctx);
+
+/* Replaces the timestep hot-swap of Simulation::post_iteration
+ * (src/Simulation/src/Simulation.cpp:68-72); takes effect at the next step. */
+NB_API int nb_set_timestep(nb_ctx* ctx, double dt);
+
+/* Overwrites the device state with host bodies in original order (the upload
+ * half of init_device_resources, BarnesHutCuda.cu:596-605). */
+NB_API int nb_upload(nb_ctx* ctx, const double* mass, const double* pos_xy, const double* vel_xy);
+
+/* Replaces sync_from_gpu_bodies (BarnesHutCuda.cu:632-646): scatters the
+ * state back to original order and copies it to the host.  Either pointer
+ * may be NULL.  Blocks until the copy is done. */
+NB_API int nb_download(nb_ctx* ctx, double* pos_xy, double* vel_xy);
+
+/* Accelerations (without G) of the current state, original order, as the
+ * force pass would apply them (BarnesHutCuda.cu:382-486); no integration.
+ * Re-sorts the device state, which does not change the bodies. */
+NB_API int nb_accelerations(nb_ctx* ctx, double* acc_xy);
+
+/* Debug view of the sort stage (BarnesHutCuda.cu:648-711) on the current
+ * state without changing it: sorted 64-bit Morton codes and the permutation
+ * (order[r] = device slot of the body ranked r); box_out (nullable) receives
+ * the squared root box {x_min, x_max, y_min, y_max}. */
+NB_API int nb_debug_morton(nb_ctx* ctx, uint64_t* codes, int32_t* order, double* box_out);
+
+/* Debug view of the raw device state in device (sorted) order. Any pointer
+ * may be NULL. orig[i] is the original index of device slot i. */
+NB_API int nb_debug_state(nb_ctx* ctx, double* mass, double* pos_xy, double* vel_xy, int32_t* orig);
+
+/* Debug view of the last tree: per-cell mass and centre of mass (FP64),
+ * level, body range, and the root reference.  Arrays sized by
+ * nb_stats.tree_nodes; any pointer may be NULL. root_ref >= 0 is a cell,
+ * < 0 is the leaf starting at body ~root_ref. */
+NB_API int nb_debug_tree(nb_ctx* ctx, double* cell_mass, double* cell_com_xy, int32_t* level,
+                  int32_t* first_body, int32_t* last_body, int32_t* root_ref);
+
+NB_API int nb_get_stats(nb_ctx* ctx, nb_stats* out);
+
+/* Device time of each phase of the most recent graph-launched step, from CUDA
+ * events recorded inside the step graph (the GPU counterpart of the phase
+ * StopWatches of the reference CPU backend, src/Simulation/src/BarnesHut.cpp:
+ * 22-25, 52-64).  Writes up to max values to ms and returns the number of
+ * phases (>= 0) or a negative NB_* status.  Phase k is named by
+ * nb_phase_name(k). */
+NB_API int nb_phase_times(nb_ctx* ctx, double* ms, int max);
+NB_API const char* nb_phase_name(int phase);
+
+/* Last error text of this context (never NULL). */
+NB_API const char* nb_last_error(const nb_ctx* ctx);
+NB_API const char* nb_status_string(int status);
+
+/* FP64 all-pairs accelerations on the GPU with the reference pair law
+ * (BarnesHutCuda.cu:427-431): a_i = sum_{j != i} m_j d_ij (|d_ij|^2+eps2)^-1.5
+ * for k targets (indices into the n sources).  Host arrays in, host array out.
+ * This is the error oracle for p50/p99 force errors at full size. */
+NB_API int nb_allpairs_accelerations(int32_t device, uint64_t n, const double* mass,
+                              const double* pos_xy, uint64_t k, const int64_t* targets,
+                              double epsilon_squared, double* acc_xy);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,348 @@
+// k_sort.cu -- bounding box, Morton codes, LSD radix sort and the sorted gather.
+//
+// Stage 1-2 of the step (reference: BarnesHutCuda.cu:648-711).  The box is
+// reduced in one launch (last-block-done) and squared on the device, so the
+// step never returns to the host; Morton codes are bit-exact with CU:54-69;
+// the sort is a project-written stable LSD radix sort over all 64 key bits,
+// so its order equals cub::DeviceRadixSort::SortPairs at CU:692 (any stable
+// sort of (code, current index) gives the same permutation).
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "nb_internal.cuh"
+
+namespace nb {
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kBoxThreads = 512;
+
+__device__ __forceinline__ double warp_min(double v) {
+    for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(kFull, v, o));
+    return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(kFull, v, o));
+    return v;
+}
+
+// Exact FP64 min/max of all positions, reduced per block, then folded and
+// squared by the last block to finish (CU:78-114 + the host squaring at
+// CU:665-677, done here on the device in the same FP64 operations).
+__global__ void __launch_bounds__(kBoxThreads)
+bbox_kernel(const double2* __restrict__ pos, int64_t n, double* __restrict__ partials,
+            DeviceScalars* __restrict__ s) {
+    double xmin = INFINITY, xmax = -INFINITY, ymin = INFINITY, ymax = -INFINITY;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const double2 p = __ldg(pos + i);
+        xmin = fmin(xmin, p.x);
+        xmax = fmax(xmax, p.x);
+        ymin = fmin(ymin, p.y);
+        ymax = fmax(ymax, p.y);
+    }
+    xmin = warp_min(xmin);
+    xmax = warp_max(xmax);
+    ymin = warp_min(ymin);
+    ymax = warp_max(ymax);
+    __shared__ double red[4][kBoxThreads / 32];
+    __shared__ bool last_block;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
+        red[0][warp] = xmin;
+        red[1][warp] = xmax;
+        red[2][warp] = ymin;
+        red[3][warp] = ymax;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < kBoxThreads / 32; ++w) {
+            xmin = fmin(xmin, red[0][w]);
+            xmax = fmax(xmax, red[1][w]);
+            ymin = fmin(ymin, red[2][w]);
+            ymax = fmax(ymax, red[3][w]);
+        }
+        double* out = partials + 4 * blockIdx.x;
+        out[0] = xmin;
+        out[1] = xmax;
+        out[2] = ymin;
+        out[3] = ymax;
+        __threadfence();
+        last_block = atomicAdd(&s->bbox_ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last_block) return;
+    if (threadIdx.x == 0) {
+        __threadfence();
+        // CU:649-654 seeds with +-DBL_MAX; folding from there is identical.
+        double bx0 = 1.7976931348623157e308, bx1 = -1.7976931348623157e308;
+        double by0 = 1.7976931348623157e308, by1 = -1.7976931348623157e308;
+        for (unsigned b = 0; b < gridDim.x; ++b) {
+            const double* in = partials + 4 * b;
+            bx0 = fmin(bx0, __ldcg(in + 0));
+            bx1 = fmax(bx1, __ldcg(in + 1));
+            by0 = fmin(by0, __ldcg(in + 2));
+            by1 = fmax(by1, __ldcg(in + 3));
+        }
+        const double x_range = bx1 - bx0;
+        const double y_range = by1 - by0;
+        if (x_range > y_range) {
+            const double mid = (by0 + by1) * 0.5;
+            by0 = mid - x_range * 0.5;
+            by1 = mid + x_range * 0.5;
+        } else {
+            const double mid = (bx0 + bx1) * 0.5;
+            bx0 = mid - y_range * 0.5;
+            bx1 = mid + y_range * 0.5;
+        }
+        s->box[0] = bx0;
+        s->box[1] = bx1;
+        s->box[2] = by0;
+        s->box[3] = by1;
+        // CU:717 root width_sq, then CU:216 child_wsq = parent * 0.25 per level.
+        const double w = bx1 - bx0;
+        double wsq = w * w;
+        for (int l = 0; l <= kMaxLevel; ++l) {
+            s->wsq[l] = wsq;
+            wsq *= 0.25;
+        }
+        s->bbox_ticket = 0;
+    }
+}
+
+__device__ __forceinline__ uint64_t expand_bits_2d(uint32_t v) {
+    uint64_t x = v;
+    x = (x | (x << 16)) & 0x0000FFFF0000FFFFull;
+    x = (x | (x << 8)) & 0x00FF00FF00FF00FFull;
+    x = (x | (x << 4)) & 0x0F0F0F0F0F0F0F0Full;
+    x = (x | (x << 2)) & 0x3333333333333333ull;
+    x = (x | (x << 1)) & 0x5555555555555555ull;
+    return x;
+}
+
+// CU:117-132: code from (p - min) * (1 / width), quantised to 32 bits per axis
+// with round-down; x bits land on odd positions.  val = current slot.
+__global__ void morton_kernel(const double2* __restrict__ pos, int64_t n,
+                              const DeviceScalars* __restrict__ s, uint64_t* __restrict__ key,
+                              uint32_t* __restrict__ val) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double x0 = s->box[0], x1 = s->box[1], y0 = s->box[2], y1 = s->box[3];
+    const double inv_w = 1.0 / (x1 - x0);
+    const double inv_h = 1.0 / (y1 - y0);
+    const double2 p = __ldg(pos + i);
+    const double nx = (p.x - x0) * inv_w;
+    const double ny = (p.y - y0) * inv_h;
+    const uint32_t ix = __double2uint_rd(fmin(fmax(nx * 4294967296.0, 0.0), 4294967295.0));
+    const uint32_t iy = __double2uint_rd(fmin(fmax(ny * 4294967296.0, 0.0), 4294967295.0));
+    key[i] = (expand_bits_2d(ix) << 1) | expand_bits_2d(iy);
+    val[i] = (uint32_t)i;
+}
+
+// ---------------------------------------------------------------------------
+// LSD radix sort, 8-bit digits, 8 passes.  Each pass: per-tile digit counts
+// (upsweep), a per-digit scan over tiles, and a stable scatter (downsweep)
+// that ranks keys inside the tile with warp-private histograms and
+// __match_any_sync, stages the tile in shared memory sorted by digit, and
+// writes each digit's run with consecutive threads (coalesced).
+// ---------------------------------------------------------------------------
+constexpr int kWarps = kSortThreads / 32;
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// Exclusive scan of one value per thread over a 256-thread block.
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* warp_tot,
+                                                         uint32_t* total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t inc = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(kFull, inc, o);
+        if (lane >= o) inc += t;
+    }
+    if (lane == 31) warp_tot[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = lane < kWarps ? warp_tot[lane] : 0;
+        uint32_t winc = w;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(kFull, winc, o);
+            if (lane >= o) winc += t;
+        }
+        if (lane < kWarps) warp_tot[lane] = winc - w;
+        if (lane == kWarps - 1 && total) *total = winc;
+    }
+    __syncthreads();
+    const uint32_t r = warp_tot[warp] + inc - v;
+    __syncthreads();
+    return r;
+}
+
+__global__ void __launch_bounds__(kSortThreads)
+sort_upsweep(const uint64_t* __restrict__ key, int64_t n, int shift, uint32_t* __restrict__ counts,
+             int tiles) {
+    __shared__ uint32_t hist[256];
+    hist[threadIdx.x] = 0;
+    __syncthreads();
+    const int64_t base = (int64_t)blockIdx.x * kSortTile;
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int k = 0; k < kSortTileItems; ++k) {
+        const int64_t i = base + k * kSortThreads + threadIdx.x;
+        const bool valid = i < n;
+        const uint32_t d = valid ? (uint32_t)((__ldg(key + i) >> shift) & 0xFF) : 0x100u + lane;
+        const unsigned peers = __match_any_sync(kFull, d);
+        if (valid && lane == __ffs(peers) - 1) atomicAdd(&hist[d], (uint32_t)__popc(peers));
+    }
+    __syncthreads();
+    counts[(int64_t)threadIdx.x * tiles + blockIdx.x] = hist[threadIdx.x];
+}
+
+// Block d turns row d of counts into exclusive offsets and writes its total.
+__global__ void __launch_bounds__(kSortThreads)
+sort_scan_rows(uint32_t* __restrict__ counts, int tiles, uint32_t* __restrict__ totals) {
+    __shared__ uint32_t warp_tot[kWarps];
+    __shared__ uint32_t chunk_total;
+    uint32_t* row = counts + (int64_t)blockIdx.x * tiles;
+    uint32_t carry = 0;
+    for (int b = 0; b < tiles; b += kSortThreads) {
+        const int t = b + threadIdx.x;
+        const uint32_t v = t < tiles ? row[t] : 0;
+        const uint32_t ex = block_exclusive_scan(v, warp_tot, &chunk_total);
+        if (t < tiles) row[t] = carry + ex;
+        carry += chunk_total;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) totals[blockIdx.x] = carry;
+}
+
+__global__ void __launch_bounds__(kSortThreads)
+sort_downsweep(const uint64_t* __restrict__ key_in, const uint32_t* __restrict__ val_in,
+               uint64_t* __restrict__ key_out, uint32_t* __restrict__ val_out, int64_t n, int shift,
+               const uint32_t* __restrict__ counts, const uint32_t* __restrict__ totals, int tiles) {
+    __shared__ uint32_t whist[kWarps][256];
+    __shared__ uint32_t tile_start[256];
+    __shared__ uint32_t goff[256];
+    __shared__ uint32_t warp_tot[kWarps];
+    __shared__ uint64_t skey[kSortTile];
+    __shared__ uint32_t sval[kSortTile];
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) whist[w][tid] = 0;
+    {
+        const uint32_t tot = totals[tid];
+        const uint32_t pre = block_exclusive_scan(tot, warp_tot, nullptr);
+        goff[tid] = pre + counts[(int64_t)tid * tiles + blockIdx.x];
+    }
+    __syncthreads();
+
+    const int64_t base = (int64_t)blockIdx.x * kSortTile;
+    const int64_t seg = base + warp * (32 * kSortTileItems);
+    uint64_t k_reg[kSortTileItems];
+    uint32_t v_reg[kSortTileItems];
+    uint32_t r_reg[kSortTileItems];
+    const unsigned below = lanemask_lt();
+#pragma unroll
+    for (int k = 0; k < kSortTileItems; ++k) {
+        const int64_t i = seg + k * 32 + lane;
+        const bool valid = i < n;
+        k_reg[k] = valid ? key_in[i] : 0ull;
+        v_reg[k] = valid ? val_in[i] : 0u;
+        const uint32_t d = valid ? (uint32_t)((k_reg[k] >> shift) & 0xFF) : 0x100u + lane;
+        const unsigned peers = __match_any_sync(kFull, d);
+        const int leader = __ffs(peers) - 1;
+        uint32_t b = 0;
+        if (valid && lane == leader) {
+            b = whist[warp][d];
+            whist[warp][d] = b + __popc(peers);
+        }
+        b = __shfl_sync(kFull, b, leader);
+        r_reg[k] = b + __popc(peers & below);
+        __syncwarp();
+    }
+    __syncthreads();
+    {
+        uint32_t run = 0;
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) {
+            const uint32_t c = whist[w][tid];
+            whist[w][tid] = run;
+            run += c;
+        }
+        tile_start[tid] = block_exclusive_scan(run, warp_tot, nullptr);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < kSortTileItems; ++k) {
+        const int64_t i = seg + k * 32 + lane;
+        if (i < n) {
+            const uint32_t d = (uint32_t)((k_reg[k] >> shift) & 0xFF);
+            const uint32_t lp = tile_start[d] + whist[warp][d] + r_reg[k];
+            skey[lp] = k_reg[k];
+            sval[lp] = v_reg[k];
+        }
+    }
+    __syncthreads();
+    const int tile_n = (int)min((int64_t)kSortTile, n - base);
+    for (int p = tid; p < tile_n; p += kSortThreads) {
+        const uint64_t kk = skey[p];
+        const uint32_t d = (uint32_t)((kk >> shift) & 0xFF);
+        const uint32_t gp = goff[d] + (uint32_t)p - tile_start[d];
+        key_out[gp] = kk;
+        val_out[gp] = sval[p];
+    }
+}
+
+__global__ void gather_kernel(const uint32_t* __restrict__ order, int64_t n, BodyBuffers src,
+                              BodyBuffers dst) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t j = __ldg(order + i);
+    dst.pos[i] = __ldg(src.pos + j);
+    dst.vel[i] = __ldg(src.vel + j);
+    dst.mass[i] = __ldg(src.mass + j);
+    dst.orig[i] = __ldg(src.orig + j);
+}
+
+inline unsigned blocks_for(int64_t n, int threads) {
+    return (unsigned)((n + threads - 1) / threads);
+}
+
+}  // namespace
+
+void launch_bbox(nb_ctx* c, const double2* pos) {
+    c->launches += 1;
+    bbox_kernel<<<c->bbox_blocks, kBoxThreads, 0, c->stream>>>(pos, c->n, c->bbox_partials, c->scal);
+}
+
+void launch_morton(nb_ctx* c, const double2* pos) {
+    c->launches += 1;
+    morton_kernel<<<blocks_for(c->n, 256), 256, 0, c->stream>>>(pos, c->n, c->scal, c->sort.key[0],
+                                                               c->sort.val[0]);
+}
+
+void launch_sort(nb_ctx* c) {
+    const int tiles = c->sort.tiles;
+    c->launches += 3 * 8;
+    for (int pass = 0; pass < 8; ++pass) {
+        const int src = pass & 1, dst = src ^ 1;
+        const int shift = 8 * pass;
+        sort_upsweep<<<tiles, kSortThreads, 0, c->stream>>>(c->sort.key[src], c->n, shift,
+                                                             c->sort.counts, tiles);
+        sort_scan_rows<<<256, kSortThreads, 0, c->stream>>>(c->sort.counts, tiles, c->sort.totals);
+        sort_downsweep<<<tiles, kSortThreads, 0, c->stream>>>(
+            c->sort.key[src], c->sort.val[src], c->sort.key[dst], c->sort.val[dst], c->n, shift,
+            c->sort.counts, c->sort.totals, tiles);
+    }
+}
+
+void launch_gather(nb_ctx* c, const BodyBuffers& src, const BodyBuffers& dst) {
+    c->launches += 1;
+    gather_kernel<<<blocks_for(c->n, 256), 256, 0, c->stream>>>(c->sort.val[0], c->n, src, dst);
+}
+
+}  // namespace nb

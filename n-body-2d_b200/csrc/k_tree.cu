@@ -1,0 +1,376 @@
+// k_tree.cu -- compressed quadtree from sorted Morton codes, and its moments.
+//
+// Replaces the reference's level-by-level build (BarnesHutCuda.cu:153-240 and
+// the host loop at CU:713-777, up to 31 launches each followed by a
+// device-to-host copy) and its per-level COM passes (CU:251-344, CU:787-807).
+//
+// Construction (Karras-style, no host round trips):
+//   For the boundary i between sorted bodies i and i+1 let d_i be the number
+//   of leading 2-bit digits their codes share.  Every boundary with d_i < 30
+//   separates two children of the cell "bodies sharing d_i digits with body
+//   i", whose level is d_i.  That cell is created once, by its first child
+//   boundary (the one whose left neighbour run starts the cell), found with
+//   an O(1) test after one galloping search.  Cells are numbered by an
+//   exclusive scan over those boundaries, which lays every subtree out as a
+//   contiguous id range.  A third pass links children (<= 4 per cell) and
+//   parents.
+//
+// The reference tree is uncompressed: a cell with one non-empty child is
+// followed by a chain of single-child cells down to the next split, all with
+// the same mass and centre of mass.  The reference accepts a chain at its
+// first level that passes width^2 < theta^2 d^2, and because widths shrink
+// with depth that happens iff the deepest level of the chain passes.  This
+// tree therefore keeps only the deepest level of every chain and stores that
+// level, so opening decisions and force terms equal the reference's
+// (cell widths come from the level, never from the body range).
+#include <climits>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "nb_internal.cuh"
+
+namespace nb {
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kThreads * kScanItems;
+constexpr unsigned kFull = 0xffffffffu;
+
+__device__ __forceinline__ int lcp_digits(uint64_t a, uint64_t b) {
+    const uint64_t x = a ^ b;
+    return x ? (__clzll((long long)x) >> 1) : 32;
+}
+
+__device__ __forceinline__ bool share(uint64_t a, uint64_t b, int digits) {
+    return digits <= 0 ? true : (digits >= 32 ? a == b : ((a ^ b) >> (64 - 2 * digits)) == 0);
+}
+
+// First index s in [lo, i] whose code shares `digits` leading digits with
+// key[i] (the run of such codes is contiguous and contains i).
+__device__ int gallop_left(const uint64_t* __restrict__ key, int lo, int i, int digits) {
+    const uint64_t ki = key[i];
+    int j = i, step = 1;
+    while (true) {
+        const int cand = i - step;
+        if (cand < lo || !share(key[cand], ki, digits)) break;
+        j = cand;
+        step <<= 1;
+    }
+    int a = max(lo, i - step + 1), b = j;
+    while (a < b) {
+        const int mid = (a + b) >> 1;
+        if (share(key[mid], ki, digits)) b = mid; else a = mid + 1;
+    }
+    return a;
+}
+
+// Last index e in [i, hi] whose code shares `digits` leading digits with key[i].
+__device__ int gallop_right(const uint64_t* __restrict__ key, int i, int hi, int digits) {
+    const uint64_t ki = key[i];
+    int j = i, step = 1;
+    while (true) {
+        const int cand = i + step;
+        if (cand > hi || !share(key[cand], ki, digits)) break;
+        j = cand;
+        step <<= 1;
+    }
+    int a = j, b = min(hi, i + step - 1);
+    while (a < b) {
+        const int mid = (a + b + 1) >> 1;
+        if (share(key[mid], ki, digits)) a = mid; else b = mid - 1;
+    }
+    return a;
+}
+
+// Pass 1: flag the boundaries that create a cell.
+__global__ void tree_mark(const uint64_t* __restrict__ key, int n, int32_t* __restrict__ flag,
+                          int32_t* __restrict__ start_of) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int f = 0, s = 0;
+    if (i < n - 1) {
+        const uint64_t ki = key[i];
+        const int c = lcp_digits(ki, key[i + 1]);
+        if (c < kMaxLevel) {
+            s = c == 0 ? 0 : gallop_left(key, 0, i, c);
+            // i opens the cell iff bodies s..i all sit in its first child.
+            f = share(key[s], ki, c + 1) ? 1 : 0;
+        }
+    }
+    flag[i] = f;
+    start_of[i] = s;
+}
+
+// ---- exclusive scan of flag[] -> cell_of[], total -> scal->cells ----------
+__device__ __forceinline__ int warp_inclusive(int v) {
+    const int lane = threadIdx.x & 31;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(kFull, v, o);
+        if (lane >= o) v += t;
+    }
+    return v;
+}
+
+__device__ int block_exclusive(int v, int* wsum, int* total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int inc = warp_inclusive(v);
+    if (lane == 31) wsum[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        const int w = lane < kThreads / 32 ? wsum[lane] : 0;
+        const int winc = warp_inclusive(w);
+        if (lane < kThreads / 32) wsum[lane] = winc - w;
+        if (lane == kThreads / 32 - 1 && total) *total = winc;
+    }
+    __syncthreads();
+    const int r = wsum[warp] + inc - v;
+    __syncthreads();
+    return r;
+}
+
+__global__ void __launch_bounds__(kThreads)
+scan_reduce(const int32_t* __restrict__ in, int n, int32_t* __restrict__ block_sums) {
+    __shared__ int wsum[kThreads / 32];
+    __shared__ int total;
+    const int base = blockIdx.x * kScanTile;
+    int v = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        const int i = base + k * kThreads + threadIdx.x;
+        if (i < n) v += in[i];
+    }
+    block_exclusive(v, wsum, &total);
+    if (threadIdx.x == 0) block_sums[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(kThreads)
+scan_block_sums(int32_t* __restrict__ block_sums, int blocks, DeviceScalars* __restrict__ s) {
+    __shared__ int wsum[kThreads / 32];
+    __shared__ int total;
+    int carry = 0;
+    for (int b = 0; b < blocks; b += kThreads) {
+        const int t = b + threadIdx.x;
+        const int v = t < blocks ? block_sums[t] : 0;
+        const int ex = block_exclusive(v, wsum, &total);
+        if (t < blocks) block_sums[t] = carry + ex;
+        carry += total;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) s->cells = carry;
+}
+
+__global__ void __launch_bounds__(kThreads)
+scan_apply(const int32_t* __restrict__ in, int n, const int32_t* __restrict__ block_sums,
+           int32_t* __restrict__ out) {
+    __shared__ int wsum[kThreads / 32];
+    __shared__ int total;
+    // Items of a thread are consecutive so one block scan covers the tile.
+    const int base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+    int v[kScanItems];
+    int sum = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        v[k] = base + k < n ? in[base + k] : 0;
+        sum += v[k];
+    }
+    int run = block_exclusive(sum, wsum, &total) + block_sums[blockIdx.x];
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        if (base + k < n) out[base + k] = run;
+        run += v[k];
+    }
+}
+
+// Moments of a multi-body leaf in the reference's summation order: 128
+// strided partial sums, then a halving tree (CU:284-309).  The halving tree
+// adds the partials as a balanced binary tree whose leaves, left to right, are
+// the partials in 7-bit bit-reversed order, so a binary-counter pairwise sum
+// over that sequence reproduces it with an 8-entry stack.  Such leaves only
+// hold bodies whose codes agree in 60 bits, so they are rare and small.
+__device__ void bucket_moments(const double2* __restrict__ pos, const double* __restrict__ mass,
+                               int first, int last, double* out_m, double2* out_c) {
+    double sm[8], sx[8], sy[8];
+    for (int k = 0; k < 128; ++k) {
+        const int tx = (int)(__brev((unsigned)k) >> 25);
+        double M = 0.0, Rx = 0.0, Ry = 0.0;
+        for (int i = first + tx; i <= last; i += 128) {
+            const double m = mass[i];
+            M += m;
+            Rx = fma(m, pos[i].x, Rx);
+            Ry = fma(m, pos[i].y, Ry);
+        }
+        int lvl = 0;
+        while ((k >> lvl) & 1) {
+            M = sm[lvl] + M;
+            Rx = sx[lvl] + Rx;
+            Ry = sy[lvl] + Ry;
+            ++lvl;
+        }
+        sm[lvl] = M;
+        sx[lvl] = Rx;
+        sy[lvl] = Ry;
+    }
+    *out_m = sm[7];
+    *out_c = make_double2(sx[7] / sm[7], sy[7] / sm[7]);
+}
+
+// Pass 3: every flagged boundary writes its cell, its children and their
+// parent links.
+__global__ void tree_link(const uint64_t* __restrict__ key, int n,
+                          const double2* __restrict__ pos, const double* __restrict__ mass,
+                          Tree t, DeviceScalars* __restrict__ s) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n - 1 || !t.flag[i]) return;
+    const int id = t.cell_of[i];
+    const int c = lcp_digits(key[i], key[i + 1]);
+    const int first = t.start_of[i];
+    const int last = c == 0 ? n - 1 : gallop_right(key, i + 1, n - 1, c);
+    int cs[4], ce[4];
+    int nc = 1;
+    cs[0] = first;
+    ce[0] = i;
+    int p = i + 1;
+    while (p <= last && nc < 4) {
+        const int e = gallop_right(key, p, last, c + 1);
+        cs[nc] = p;
+        ce[nc] = e;
+        ++nc;
+        p = e + 1;
+    }
+    if (p <= last) atomicOr(&s->error, kErrTree);
+    int ref[4] = {INT_MIN, INT_MIN, INT_MIN, INT_MIN};
+    int nint = 0;
+    for (int q = 0; q < nc; ++q) {
+        const int a = cs[q], b = ce[q];
+        if (a == b) {
+            ref[q] = ~a;
+            t.leaf_last[a] = a;
+            t.leaf_plevel[a] = c;
+            continue;
+        }
+        const int c2 = lcp_digits(key[a], key[b]);
+        if (c2 >= kMaxLevel) {
+            ref[q] = ~a;
+            t.leaf_last[a] = b;
+            t.leaf_plevel[a] = c;
+            bucket_moments(pos, mass, a, b, t.bucket_mass + a, t.bucket_com + a);
+            continue;
+        }
+        const int rep = gallop_right(key, a, b, c2 + 1);
+        const int cid = t.cell_of[rep];
+        ref[q] = cid;
+        t.parent[cid] = id;
+        ++nint;
+    }
+    t.first[id] = first;
+    t.last[id] = last;
+    t.level[id] = c;
+    t.child[id] = make_int4(ref[0], ref[1], ref[2], ref[3]);
+    t.nint[id] = nint;
+    t.ready[id] = 0;
+    if (first == 0 && last == n - 1) {
+        s->root = id;
+        t.parent[id] = -1;
+    }
+}
+
+// A tree without internal cells: one body, or all bodies in one level-30 leaf.
+__global__ void tree_trivial_root(const double2* __restrict__ pos, const double* __restrict__ mass,
+                                  int n, Tree t, DeviceScalars* __restrict__ s) {
+    if (s->cells != 0) return;
+    s->root = ~0;
+    t.leaf_last[0] = n - 1;
+    t.leaf_plevel[0] = -1;
+    if (n > 1) bucket_moments(pos, mass, 0, n - 1, t.bucket_mass, t.bucket_com);
+}
+
+// Bottom-up FP64 moments.  Threads start at cells without internal children
+// and climb; the last child to arrive at a parent (atomic counter) computes
+// it.  Sums run over the children in quadrant order with the reference's
+// arithmetic (CU:329-343): M += m; R = fma(m, com, R); com = R / M.
+__global__ void tree_moments(DeviceScalars* __restrict__ s, const double2* __restrict__ pos,
+                             const double* __restrict__ mass, Tree t) {
+    int id = blockIdx.x * blockDim.x + threadIdx.x;
+    const int cells = s->cells;
+    if (id >= cells || t.nint[id] != 0) return;
+    // A path to the root crosses at most 30 cells; the bound only guards
+    // against a malformed tree.
+    for (int hop = 0;; ++hop) {
+        if (hop > kMaxLevel + 1) {
+            atomicOr(&s->error, kErrTree);
+            return;
+        }
+        const int4 ch = t.child[id];
+        const int refs[4] = {ch.x, ch.y, ch.z, ch.w};
+        double M = 0.0, Rx = 0.0, Ry = 0.0;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int r = refs[q];
+            if (r == INT_MIN) break;
+            double cm;
+            double2 cc;
+            if (r >= 0) {
+                cm = __ldcg(t.mass + r);
+                cc = __ldcg(t.com + r);
+            } else {
+                const int b = ~r;
+                if (t.leaf_last[b] == b) {
+                    cm = mass[b];
+                    cc = pos[b];
+                } else {
+                    cm = t.bucket_mass[b];
+                    cc = t.bucket_com[b];
+                }
+            }
+            M += cm;
+            Rx = fma(cm, cc.x, Rx);
+            Ry = fma(cm, cc.y, Ry);
+        }
+        __stcg(t.mass + id, M);
+        __stcg(t.com + id, make_double2(Rx / M, Ry / M));
+        __threadfence();
+        const int par = t.parent[id];
+        if (par < 0) return;
+        if (par >= cells) {
+            atomicOr(&s->error, kErrTree);
+            return;
+        }
+        const int arrived = atomicAdd(t.ready + par, 1);
+        if (arrived != t.nint[par] - 1) return;
+        __threadfence();
+        id = par;
+    }
+}
+
+inline unsigned blocks_for(int64_t n, int threads) {
+    return (unsigned)((n + threads - 1) / threads);
+}
+
+}  // namespace
+
+void launch_tree(nb_ctx* c, const BodyBuffers& b) {
+    const int n = (int)c->n;
+    const uint64_t* key = c->sort.key[0];
+    c->launches += 6;
+    tree_mark<<<blocks_for(n, kThreads), kThreads, 0, c->stream>>>(key, n, c->tree.flag,
+                                                                    c->tree.start_of);
+    const int sblocks = (int)blocks_for(n, kScanTile);
+    scan_reduce<<<sblocks, kThreads, 0, c->stream>>>(c->tree.flag, n, c->scan.block_sums);
+    scan_block_sums<<<1, kThreads, 0, c->stream>>>(c->scan.block_sums, sblocks, c->scal);
+    scan_apply<<<sblocks, kThreads, 0, c->stream>>>(c->tree.flag, n, c->scan.block_sums,
+                                                     c->tree.cell_of);
+    tree_link<<<blocks_for(n, kThreads), kThreads, 0, c->stream>>>(key, n, b.pos, b.mass, c->tree,
+                                                                    c->scal);
+    tree_trivial_root<<<1, 1, 0, c->stream>>>(b.pos, b.mass, n, c->tree, c->scal);
+}
+
+void launch_moments(nb_ctx* c, const BodyBuffers& b) {
+    // Cells never exceed n - 1; threads beyond the live count exit at once.
+    const int cap = (int)(c->n > 1 ? c->n - 1 : 1);
+    c->launches += 1;
+    tree_moments<<<blocks_for(cap, kThreads), kThreads, 0, c->stream>>>(c->scal, b.pos, b.mass,
+                                                                        c->tree);
+}
+
+}  // namespace nb

@@ -1,0 +1,452 @@
+// nb_capi.cu -- the extern "C" surface of libnbody_b200.so (include/nbody_b200.h).
+//
+// Owns the context: device buffers (allocated once, as init_device_resources
+// does at BarnesHutCuda.cu:550-606), the stream, and one captured CUDA graph
+// per buffer parity that holds a whole step, so a step costs one graph launch
+// and no host synchronisation (the reference synchronises ~40 times per step).
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "nb_internal.cuh"
+
+namespace {
+
+int fail(nb_ctx* c, int code, const std::string& msg) {
+    if (c) c->err = msg;
+    return code;
+}
+
+#define NB_CUDA(ctx, call)                                                                     \
+    do {                                                                                       \
+        const cudaError_t e_ = (call);                                                         \
+        if (e_ != cudaSuccess)                                                                 \
+            return fail((ctx), NB_ERR_CUDA,                                                    \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));                   \
+    } while (0)
+
+template <typename T>
+cudaError_t dalloc(T** p, size_t count) {
+    return cudaMalloc(reinterpret_cast<void**>(p), sizeof(T) * (count ? count : 1));
+}
+
+bool finite_array(const double* a, size_t count) {
+    for (size_t i = 0; i < count; ++i)
+        if (!std::isfinite(a[i])) return false;
+    return true;
+}
+
+int check_params(const nb_params* p) {
+    if (!p) return NB_ERR_INVALID;
+    if (!std::isfinite(p->G) || !std::isfinite(p->timestep) || !std::isfinite(p->theta) ||
+        !std::isfinite(p->epsilon_squared))
+        return NB_ERR_INVALID;
+    if (p->theta < 0.0 || p->epsilon_squared < 0.0) return NB_ERR_INVALID;
+    if (p->mode != NB_MODE_FP64 && p->mode != NB_MODE_SPLIT) return NB_ERR_INVALID;
+    if (p->leaf_size < 0 || p->flags != 0) return NB_ERR_INVALID;
+    return NB_OK;
+}
+
+int alloc_all(nb_ctx* c) {
+    const size_t n = (size_t)c->n;
+    for (int k = 0; k < 2; ++k) {
+        NB_CUDA(c, dalloc(&c->buf[k].pos, n));
+        NB_CUDA(c, dalloc(&c->buf[k].vel, n));
+        NB_CUDA(c, dalloc(&c->buf[k].mass, n));
+        NB_CUDA(c, dalloc(&c->buf[k].orig, n));
+        NB_CUDA(c, dalloc(&c->sort.key[k], n));
+        NB_CUDA(c, dalloc(&c->sort.val[k], n));
+    }
+    c->sort.tiles = (int)((n + nb::kSortTile - 1) / nb::kSortTile);
+    NB_CUDA(c, dalloc(&c->sort.counts, (size_t)256 * c->sort.tiles));
+    NB_CUDA(c, dalloc(&c->sort.totals, 256));
+    c->scan.blocks = (int)((n + 2047) / 2048);
+    NB_CUDA(c, dalloc(&c->scan.block_sums, (size_t)c->scan.blocks));
+    nb::Tree& t = c->tree;
+    NB_CUDA(c, dalloc(&t.first, n));
+    NB_CUDA(c, dalloc(&t.last, n));
+    NB_CUDA(c, dalloc(&t.level, n));
+    NB_CUDA(c, dalloc(&t.child, n));
+    NB_CUDA(c, dalloc(&t.parent, n));
+    NB_CUDA(c, dalloc(&t.nint, n));
+    NB_CUDA(c, dalloc(&t.ready, n));
+    NB_CUDA(c, dalloc(&t.mass, n));
+    NB_CUDA(c, dalloc(&t.com, n));
+    NB_CUDA(c, dalloc(&t.leaf_last, n));
+    NB_CUDA(c, dalloc(&t.leaf_plevel, n));
+    NB_CUDA(c, dalloc(&t.bucket_mass, n));
+    NB_CUDA(c, dalloc(&t.bucket_com, n));
+    NB_CUDA(c, dalloc(&t.flag, n));
+    NB_CUDA(c, dalloc(&t.cell_of, n));
+    NB_CUDA(c, dalloc(&t.start_of, n));
+    NB_CUDA(c, dalloc(&c->scal, 1));
+    NB_CUDA(c, cudaMemset(c->scal, 0, sizeof(nb::DeviceScalars)));
+    c->bbox_blocks = 2 * c->sm_count;
+    NB_CUDA(c, dalloc(&c->bbox_partials, (size_t)4 * c->bbox_blocks));
+    NB_CUDA(c, dalloc(&c->acc, n));
+    NB_CUDA(c, dalloc(&c->stage_pos, n));
+    NB_CUDA(c, dalloc(&c->stage_vel, n));
+    return NB_OK;
+}
+
+void free_all(nb_ctx* c) {
+    for (int k = 0; k < 2; ++k) {
+        cudaFree(c->buf[k].pos);
+        cudaFree(c->buf[k].vel);
+        cudaFree(c->buf[k].mass);
+        cudaFree(c->buf[k].orig);
+        cudaFree(c->sort.key[k]);
+        cudaFree(c->sort.val[k]);
+    }
+    cudaFree(c->sort.counts);
+    cudaFree(c->sort.totals);
+    cudaFree(c->scan.block_sums);
+    nb::Tree& t = c->tree;
+    void* tree_ptrs[] = {t.first,     t.last,        t.level,       t.child,      t.parent,
+                         t.nint,      t.ready,       t.mass,        t.com,        t.leaf_last,
+                         t.leaf_plevel, t.bucket_mass, t.bucket_com, t.flag,      t.cell_of,
+                         t.start_of};
+    for (void* q : tree_ptrs) cudaFree(q);
+    cudaFree(c->scal);
+    cudaFree(c->bbox_partials);
+    cudaFree(c->acc);
+    cudaFree(c->stage_pos);
+    cudaFree(c->stage_vel);
+}
+
+void drop_graphs(nb_ctx* c) {
+    for (auto& g : c->graph)
+        if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+}
+
+const char* const kPhaseNames[nb::kPhases] = {"bbox+morton", "sort", "gather", "tree",
+                                              "moments", "force", "drift"};
+
+// Enqueues one step reading the state from buf[parity]; leaves it in the
+// other buffer.  integrate=false stops after the force pass (no kick/drift).
+// timed=true records the phase events between stages.
+void enqueue_step(nb_ctx* c, int parity, bool integrate, bool store_acc, bool timed = false) {
+    const nb::BodyBuffers& A = c->buf[parity];
+    const nb::BodyBuffers& B = c->buf[parity ^ 1];
+    auto mark = [&](int k) {
+        if (timed) cudaEventRecord(c->phase_ev[k], c->stream);
+    };
+    mark(0);
+    cudaMemsetAsync(&c->scal->cell_terms, 0, 2 * sizeof(unsigned long long), c->stream);
+    nb::launch_bbox(c, A.pos);
+    nb::launch_morton(c, A.pos);
+    mark(1);
+    nb::launch_sort(c);
+    mark(2);
+    nb::launch_gather(c, A, B);
+    mark(3);
+    nb::launch_tree(c, B);
+    mark(4);
+    nb::launch_moments(c, B);
+    mark(5);
+    nb::launch_force_fp64(c, B, integrate, store_acc);
+    mark(6);
+    if (integrate) nb::launch_drift(c, B);
+    mark(7);
+}
+
+int capture_graph(nb_ctx* c, int parity) {
+    cudaGraph_t g = nullptr;
+    NB_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    const uint64_t before = c->launches;
+    enqueue_step(c, parity, true, false, true);
+    c->kernels_per_step = c->launches - before;
+    const cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    if (e != cudaSuccess) return fail(c, NB_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    const cudaError_t e2 = cudaGraphInstantiate(&c->graph[parity], g, 0);
+    cudaGraphDestroy(g);
+    if (e2 != cudaSuccess)
+        return fail(c, NB_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e2));
+    return NB_OK;
+}
+
+int read_device_error(nb_ctx* c) {
+    unsigned flags = 0;
+    NB_CUDA(c, cudaMemcpyAsync(&flags, &c->scal->error, sizeof(unsigned), cudaMemcpyDeviceToHost,
+                               c->stream));
+    NB_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (!flags) return NB_OK;
+    NB_CUDA(c, cudaMemsetAsync(&c->scal->error, 0, sizeof(unsigned), c->stream));
+    if (flags & nb::kErrTimeout) return fail(c, NB_ERR_TIMEOUT, "a bounded device wait gave up");
+    if (flags & nb::kErrStack) return fail(c, NB_ERR_CAPACITY, "traversal stack bound exceeded");
+    return fail(c, NB_ERR_CAPACITY, "tree build saw more than four children in a cell");
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+}  // namespace
+
+extern "C" {
+
+int nb_params_default(nb_params* p) {
+    if (!p) return NB_ERR_INVALID;
+    std::memset(p, 0, sizeof(*p));
+    p->G = 1.0;
+    p->timestep = 1e-4;
+    p->theta = 0.5;
+    p->epsilon_squared = 1e-4;
+    p->mode = NB_MODE_FP64;
+    return NB_OK;
+}
+
+const char* nb_status_string(int s) {
+    switch (s) {
+        case NB_OK: return "ok";
+        case NB_ERR_INVALID: return "invalid argument";
+        case NB_ERR_CUDA: return "CUDA error";
+        case NB_ERR_CAPACITY: return "device capacity exceeded";
+        case NB_ERR_TIMEOUT: return "device wait timed out";
+        case NB_ERR_NOMEM: return "out of memory";
+        case NB_ERR_NOTFOUND: return "no such CUDA device";
+        default: return "unknown status";
+    }
+}
+
+const char* nb_last_error(const nb_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+int nb_create(const nb_params* p, uint64_t n, const double* mass, const double* pos_xy,
+              const double* vel_xy, nb_ctx** out) {
+    if (!out) return NB_ERR_INVALID;
+    *out = nullptr;
+    if (check_params(p) != NB_OK) return NB_ERR_INVALID;
+    if (n == 0 || n > (uint64_t)INT32_MAX - 1 || !mass || !pos_xy || !vel_xy) return NB_ERR_INVALID;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || p->device < 0 || p->device >= ndev)
+        return NB_ERR_NOTFOUND;
+    nb_ctx* c = new (std::nothrow) nb_ctx();
+    if (!c) return NB_ERR_NOMEM;
+    c->p = *p;
+    c->n = (int64_t)n;
+    c->device = p->device;
+    DeviceGuard guard(c->device);
+    int rc = NB_OK;
+    if (cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) {
+        rc = NB_ERR_CUDA;
+    }
+    for (auto& e : c->phase_ev)
+        if (rc == NB_OK && cudaEventCreate(&e) != cudaSuccess) rc = NB_ERR_CUDA;
+    if (rc == NB_OK) rc = alloc_all(c);
+    if (rc == NB_OK) rc = nb_upload(c, mass, pos_xy, vel_xy);
+    if (rc != NB_OK) {
+        nb_destroy(c);
+        return rc == NB_ERR_CUDA ? NB_ERR_NOMEM : rc;
+    }
+    *out = c;
+    return NB_OK;
+}
+
+int nb_destroy(nb_ctx* c) {
+    if (!c) return NB_OK;
+    DeviceGuard guard(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    drop_graphs(c);
+    free_all(c);
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    for (auto& e : c->phase_ev)
+        if (e) cudaEventDestroy(e);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return NB_OK;
+}
+
+int nb_upload(nb_ctx* c, const double* mass, const double* pos_xy, const double* vel_xy) {
+    if (!c || !mass || !pos_xy || !vel_xy) return NB_ERR_INVALID;
+    const size_t n = (size_t)c->n;
+    if (!finite_array(mass, n) || !finite_array(pos_xy, 2 * n) || !finite_array(vel_xy, 2 * n))
+        return fail(c, NB_ERR_INVALID, "non-finite mass, position or velocity");
+    for (size_t i = 0; i < n; ++i)
+        if (!(mass[i] > 0.0)) return fail(c, NB_ERR_INVALID, "masses must be positive");
+    DeviceGuard guard(c->device);
+    c->parity = 0;
+    const nb::BodyBuffers& A = c->buf[0];
+    NB_CUDA(c, cudaMemcpyAsync(A.mass, mass, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    NB_CUDA(c, cudaMemcpyAsync(A.pos, pos_xy, n * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+    NB_CUDA(c, cudaMemcpyAsync(A.vel, vel_xy, n * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+    nb::launch_identity(c, A.orig);
+    NB_CUDA(c, cudaGetLastError());
+    return NB_OK;
+}
+
+int nb_set_timestep(nb_ctx* c, double dt) {
+    if (!c || !std::isfinite(dt)) return NB_ERR_INVALID;
+    if (dt != c->p.timestep) {
+        DeviceGuard guard(c->device);
+        NB_CUDA(c, cudaStreamSynchronize(c->stream));
+        c->p.timestep = dt;
+        drop_graphs(c);
+    }
+    return NB_OK;
+}
+
+int nb_step(nb_ctx* c, uint32_t nsteps) {
+    if (!c) return NB_ERR_INVALID;
+    if (nsteps == 0) return NB_OK;
+    DeviceGuard guard(c->device);
+    for (int par = 0; par < 2; ++par)
+        if (!c->graph[par]) {
+            const int rc = capture_graph(c, par);
+            if (rc != NB_OK) return rc;
+        }
+    NB_CUDA(c, cudaEventRecord(c->ev0, c->stream));
+    for (uint32_t k = 0; k < nsteps; ++k) {
+        NB_CUDA(c, cudaGraphLaunch(c->graph[c->parity], c->stream));
+        c->parity ^= 1;
+    }
+    NB_CUDA(c, cudaEventRecord(c->ev1, c->stream));
+    c->steps += nsteps;
+    c->batch_steps = nsteps;
+    return NB_OK;
+}
+
+int nb_sync(nb_ctx* c) {
+    if (!c) return NB_ERR_INVALID;
+    DeviceGuard guard(c->device);
+    NB_CUDA(c, cudaStreamSynchronize(c->stream));
+    float ms = 0.f;
+    if (c->batch_steps && cudaEventElapsedTime(&ms, c->ev0, c->ev1) == cudaSuccess)
+        c->ms_last = ms / c->batch_steps;
+    c->batch_steps = 0;
+    return read_device_error(c);
+}
+
+int nb_download(nb_ctx* c, double* pos_xy, double* vel_xy) {
+    if (!c) return NB_ERR_INVALID;
+    if (!pos_xy && !vel_xy) return NB_OK;
+    DeviceGuard guard(c->device);
+    const nb::BodyBuffers& A = c->buf[c->parity];
+    const size_t bytes = (size_t)c->n * sizeof(double2);
+    nb::launch_scatter(c, A, pos_xy ? c->stage_pos : nullptr, vel_xy ? c->stage_vel : nullptr,
+                       nullptr, nullptr);
+    NB_CUDA(c, cudaGetLastError());
+    if (pos_xy)
+        NB_CUDA(c, cudaMemcpyAsync(pos_xy, c->stage_pos, bytes, cudaMemcpyDeviceToHost, c->stream));
+    if (vel_xy)
+        NB_CUDA(c, cudaMemcpyAsync(vel_xy, c->stage_vel, bytes, cudaMemcpyDeviceToHost, c->stream));
+    NB_CUDA(c, cudaStreamSynchronize(c->stream));
+    return read_device_error(c);
+}
+
+int nb_accelerations(nb_ctx* c, double* acc_xy) {
+    if (!c || !acc_xy) return NB_ERR_INVALID;
+    DeviceGuard guard(c->device);
+    enqueue_step(c, c->parity, false, true);
+    NB_CUDA(c, cudaGetLastError());
+    c->parity ^= 1;
+    const nb::BodyBuffers& A = c->buf[c->parity];
+    nb::launch_scatter(c, A, nullptr, nullptr, c->acc, c->stage_pos);
+    NB_CUDA(c, cudaGetLastError());
+    NB_CUDA(c, cudaMemcpyAsync(acc_xy, c->stage_pos, (size_t)c->n * sizeof(double2),
+                               cudaMemcpyDeviceToHost, c->stream));
+    NB_CUDA(c, cudaStreamSynchronize(c->stream));
+    return read_device_error(c);
+}
+
+int nb_debug_morton(nb_ctx* c, uint64_t* codes, int32_t* order, double* box_out) {
+    if (!c) return NB_ERR_INVALID;
+    DeviceGuard guard(c->device);
+    const nb::BodyBuffers& A = c->buf[c->parity];
+    nb::launch_bbox(c, A.pos);
+    nb::launch_morton(c, A.pos);
+    nb::launch_sort(c);
+    NB_CUDA(c, cudaGetLastError());
+    const size_t n = (size_t)c->n;
+    if (codes)
+        NB_CUDA(c, cudaMemcpyAsync(codes, c->sort.key[0], n * 8, cudaMemcpyDeviceToHost, c->stream));
+    if (order)
+        NB_CUDA(c, cudaMemcpyAsync(order, c->sort.val[0], n * 4, cudaMemcpyDeviceToHost, c->stream));
+    if (box_out)
+        NB_CUDA(c, cudaMemcpyAsync(box_out, c->scal->box, 4 * sizeof(double), cudaMemcpyDeviceToHost,
+                                   c->stream));
+    NB_CUDA(c, cudaStreamSynchronize(c->stream));
+    return read_device_error(c);
+}
+
+int nb_debug_state(nb_ctx* c, double* mass, double* pos_xy, double* vel_xy, int32_t* orig) {
+    if (!c) return NB_ERR_INVALID;
+    DeviceGuard guard(c->device);
+    const nb::BodyBuffers& A = c->buf[c->parity];
+    const size_t n = (size_t)c->n;
+    if (mass) NB_CUDA(c, cudaMemcpyAsync(mass, A.mass, n * 8, cudaMemcpyDeviceToHost, c->stream));
+    if (pos_xy) NB_CUDA(c, cudaMemcpyAsync(pos_xy, A.pos, n * 16, cudaMemcpyDeviceToHost, c->stream));
+    if (vel_xy) NB_CUDA(c, cudaMemcpyAsync(vel_xy, A.vel, n * 16, cudaMemcpyDeviceToHost, c->stream));
+    if (orig) NB_CUDA(c, cudaMemcpyAsync(orig, A.orig, n * 4, cudaMemcpyDeviceToHost, c->stream));
+    NB_CUDA(c, cudaStreamSynchronize(c->stream));
+    return NB_OK;
+}
+
+int nb_debug_tree(nb_ctx* c, double* cell_mass, double* cell_com_xy, int32_t* level,
+                  int32_t* first_body, int32_t* last_body, int32_t* root_ref) {
+    if (!c) return NB_ERR_INVALID;
+    DeviceGuard guard(c->device);
+    NB_CUDA(c, cudaStreamSynchronize(c->stream));
+    nb::DeviceScalars s;
+    NB_CUDA(c, cudaMemcpy(&s, c->scal, sizeof(s), cudaMemcpyDeviceToHost));
+    const size_t m = (size_t)s.cells;
+    const nb::Tree& t = c->tree;
+    if (cell_mass && m) NB_CUDA(c, cudaMemcpy(cell_mass, t.mass, m * 8, cudaMemcpyDeviceToHost));
+    if (cell_com_xy && m) NB_CUDA(c, cudaMemcpy(cell_com_xy, t.com, m * 16, cudaMemcpyDeviceToHost));
+    if (level && m) NB_CUDA(c, cudaMemcpy(level, t.level, m * 4, cudaMemcpyDeviceToHost));
+    if (first_body && m) NB_CUDA(c, cudaMemcpy(first_body, t.first, m * 4, cudaMemcpyDeviceToHost));
+    if (last_body && m) NB_CUDA(c, cudaMemcpy(last_body, t.last, m * 4, cudaMemcpyDeviceToHost));
+    if (root_ref) *root_ref = s.root;
+    return NB_OK;
+}
+
+int nb_get_stats(nb_ctx* c, nb_stats* out) {
+    if (!c || !out) return NB_ERR_INVALID;
+    DeviceGuard guard(c->device);
+    NB_CUDA(c, cudaStreamSynchronize(c->stream));
+    nb::DeviceScalars s;
+    NB_CUDA(c, cudaMemcpy(&s, c->scal, sizeof(s), cudaMemcpyDeviceToHost));
+    std::memset(out, 0, sizeof(*out));
+    out->steps = c->steps;
+    out->n = (uint64_t)c->n;
+    out->tree_nodes = (uint64_t)s.cells;
+    out->cell_interactions = s.cell_terms;
+    out->body_interactions = s.body_terms;
+    out->ms_last_step = c->ms_last;
+    out->root_width = s.box[1] - s.box[0];
+    out->kernels_per_step = c->kernels_per_step;
+    return NB_OK;
+}
+
+int nb_phase_times(nb_ctx* c, double* ms, int max) {
+    if (!c || (!ms && max > 0)) return -NB_ERR_INVALID;
+    DeviceGuard guard(c->device);
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return -NB_ERR_CUDA;
+    for (int k = 0; k < nb::kPhases && k < max; ++k) {
+        float t = 0.f;
+        ms[k] = cudaEventElapsedTime(&t, c->phase_ev[k], c->phase_ev[k + 1]) == cudaSuccess ? t : -1.0;
+    }
+    cudaGetLastError();
+    return nb::kPhases;
+}
+
+const char* nb_phase_name(int k) { return k >= 0 && k < nb::kPhases ? kPhaseNames[k] : ""; }
+
+}  // extern "C"

@@ -1,0 +1,128 @@
+// nb_internal.cuh -- device data layout and kernel entry points of the B200
+// Barnes-Hut step.  Everything here is private to libnbody_b200.so; the public
+// surface is include/nbody_b200.h.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "nbody_b200.h"
+
+namespace nb {
+
+constexpr int kMaxLevel = 30;     // level-30 cells are leaves (BarnesHutCuda.cu:182)
+constexpr int kStackDepth = 96;   // >= 1 + 3 * 30 pending cells of a DFS
+constexpr int kSortTileItems = 8; // keys per thread in a radix tile
+constexpr int kSortThreads = 256;
+constexpr int kSortTile = kSortTileItems * kSortThreads;  // 2048 keys
+constexpr int kPhases = 7;        // morton, sort, gather, tree, moments, force, drift
+
+// Device error flags (bit mask in DeviceScalars::error).
+constexpr unsigned kErrStack = 1u;      // DFS stack bound exceeded
+constexpr unsigned kErrTree = 2u;       // tree build saw an impossible range
+constexpr unsigned kErrTimeout = 4u;    // a bounded wait gave up
+
+// Small device-resident values written and read by kernels of one step.
+struct DeviceScalars {
+    double box[4];            // squared root box: x_min, x_max, y_min, y_max
+    double wsq[kMaxLevel + 1];// squared cell width per level (root * 0.25^L)
+    int32_t root;             // >= 0 cell id, < 0 leaf ~first_body
+    int32_t cells;            // internal cells of the current tree
+    unsigned error;           // kErr* bits, sticky until read by the host
+    unsigned bbox_ticket;     // last-block-done counter of the bbox reduction
+    unsigned long long cell_terms;
+    unsigned long long body_terms;
+};
+
+// Body state; two copies so the Morton gather can ping-pong.
+struct BodyBuffers {
+    double2* pos = nullptr;
+    double2* vel = nullptr;
+    double* mass = nullptr;
+    int32_t* orig = nullptr;
+};
+
+// Compressed quadtree, one entry per internal cell (capacity n).
+struct Tree {
+    int32_t* first = nullptr;    // first body of the cell
+    int32_t* last = nullptr;     // last body of the cell
+    int32_t* level = nullptr;    // depth in the reference's uncompressed tree
+    int4* child = nullptr;       // child refs: >= 0 cell, < 0 leaf ~first_body, INT_MIN none
+    int32_t* parent = nullptr;   // parent cell, -1 at the root
+    int32_t* nint = nullptr;     // children that are internal cells
+    int32_t* ready = nullptr;    // bottom-up arrival counter
+    double* mass = nullptr;      // FP64 monopole
+    double2* com = nullptr;
+    // per-body side tables, only meaningful at leaf starts
+    int32_t* leaf_last = nullptr;   // last body of the leaf starting here
+    int32_t* leaf_plevel = nullptr; // level of the leaf's parent cell (-1: root leaf)
+    double* bucket_mass = nullptr;  // moments of multi-body leaves
+    double2* bucket_com = nullptr;
+    // build scratch (per boundary i between bodies i and i+1)
+    int32_t* flag = nullptr;
+    int32_t* cell_of = nullptr;     // exclusive scan of flag
+    int32_t* start_of = nullptr;    // first body of the cell owning boundary i
+};
+
+struct SortBuffers {
+    uint64_t* key[2] = {nullptr, nullptr};
+    uint32_t* val[2] = {nullptr, nullptr};
+    uint32_t* counts = nullptr;   // [256][tiles]
+    uint32_t* totals = nullptr;   // [256]
+    int tiles = 0;
+};
+
+struct ScanBuffers {
+    int32_t* block_sums = nullptr;
+    int blocks = 0;
+};
+
+}  // namespace nb
+
+struct nb_ctx {
+    nb_params p{};
+    int64_t n = 0;
+    int device = 0;
+    int sm_count = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t phase_ev[nb::kPhases + 1] = {};
+    int parity = 0;                 // which BodyBuffers holds the state
+    nb::BodyBuffers buf[2];
+    nb::SortBuffers sort;
+    nb::ScanBuffers scan;
+    nb::Tree tree;
+    nb::DeviceScalars* scal = nullptr;   // device
+    double* bbox_partials = nullptr;     // [blocks][4]
+    int bbox_blocks = 0;
+    double2* acc = nullptr;              // optional FP64 accelerations (sorted order)
+    double2* stage_pos = nullptr;        // original-order staging for downloads
+    double2* stage_vel = nullptr;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};  // one step from parity 0 / 1
+    double graph_dt = 0.0;
+    uint64_t steps = 0;
+    uint32_t batch_steps = 0;       // steps of the last nb_step batch
+    double ms_last = 0.0;
+    uint64_t launches = 0;          // kernel launches enqueued (counted by launchers)
+    uint64_t kernels_per_step = 0;
+    std::string err;
+};
+
+namespace nb {
+
+// Kernel launchers (all enqueue on ctx->stream, no host synchronisation).
+void launch_bbox(nb_ctx* c, const double2* pos);
+void launch_morton(nb_ctx* c, const double2* pos);
+void launch_sort(nb_ctx* c);                                   // result in key[0]/val[0]
+void launch_gather(nb_ctx* c, const BodyBuffers& src, const BodyBuffers& dst);
+void launch_tree(nb_ctx* c, const BodyBuffers& b);
+void launch_moments(nb_ctx* c, const BodyBuffers& b);
+void launch_force_fp64(nb_ctx* c, const BodyBuffers& b, bool kick, bool store_acc);
+void launch_drift(nb_ctx* c, const BodyBuffers& b);
+void launch_scatter(nb_ctx* c, const BodyBuffers& b, double2* out_pos, double2* out_vel,
+                    const double2* acc, double2* out_acc);
+void launch_identity(nb_ctx* c, int32_t* orig);
+
+}  // namespace nb

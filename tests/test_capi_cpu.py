@@ -1,0 +1,54 @@
+"""CPU checks of the C-ABI library: it loads without a GPU and exports every
+entry point the public header declares."""
+import ctypes as C
+import pathlib
+import re
+
+import pytest
+
+ROOT = pathlib.Path(__file__).resolve().parents[1]
+
+
+def header_symbols() -> set[str]:
+    names = set()
+    for h in (ROOT / "include").glob("*.h"):
+        names |= set(re.findall(r"^NB_API\s+[\w\s\*]+?\b(nb_\w+)\s*\(", h.read_text(), re.M))
+    return names
+
+
+def test_header_declares_the_binding_list(nbp):
+    assert header_symbols() == set(nbp.EXPORTS)
+
+
+def test_library_exports_every_declared_symbol(nbp):
+    lib = nbp.load()
+    for name in header_symbols():
+        assert hasattr(lib, name), name
+
+
+def test_status_strings(nbp):
+    lib = nbp.load()
+    assert lib.nb_status_string(0) == b"ok"
+    assert lib.nb_status_string(3) == b"device capacity exceeded"
+    assert lib.nb_last_error(None) == b"null context"
+
+
+def test_params_default(nbp):
+    lib = nbp.load()
+    p = nbp.NbParams()
+    assert lib.nb_params_default(C.byref(p)) == 0
+    assert (p.G, p.timestep, p.theta, p.epsilon_squared, p.mode) == (1.0, 1e-4, 0.5, 1e-4, 0)
+
+
+def test_invalid_arguments_rejected_before_any_device_call(nbp):
+    lib = nbp.load()
+    h = C.c_void_p()
+    p = nbp.NbParams()
+    lib.nb_params_default(C.byref(p))
+    p.theta = -1.0
+    one = (C.c_double * 2)(0.0, 0.0)
+    assert lib.nb_create(C.byref(p), 1, one, one, one, C.byref(h)) == 1
+    lib.nb_params_default(C.byref(p))
+    assert lib.nb_create(C.byref(p), 0, one, one, one, C.byref(h)) == 1
+    assert lib.nb_create(None, 1, one, one, one, C.byref(h)) == 1
+    assert lib.nb_destroy(None) == 0

@@ -1,0 +1,191 @@
+"""GPU parity: the CUDA path through the C ABI against the CPU oracle.
+
+Bit-exact for Morton codes, the squared box and the sort permutation;
+accelerations within 1e-5 relative (FP64 mode) of the oracle's restatement
+of the reference traversal, with the same accepted-cell counts."""
+import numpy as np
+import pytest
+
+from conftest import rel_err
+
+pytestmark = pytest.mark.gpu
+
+EPS2 = 1e-4
+TOL = 1e-5  # FP64 mode: relative acceleration tolerance vs the oracle
+
+
+def ctx_for(nbp, m, p, v, theta=0.5, dt=1e-4, G=1.0, mode=0):
+    cfg = nbp.SimConfig(timestep=dt, theta=theta, epsilon_squared=EPS2, G=G, mode=mode)
+    return nbp.NbContext(cfg, m, p, v)
+
+
+def universes(nbp):
+    u = nbp.universes
+    rng = np.random.default_rng(7)
+    yield "disc16k", u.exponential_disc(16384, 0)
+    yield "collision8k", u.colliding_discs(8192, 1)
+    yield "plummer5k", u.plummer_disc(5000, 2)
+    m = rng.random(3001) + 0.1
+    yield "uniform3001", (m, rng.random((3001, 2)) * 100 - 50, rng.normal(size=(3001, 2)))
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 31, 2047, 2048, 2049, 65537])
+def test_morton_sort_bitexact_ragged(nbp, orc, n):
+    rng = np.random.default_rng(n)
+    p = rng.normal(size=(n, 2)) * [4.0, 1.0]
+    if n > 8:
+        p[5] = p[3]  # exact ties keep their slot order
+        p[7] = p[3]
+    m = np.ones(n)
+    with ctx_for(nbp, m, p, np.zeros((n, 2))) as ctx:
+        codes, order, box = ctx.debug_morton()
+    box_o = orc.bbox_squared(p)
+    assert np.array_equal(box, box_o)
+    codes_o, order_o = orc.stable_sort(orc.morton(p, box_o))
+    assert np.array_equal(codes, codes_o)
+    assert np.array_equal(order, order_o)
+
+
+def test_morton_sort_bitexact_workloads(nbp, orc):
+    for name, (m, p, v) in universes(nbp):
+        with ctx_for(nbp, m, p, v) as ctx:
+            codes, order, box = ctx.debug_morton()
+        codes_o, order_o = orc.stable_sort(orc.morton(p))
+        assert np.array_equal(codes, codes_o), name
+        assert np.array_equal(order, order_o), name
+
+
+@pytest.mark.parametrize("theta", [0.0, 0.3, 0.5, 1.0])
+def test_accelerations_fp64(nbp, orc, theta):
+    for name, (m, p, v) in universes(nbp):
+        with ctx_for(nbp, m, p, v, theta=theta) as ctx:
+            acc = ctx.accelerations()
+            st = ctx.stats()
+        ref = orc.RefState(m, p, v)
+        r = ref.step(theta=theta, eps2=EPS2, integrate=False, want_acc=True)
+        acc_o = ref.in_original_order(r["acc"])
+        err = rel_err(acc, acc_o)
+        assert err.max() < TOL, (name, theta, err.max())
+        s = r["stats"]
+        total_o = s["cell_interactions"] + s["body_interactions"]
+        total = st.cell_interactions + st.body_interactions
+        assert abs(total - total_o) <= 1e-6 * total_o + 2, (name, theta, total, total_o)
+
+
+def test_steps_track_oracle(nbp, orc):
+    # Each GPU step is checked against one oracle step taken from the GPU's own
+    # device-order state, so chaos cannot amplify earlier rounding.
+    m, p, v = nbp.universes.exponential_disc(16384, 0)
+    dt = 1e-4
+    with ctx_for(nbp, m, p, v, dt=dt) as ctx:
+        for _ in range(5):
+            mass, pos, vel, orig = ctx.debug_state()
+            v_pre = np.empty_like(vel)
+            v_pre[orig] = vel
+            ref = orc.RefState(mass, pos, vel, orig)
+            ref.step(theta=0.5, eps2=EPS2, dt=dt, G=1.0)
+            ctx.step(1)
+            mass2, pos2, vel2, orig2 = ctx.debug_state()
+            assert np.array_equal(orig2, ref.orig)
+            assert np.array_equal(mass2, ref.mass)
+            kick = vel2 - v_pre[orig2]
+            kick_o = ref.vel - v_pre[ref.orig]
+            assert rel_err(kick, kick_o).max() < TOL
+            bound = 1e-15 * np.abs(ref.pos).max() + dt * np.abs(vel2 - ref.vel).max() * 1.01
+            assert np.abs(pos2 - ref.pos).max() <= bound + 1e-300
+
+
+def test_download_original_order(nbp, orc):
+    m, p, v = nbp.universes.colliding_discs(4096, 3)
+    with ctx_for(nbp, m, p, v) as ctx:
+        pos0, vel0 = ctx.download()
+        assert np.array_equal(pos0, p) and np.array_equal(vel0, v)
+        ctx.step(3)
+        pos, vel = ctx.download()
+    ref = orc.RefState(m, p, v)
+    for _ in range(3):
+        ref.step(theta=0.5, eps2=EPS2)
+    assert np.abs(ref.in_original_order(ref.pos) - pos).max() < 1e-10
+    assert np.abs(ref.in_original_order(ref.vel) - vel).max() < 1e-8
+
+
+def test_tree_invariants(nbp):
+    m, p, v = nbp.universes.exponential_disc(20000, 4)
+    with ctx_for(nbp, m, p, v) as ctx:
+        ctx.accelerations()
+        t = ctx.debug_tree()
+        mass, pos, _, _ = ctx.debug_state()
+    root = t["root"]
+    assert root >= 0
+    assert t["first"][root] == 0 and t["last"][root] == len(m) - 1
+    assert t["mass"][root] == pytest.approx(m.sum(), rel=1e-12)
+    # every cell's mass and centre of mass equal the direct sums over its range
+    for cid in range(0, len(t["mass"]), 37):
+        a, b = t["first"][cid], t["last"][cid]
+        mm = mass[a:b + 1]
+        assert t["mass"][cid] == pytest.approx(mm.sum(), rel=1e-12)
+        com = (mm[:, None] * pos[a:b + 1]).sum(0) / mm.sum()
+        assert np.allclose(t["com"][cid], com, rtol=1e-12, atol=1e-12)
+    assert (t["level"] >= 0).all() and (t["level"] < 30).all()
+
+
+def test_single_body_and_coincident_bodies(nbp, orc):
+    with ctx_for(nbp, np.ones(1), np.zeros((1, 2)), np.ones((1, 2))) as ctx:
+        assert np.array_equal(ctx.accelerations(), np.zeros((1, 2)))
+        ctx.step(2)
+        pos, vel = ctx.download()
+        assert np.allclose(pos, 2e-4) and np.allclose(vel, 1.0)
+    # all bodies on one point: one level-30 leaf holds everything
+    n = 64
+    p = np.full((n, 2), 3.25)
+    m = np.linspace(1.0, 2.0, n)
+    for theta in (0.5, 1.0, 2.0):
+        with ctx_for(nbp, m, p, np.zeros((n, 2)), theta=theta) as ctx:
+            acc = ctx.accelerations()
+        ref = orc.RefState(m, p, np.zeros((n, 2)))
+        r = ref.step(theta=theta, eps2=EPS2, integrate=False, want_acc=True)
+        assert np.allclose(acc, ref.in_original_order(r["acc"]), atol=1e-12)
+
+
+def test_coincident_pairs_inside_disc(nbp, orc):
+    m, p, v = nbp.universes.exponential_disc(8192, 9)
+    p[100:110] = p[50]       # a 11-body multi-body leaf
+    p[200] = p[201]          # and a pair
+    for theta in (0.5, 1.0):
+        with ctx_for(nbp, m, p, v, theta=theta) as ctx:
+            acc = ctx.accelerations()
+        ref = orc.RefState(m, p, v)
+        r = ref.step(theta=theta, eps2=EPS2, integrate=False, want_acc=True)
+        assert r["stats"]["multi_leaves"] == 2
+        err = rel_err(acc, ref.in_original_order(r["acc"]))
+        assert err.max() < TOL, (theta, err.max())
+
+
+def test_rejects_nonfinite_and_nonpositive(nbp):
+    p = np.zeros((4, 2))
+    p[2, 1] = np.nan
+    with pytest.raises(nbp.NbError):
+        ctx_for(nbp, np.ones(4), p, np.zeros((4, 2)))
+    with pytest.raises(nbp.NbError):
+        ctx_for(nbp, np.array([1.0, 0.0]), np.zeros((2, 2)), np.zeros((2, 2)))
+
+
+def test_timestep_hot_swap(nbp, orc):
+    m, p, v = nbp.universes.exponential_disc(2048, 6)
+    with ctx_for(nbp, m, p, v, dt=1e-4) as ctx:
+        ctx.step(1)
+        ctx.set_timestep(2e-4)
+        ctx.step(1)
+        pos, vel = ctx.download()
+    ref = orc.RefState(m, p, v)
+    ref.step(dt=1e-4, eps2=EPS2)
+    ref.step(dt=2e-4, eps2=EPS2)
+    assert np.abs(ref.in_original_order(ref.pos) - pos).max() < 1e-10
+
+
+def test_allpairs_kernel_matches_oracle(nbp, orc):
+    m, p, _ = nbp.universes.colliding_discs(10000, 5)
+    tgt = np.arange(0, 10000, 7)
+    acc = nbp.allpairs_accelerations(m, p, tgt, EPS2)
+    acc_o = orc.allpairs_plummer(m, p, tgt, eps2=EPS2)
+    assert rel_err(acc, acc_o).max() < 1e-12
