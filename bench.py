@@ -182,6 +182,7 @@ def run_reference(args) -> None:
 
 def _config(args) -> dict:
     return {"workload": args.workload, "n": args.n, "theta": args.theta, "mode": args.mode,
+            "quadrupole": bool(getattr(args, "quad", False)), "leaf_size": getattr(args, "leaf", 0),
             "softening": 0.01, "dt": 1e-4, "G": 1.0, "state": "f64",
             "l2": "inputs larger than L2 (state + tree > 126 MB at this N)"}
 
@@ -201,7 +202,7 @@ def run_ours(args) -> None:
     m, p, v = _workload(args.kind, args.n, seed=rank)
     mode = nb.NB_MODE_SPLIT if args.mode == "split" else nb.NB_MODE_FP64
     cfg = nb.SimConfig(timestep=1e-4, theta=args.theta, epsilon_squared=1e-4, G=1.0, mode=mode,
-                       device=local)
+                       device=local, quadrupole=args.quad, leaf_size=args.leaf)
     ctx = nb.NbContext(cfg, m, p, v)
     ctx.step(args.warmup)
 
@@ -247,6 +248,16 @@ def run_ours(args) -> None:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_t = float(t.item())
 
+    accuracy = None
+    if not args.no_accuracy:
+        from nbody_b200 import accuracy as acc_mod
+
+        acc_now = ctx.accelerations()
+        pos_now, _ = ctx.download()
+        accuracy = acc_mod.force_errors(acc_now, m, pos_now, 1e-4, k=args.error_sample,
+                                        device=local)
+        accuracy["oracle"] = "FP64 all-pairs (GPU kernel), same Plummer law"
+
     peaks, peak_kind = _peaks()
     clk = clocks.summary()
     sm_mhz = clk["sm_mhz"] or peaks.get("sm_max_mhz", 1965.0)
@@ -286,6 +297,7 @@ def run_ours(args) -> None:
                 "steps": e2e_steps},
         "gpu_launches": int(st.kernels_per_step) * args.steps,
         "clocks": clk,
+        "accuracy": accuracy,
     }
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.n, args.theta, m, p, v)
@@ -317,6 +329,10 @@ def main(argv=None):
     ap.add_argument("--n", type=int, default=None, help="override the body count")
     ap.add_argument("--theta", type=float, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--quad", action="store_true", help="SPLIT: add quadrupole terms")
+    ap.add_argument("--leaf", type=int, default=0, help="SPLIT: direct-sum cell size (0=default)")
+    ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--error-sample", type=int, default=65536)
     args = ap.parse_args(argv)
     kind, n, theta = WORKLOADS[args.workload]
     args.kind = kind

@@ -54,6 +54,9 @@ extern "C" {
 #define NB_MODE_FP64 0
 #define NB_MODE_SPLIT 1
 
+/* nb_params.flags bits */
+#define NB_FLAG_QUADRUPOLE 1u  /* SPLIT: add the cells' second-moment term */
+
 typedef struct nb_params {
     double G;               /* gravitational constant (Constants::Simulation::G)    */
     double timestep;        /* dt (Config::Simulation::timestep)                    */
@@ -63,7 +66,7 @@ typedef struct nb_params {
     int32_t leaf_size;      /* SPLIT: bodies a cell may hold and still be summed
                                body by body instead of opened (0 = default)         */
     int32_t device;         /* CUDA device ordinal                                  */
-    int32_t flags;          /* reserved, must be 0                                  */
+    int32_t flags;          /* NB_FLAG_* bits; others must be 0                     */
 } nb_params;
 
 typedef struct nb_stats {

@@ -23,6 +23,7 @@ NB_ERR_NOTFOUND = 6
 
 NB_MODE_FP64 = 0
 NB_MODE_SPLIT = 1
+NB_FLAG_QUADRUPOLE = 1
 
 # Every symbol include/nbody_b200.h declares.
 EXPORTS = (

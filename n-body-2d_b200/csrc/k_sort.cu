@@ -99,6 +99,8 @@ bbox_kernel(const double2* __restrict__ pos, int64_t n, double* __restrict__ par
         s->box[1] = bx1;
         s->box[2] = by0;
         s->box[3] = by1;
+        s->center[0] = 0.5 * (bx0 + bx1);
+        s->center[1] = 0.5 * (by0 + by1);
         // CU:717 root width_sq, then CU:216 child_wsq = parent * 0.25 per level.
         const double w = bx1 - bx0;
         double wsq = w * w;
@@ -297,15 +299,23 @@ sort_downsweep(const uint64_t* __restrict__ key_in, const uint32_t* __restrict__
     }
 }
 
+// CU:135-147: gather the bodies into Morton order.  In SPLIT mode it also
+// writes the FP32 source record of each body relative to the box centre.
 __global__ void gather_kernel(const uint32_t* __restrict__ order, int64_t n, BodyBuffers src,
-                              BodyBuffers dst) {
+                              BodyBuffers dst, float4* __restrict__ body4,
+                              const DeviceScalars* __restrict__ s) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
     const uint32_t j = __ldg(order + i);
-    dst.pos[i] = __ldg(src.pos + j);
+    const double2 p = __ldg(src.pos + j);
+    const double m = __ldg(src.mass + j);
+    dst.pos[i] = p;
     dst.vel[i] = __ldg(src.vel + j);
-    dst.mass[i] = __ldg(src.mass + j);
+    dst.mass[i] = m;
     dst.orig[i] = __ldg(src.orig + j);
+    if (body4)
+        body4[i] = make_float4((float)(p.x - s->center[0]), (float)(p.y - s->center[1]), (float)m,
+                               __int_as_float((int)i));
 }
 
 inline unsigned blocks_for(int64_t n, int threads) {
@@ -340,9 +350,10 @@ void launch_sort(nb_ctx* c) {
     }
 }
 
-void launch_gather(nb_ctx* c, const BodyBuffers& src, const BodyBuffers& dst) {
+void launch_gather(nb_ctx* c, const BodyBuffers& src, const BodyBuffers& dst, float4* body4) {
     c->launches += 1;
-    gather_kernel<<<blocks_for(c->n, 256), 256, 0, c->stream>>>(c->sort.val[0], c->n, src, dst);
+    gather_kernel<<<blocks_for(c->n, 256), 256, 0, c->stream>>>(c->sort.val[0], c->n, src, dst,
+                                                                body4, c->scal);
 }
 
 }  // namespace nb

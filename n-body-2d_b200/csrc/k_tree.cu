@@ -265,6 +265,7 @@ __global__ void tree_link(const uint64_t* __restrict__ key, int n,
     }
     t.first[id] = first;
     t.last[id] = last;
+    t.range[id] = make_int2(first, last);
     t.level[id] = c;
     t.child[id] = make_int4(ref[0], ref[1], ref[2], ref[3]);
     t.nint[id] = nint;
@@ -289,6 +290,11 @@ __global__ void tree_trivial_root(const double2* __restrict__ pos, const double*
 // and climb; the last child to arrive at a parent (atomic counter) computes
 // it.  Sums run over the children in quadrant order with the reference's
 // arithmetic (CU:329-343): M += m; R = fma(m, com, R); com = R / M.
+// kSplit also accumulates second moments about the COM by the parallel-axis
+// rule, S = sum_c [S_c + m_c d_c d_c^T] with d_c = com_c - com, in FP64, and
+// packs the FP32 records the group traversal reads.  Leaves have S = 0 (a
+// multi-body leaf spans less than width / 2^30, so its own S is negligible).
+template <bool kSplit>
 __global__ void tree_moments(DeviceScalars* __restrict__ s, const double2* __restrict__ pos,
                              const double* __restrict__ mass, Tree t) {
     int id = blockIdx.x * blockDim.x + threadIdx.x;
@@ -303,32 +309,60 @@ __global__ void tree_moments(DeviceScalars* __restrict__ s, const double2* __res
         }
         const int4 ch = t.child[id];
         const int refs[4] = {ch.x, ch.y, ch.z, ch.w};
+        double cm[4], cmx[4], cmy[4];
         double M = 0.0, Rx = 0.0, Ry = 0.0;
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             const int r = refs[q];
-            if (r == INT_MIN) break;
-            double cm;
+            cm[q] = 0.0;
+            cmx[q] = 0.0;
+            cmy[q] = 0.0;
+            if (r == INT_MIN) continue;
             double2 cc;
             if (r >= 0) {
-                cm = __ldcg(t.mass + r);
+                cm[q] = __ldcg(t.mass + r);
                 cc = __ldcg(t.com + r);
             } else {
                 const int b = ~r;
                 if (t.leaf_last[b] == b) {
-                    cm = mass[b];
+                    cm[q] = mass[b];
                     cc = pos[b];
                 } else {
-                    cm = t.bucket_mass[b];
+                    cm[q] = t.bucket_mass[b];
                     cc = t.bucket_com[b];
                 }
             }
-            M += cm;
-            Rx = fma(cm, cc.x, Rx);
-            Ry = fma(cm, cc.y, Ry);
+            cmx[q] = cc.x;
+            cmy[q] = cc.y;
+            M += cm[q];
+            Rx = fma(cm[q], cc.x, Rx);
+            Ry = fma(cm[q], cc.y, Ry);
         }
+        const double2 com = make_double2(Rx / M, Ry / M);
         __stcg(t.mass + id, M);
-        __stcg(t.com + id, make_double2(Rx / M, Ry / M));
+        __stcg(t.com + id, com);
+        if (kSplit) {
+            double sxx = 0.0, sxy = 0.0, syy = 0.0;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int r = refs[q];
+                if (r == INT_MIN) continue;
+                if (r >= 0) {
+                    const double4 sc = __ldcg(t.s64 + r);
+                    sxx += sc.x;
+                    sxy += sc.y;
+                    syy += sc.z;
+                }
+                const double dx = cmx[q] - com.x, dy = cmy[q] - com.y;
+                sxx += cm[q] * dx * dx;
+                sxy += cm[q] * dx * dy;
+                syy += cm[q] * dy * dy;
+            }
+            __stcg(t.s64 + id, make_double4(sxx, sxy, syy, 0.0));
+            t.cell4[id] = make_float4((float)(com.x - s->center[0]), (float)(com.y - s->center[1]),
+                                      (float)M, (float)s->wsq[t.level[id]]);
+            t.cellq[id] = make_float4((float)sxx, (float)sxy, (float)syy, 0.f);
+        }
         __threadfence();
         const int par = t.parent[id];
         if (par < 0) return;
@@ -365,12 +399,16 @@ void launch_tree(nb_ctx* c, const BodyBuffers& b) {
     tree_trivial_root<<<1, 1, 0, c->stream>>>(b.pos, b.mass, n, c->tree, c->scal);
 }
 
-void launch_moments(nb_ctx* c, const BodyBuffers& b) {
+void launch_moments(nb_ctx* c, const BodyBuffers& b, bool split) {
     // Cells never exceed n - 1; threads beyond the live count exit at once.
     const int cap = (int)(c->n > 1 ? c->n - 1 : 1);
     c->launches += 1;
-    tree_moments<<<blocks_for(cap, kThreads), kThreads, 0, c->stream>>>(c->scal, b.pos, b.mass,
-                                                                        c->tree);
+    if (split)
+        tree_moments<true><<<blocks_for(cap, kThreads), kThreads, 0, c->stream>>>(c->scal, b.pos,
+                                                                                  b.mass, c->tree);
+    else
+        tree_moments<false><<<blocks_for(cap, kThreads), kThreads, 0, c->stream>>>(c->scal, b.pos,
+                                                                                   b.mass, c->tree);
 }
 
 }  // namespace nb

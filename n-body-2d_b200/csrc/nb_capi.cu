@@ -48,7 +48,7 @@ int check_params(const nb_params* p) {
         return NB_ERR_INVALID;
     if (p->theta < 0.0 || p->epsilon_squared < 0.0) return NB_ERR_INVALID;
     if (p->mode != NB_MODE_FP64 && p->mode != NB_MODE_SPLIT) return NB_ERR_INVALID;
-    if (p->leaf_size < 0 || p->flags != 0) return NB_ERR_INVALID;
+    if (p->leaf_size < 0 || (p->flags & ~(int32_t)NB_FLAG_QUADRUPOLE) != 0) return NB_ERR_INVALID;
     return NB_OK;
 }
 
@@ -77,6 +77,13 @@ int alloc_all(nb_ctx* c) {
     NB_CUDA(c, dalloc(&t.ready, n));
     NB_CUDA(c, dalloc(&t.mass, n));
     NB_CUDA(c, dalloc(&t.com, n));
+    NB_CUDA(c, dalloc(&t.range, n));
+    if (c->p.mode == NB_MODE_SPLIT) {
+        NB_CUDA(c, dalloc(&t.s64, n));
+        NB_CUDA(c, dalloc(&t.cell4, n));
+        NB_CUDA(c, dalloc(&t.cellq, n));
+        NB_CUDA(c, dalloc(&t.body4, n));
+    }
     NB_CUDA(c, dalloc(&t.leaf_last, n));
     NB_CUDA(c, dalloc(&t.leaf_plevel, n));
     NB_CUDA(c, dalloc(&t.bucket_mass, n));
@@ -110,7 +117,8 @@ void free_all(nb_ctx* c) {
     void* tree_ptrs[] = {t.first,     t.last,        t.level,       t.child,      t.parent,
                          t.nint,      t.ready,       t.mass,        t.com,        t.leaf_last,
                          t.leaf_plevel, t.bucket_mass, t.bucket_com, t.flag,      t.cell_of,
-                         t.start_of};
+                         t.start_of,  t.range,       t.s64,         t.cell4,      t.cellq,
+                         t.body4};
     for (void* q : tree_ptrs) cudaFree(q);
     cudaFree(c->scal);
     cudaFree(c->bbox_partials);
@@ -136,8 +144,10 @@ const char* const kPhaseNames[nb::kPhases] = {"bbox+morton", "sort", "gather", "
 void enqueue_step(nb_ctx* c, int parity, bool integrate, bool store_acc, bool timed = false) {
     const nb::BodyBuffers& A = c->buf[parity];
     const nb::BodyBuffers& B = c->buf[parity ^ 1];
+    // External records become event nodes of the captured graph, so the
+    // events carry timestamps from every replay of the step.
     auto mark = [&](int k) {
-        if (timed) cudaEventRecord(c->phase_ev[k], c->stream);
+        if (timed) cudaEventRecordWithFlags(c->phase_ev[k], c->stream, cudaEventRecordExternal);
     };
     mark(0);
     cudaMemsetAsync(&c->scal->cell_terms, 0, 2 * sizeof(unsigned long long), c->stream);
@@ -146,15 +156,21 @@ void enqueue_step(nb_ctx* c, int parity, bool integrate, bool store_acc, bool ti
     mark(1);
     nb::launch_sort(c);
     mark(2);
-    nb::launch_gather(c, A, B);
+    const bool split = c->p.mode == NB_MODE_SPLIT;
+    nb::launch_gather(c, A, B, split ? c->tree.body4 : nullptr);
     mark(3);
     nb::launch_tree(c, B);
     mark(4);
-    nb::launch_moments(c, B);
+    nb::launch_moments(c, B, split);
     mark(5);
-    nb::launch_force_fp64(c, B, integrate, store_acc);
-    mark(6);
-    if (integrate) nb::launch_drift(c, B);
+    if (split) {
+        nb::launch_force_split(c, B, integrate, store_acc);  // kick and drift fused
+        mark(6);
+    } else {
+        nb::launch_force_fp64(c, B, integrate, store_acc);
+        mark(6);
+        if (integrate) nb::launch_drift(c, B);
+    }
     mark(7);
 }
 

@@ -27,6 +27,7 @@ constexpr unsigned kErrTimeout = 4u;    // a bounded wait gave up
 // Small device-resident values written and read by kernels of one step.
 struct DeviceScalars {
     double box[4];            // squared root box: x_min, x_max, y_min, y_max
+    double center[2];         // box centre: origin of the FP32 coordinates
     double wsq[kMaxLevel + 1];// squared cell width per level (root * 0.25^L)
     int32_t root;             // >= 0 cell id, < 0 leaf ~first_body
     int32_t cells;            // internal cells of the current tree
@@ -55,6 +56,13 @@ struct Tree {
     int32_t* ready = nullptr;    // bottom-up arrival counter
     double* mass = nullptr;      // FP64 monopole
     double2* com = nullptr;
+    int2* range = nullptr;       // {first, last} body of the cell (one 8-byte load)
+    // SPLIT mode: FP64 second moments about the COM for the bottom-up pass and
+    // the packed FP32 records the traversal reads
+    double4* s64 = nullptr;      // {Sxx, Sxy, Syy, 0}
+    float4* cell4 = nullptr;     // {com_x - cx, com_y - cy, mass, width^2}
+    float4* cellq = nullptr;     // {Sxx, Sxy, Syy, 0}
+    float4* body4 = nullptr;     // per body {x - cx, y - cy, mass, index bits}
     // per-body side tables, only meaningful at leaf starts
     int32_t* leaf_last = nullptr;   // last body of the leaf starting here
     int32_t* leaf_plevel = nullptr; // level of the leaf's parent cell (-1: root leaf)
@@ -116,9 +124,10 @@ namespace nb {
 void launch_bbox(nb_ctx* c, const double2* pos);
 void launch_morton(nb_ctx* c, const double2* pos);
 void launch_sort(nb_ctx* c);                                   // result in key[0]/val[0]
-void launch_gather(nb_ctx* c, const BodyBuffers& src, const BodyBuffers& dst);
+void launch_gather(nb_ctx* c, const BodyBuffers& src, const BodyBuffers& dst, float4* body4);
 void launch_tree(nb_ctx* c, const BodyBuffers& b);
-void launch_moments(nb_ctx* c, const BodyBuffers& b);
+void launch_moments(nb_ctx* c, const BodyBuffers& b, bool split);
+void launch_force_split(nb_ctx* c, const BodyBuffers& b, bool kick, bool store_acc);
 void launch_force_fp64(nb_ctx* c, const BodyBuffers& b, bool kick, bool store_acc);
 void launch_drift(nb_ctx* c, const BodyBuffers& b);
 void launch_scatter(nb_ctx* c, const BodyBuffers& b, double2* out_pos, double2* out_vel,

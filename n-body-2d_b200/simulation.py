@@ -66,6 +66,7 @@ class SimConfig:
     mode: int = _lib.NB_MODE_FP64
     leaf_size: int = 0
     device: int = 0
+    quadrupole: bool = False
 
     def params(self) -> NbParams:
         p = NbParams()
@@ -77,6 +78,7 @@ class SimConfig:
         p.mode = self.mode
         p.leaf_size = self.leaf_size
         p.device = self.device
+        p.flags = _lib.NB_FLAG_QUADRUPOLE if self.quadrupole else 0
         return p
 
 

@@ -1,0 +1,84 @@
+"""GPU tests of SPLIT mode (warp-cooperative FP32 group traversal).
+
+SPLIT decides acceptance once per 32-body group, so its cell set differs from
+the reference's per-body walk; it is judged against the FP64 all-pairs sum and
+against the FP64 parity mode's own error."""
+import numpy as np
+import pytest
+
+from conftest import rel_err
+
+pytestmark = pytest.mark.gpu
+EPS2 = 1e-4
+
+
+def accel(nbp, m, p, v, mode, theta, quad=False, leaf=0):
+    cfg = nbp.SimConfig(theta=theta, epsilon_squared=EPS2, mode=mode, quadrupole=quad,
+                        leaf_size=leaf)
+    with nbp.NbContext(cfg, m, p, v) as ctx:
+        a = ctx.accelerations()
+        st = ctx.stats()
+    return a, st
+
+
+@pytest.mark.parametrize("n", [1, 2, 33, 1000, 16384])
+def test_theta_zero_is_allpairs_in_fp32(nbp, orc, n):
+    m, p, v = nbp.universes.exponential_disc(max(n, 2), 3)
+    m, p, v = m[:n], p[:n], v[:n]
+    a, _ = accel(nbp, m, p, v, nbp.NB_MODE_SPLIT, 0.0, leaf=1)
+    exact = orc.allpairs_plummer(m, p, eps2=EPS2)
+    if n == 1:
+        assert np.array_equal(a, np.zeros((1, 2)))
+        return
+    assert rel_err(a, exact).max() < 2e-4
+
+
+def test_monopole_error_not_worse_than_reference_walk(nbp):
+    m, p, v = nbp.universes.exponential_disc(16384, 0)
+    exact = nbp.allpairs_accelerations(m, p, np.arange(16384), EPS2)
+    a64, _ = accel(nbp, m, p, v, nbp.NB_MODE_FP64, 0.5)
+    a32, st = accel(nbp, m, p, v, nbp.NB_MODE_SPLIT, 0.5)
+    e64, e32 = rel_err(a64, exact), rel_err(a32, exact)
+    assert np.percentile(e32, 99) <= np.percentile(e64, 99) * 1.02
+    assert np.percentile(e32, 50) <= np.percentile(e64, 50) * 1.02
+    assert st.cell_interactions > 0 and st.body_interactions > 0
+
+
+@pytest.mark.parametrize("theta", [0.5, 0.8])
+def test_quadrupole_reduces_error(nbp, theta):
+    m, p, v = nbp.universes.colliding_discs(32768, 1)
+    tgt = np.arange(0, 32768, 3)
+    exact = nbp.allpairs_accelerations(m, p, tgt, EPS2)
+    a1, _ = accel(nbp, m, p, v, nbp.NB_MODE_SPLIT, theta)
+    a2, _ = accel(nbp, m, p, v, nbp.NB_MODE_SPLIT, theta, quad=True)
+    e1, e2 = rel_err(a1[tgt], exact), rel_err(a2[tgt], exact)
+    assert np.percentile(e2, 99) < 0.5 * np.percentile(e1, 99)
+    if theta == 0.5:
+        assert np.percentile(e2, 99) < 1e-3
+
+
+def test_split_step_matches_fp64_step(nbp):
+    m, p, v = nbp.universes.colliding_discs(8192, 2)
+    out = {}
+    for mode in (nbp.NB_MODE_FP64, nbp.NB_MODE_SPLIT):
+        cfg = nbp.SimConfig(theta=0.0, epsilon_squared=EPS2, mode=mode, leaf_size=1)
+        with nbp.NbContext(cfg, m, p, v) as ctx:
+            a0 = ctx.accelerations()
+            ctx.step(1)
+            out[mode] = (a0, *ctx.download())
+    a64, p64, v64 = out[nbp.NB_MODE_FP64]
+    a32, p32, v32 = out[nbp.NB_MODE_SPLIT]
+    dv = 1e-4 * np.abs(a64 - a32).max()
+    assert np.abs(v64 - v32).max() <= dv * 1.01 + 1e-15
+    assert np.abs(p64 - p32).max() <= 1e-4 * dv * 1.01 + 1e-13
+
+
+def test_split_coincident_and_ragged(nbp, orc):
+    rng = np.random.default_rng(4)
+    n = 1000
+    p = rng.random((n, 2))
+    p[10:40] = p[5]  # 31 coincident bodies (a multi-body leaf)
+    m = rng.random(n) + 0.5
+    a, _ = accel(nbp, m, p, np.zeros((n, 2)), nbp.NB_MODE_SPLIT, 0.0, leaf=1)
+    exact = orc.allpairs_plummer(m, p, eps2=EPS2)
+    assert rel_err(a, exact).max() < 2e-4
