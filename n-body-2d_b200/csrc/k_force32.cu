@@ -31,6 +31,8 @@ constexpr int kWarpsPerBlock = 4;
 constexpr int kStk = 256;              // stack bound kept by the batch size rule
 constexpr int kStkAlloc = kStk + 96;   // + one depth-first descent (<= 3 x 30 + 1)
 constexpr int kList = 64;
+constexpr int kBodiesPerLane = 2;      // group of 64 bodies per warp
+constexpr int kDefaultLeaf = 16;       // cells this small are summed body by body
 
 struct WarpLists {
     int stack[kStkAlloc];
@@ -68,77 +70,111 @@ __device__ __forceinline__ float warp_max(float v) {
     return v;
 }
 
-// Sum cnt cell entries into (ax, ay).
-template <bool kQuad>
-__device__ __forceinline__ void sum_cells(const WarpLists& L, int cnt, float px, float py,
-                                          float eps2, float& ax, float& ay) {
-    for (int j = 0; j < cnt; ++j) {
-        const float4 e = L.cell[j];
-        const float dx = e.x - px, dy = e.y - py;
+// Sum cnt cell entries into the accelerations of the lane's kBPL bodies.
+template <bool kQuad, int kBPL>
+__device__ __forceinline__ void cell_terms(const float4 e, const float4 q, const float* px,
+                                           const float* py, float eps2, float* ax, float* ay) {
+#pragma unroll
+    for (int b = 0; b < kBPL; ++b) {
+        const float dx = e.x - px[b], dy = e.y - py[b];
         const float d2 = fmaf(dx, dx, fmaf(dy, dy, eps2));
         const float inv = rsqrtf(d2);
-        const float inv3 = inv * inv * inv;
+        const float inv2 = inv * inv;
+        const float inv3 = inv * inv2;
         if (kQuad) {
-            const float4 q = L.quad[j];
-            const float inv2 = inv * inv;
             const float inv5 = inv3 * inv2;
             const float inv7 = inv5 * inv2;
             const float sdx = fmaf(q.x, dx, q.y * dy);
             const float sdy = fmaf(q.y, dx, q.z * dy);
             const float dsd = fmaf(dx, sdx, dy * sdy);
             // a = d [M r^-3 - 1.5 tr(S) r^-5 + 7.5 (d.S.d) r^-7] - 3 r^-5 S d
-            const float radial = fmaf(7.5f * dsd, inv7, fmaf(-1.5f * (q.x + q.z), inv5, e.z * inv3));
-            ax = fmaf(dx, radial, fmaf(-3.f * inv5, sdx, ax));
-            ay = fmaf(dy, radial, fmaf(-3.f * inv5, sdy, ay));
+            const float radial =
+                fmaf(7.5f * dsd, inv7, fmaf(-1.5f * (q.x + q.z), inv5, e.z * inv3));
+            ax[b] = fmaf(dx, radial, fmaf(-3.f * inv5, sdx, ax[b]));
+            ay[b] = fmaf(dy, radial, fmaf(-3.f * inv5, sdy, ay[b]));
         } else {
             const float a = e.z * inv3;
-            ax = fmaf(dx, a, ax);
-            ay = fmaf(dy, a, ay);
+            ax[b] = fmaf(dx, a, ax[b]);
+            ay[b] = fmaf(dy, a, ay[b]);
         }
     }
 }
 
-__device__ __forceinline__ void sum_bodies(const WarpLists& L, int cnt, float px, float py,
-                                           float eps2, int me, float& ax, float& ay) {
-    for (int j = 0; j < cnt; ++j) {
-        const float4 e = L.body[j];
-        const bool self = __float_as_int(e.w) == me;
-        const float dx = e.x - px, dy = e.y - py;
+template <int kBPL>
+__device__ __forceinline__ void body_terms(const float4 e, const float* px, const float* py,
+                                           const int* me, float eps2, float* ax, float* ay) {
+#pragma unroll
+    for (int b = 0; b < kBPL; ++b) {
+        const bool self = __float_as_int(e.w) == me[b];
+        const float dx = e.x - px[b], dy = e.y - py[b];
         const float d2 = self ? 1.f : fmaf(dx, dx, fmaf(dy, dy, eps2));
         const float inv = rsqrtf(d2);
-        const float a = (self ? 0.f : e.z) * inv * inv * inv;
-        ax = fmaf(dx, a, ax);
-        ay = fmaf(dy, a, ay);
+        const float a = (self ? 0.f : e.z) * (inv * inv) * inv;
+        ax[b] = fmaf(dx, a, ax[b]);
+        ay[b] = fmaf(dy, a, ay[b]);
     }
 }
 
-template <bool kQuad>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32)
-force_split(double2* __restrict__ pos, double2* __restrict__ vel, double2* __restrict__ acc_out,
-            int n, Tree t, DeviceScalars* __restrict__ s, float eps2, float theta2, int leaf_size,
-            double G_dt, double dt, int kick) {
-    __shared__ WarpLists lists[kWarpsPerBlock];
+template <bool kQuad, int kBPL>
+__device__ __forceinline__ void sum_cells(const WarpLists& L, int cnt, const float* px,
+                                          const float* py, float eps2, float* ax, float* ay) {
+    if (cnt == 32) {
+#pragma unroll 4
+        for (int j = 0; j < 32; ++j)
+            cell_terms<kQuad, kBPL>(L.cell[j], kQuad ? L.quad[j] : L.cell[j], px, py, eps2, ax, ay);
+    } else {
+        for (int j = 0; j < cnt; ++j)
+            cell_terms<kQuad, kBPL>(L.cell[j], kQuad ? L.quad[j] : L.cell[j], px, py, eps2, ax, ay);
+    }
+}
+
+template <int kBPL>
+__device__ __forceinline__ void sum_bodies(const WarpLists& L, int cnt, const float* px,
+                                           const float* py, const int* me, float eps2, float* ax,
+                                           float* ay) {
+    if (cnt == 32) {
+#pragma unroll 4
+        for (int j = 0; j < 32; ++j) body_terms<kBPL>(L.body[j], px, py, me, eps2, ax, ay);
+    } else {
+        for (int j = 0; j < cnt; ++j) body_terms<kBPL>(L.body[j], px, py, me, eps2, ax, ay);
+    }
+}
+
+// Walk the tree for one group [g0, g1] of <= 32 kBPL bodies (lane l owns
+// g0 + l, g0 + 32 + l, ...) and accumulate the FP32 accelerations.
+template <bool kQuad, int kBPL>
+__device__ __forceinline__ void walk_group(WarpLists& L, const Tree& t, int root, int n, int g0,
+                                           int g1, const float* px, const float* py, const int* me,
+                                           const bool* act_body, float eps2, float theta2,
+                                           int leaf_size, float* ax, float* ay,
+                                           unsigned long long& ncell, unsigned long long& npair,
+                                           unsigned* err) {
     const int lane = threadIdx.x & 31;
-    WarpLists& L = lists[threadIdx.x >> 5];
-    const int group = blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
-    const int g0 = group * 32;
-    if (g0 >= n) return;  // whole warp leaves together
-    const int g1 = min(g0 + 31, n - 1);
-    const int i = min(g0 + lane, g1);
-    const bool valid = g0 + lane < n;
-    const double cx = s->center[0], cy = s->center[1];
-    const double2 P = pos[i];
-    const float px = (float)(P.x - cx), py = (float)(P.y - cy);
-    const float bx0 = warp_min(px), bx1 = warp_max(px);
-    const float by0 = warp_min(py), by1 = warp_max(py);
+    float bx0 = INFINITY, bx1 = -INFINITY, by0 = INFINITY, by1 = -INFINITY;
+#pragma unroll
+    for (int b = 0; b < kBPL; ++b)
+        if (act_body[b]) {
+            bx0 = fminf(bx0, px[b]);
+            bx1 = fmaxf(bx1, px[b]);
+            by0 = fminf(by0, py[b]);
+            by1 = fmaxf(by1, py[b]);
+        }
+    bx0 = warp_min(bx0);
+    bx1 = warp_max(bx1);
+    by0 = warp_min(by0);
+    by1 = warp_max(by1);
     const float gcx = 0.5f * (bx0 + bx1), gcy = 0.5f * (by0 + by1);
     const float ghx = 0.5f * (bx1 - bx0), ghy = 0.5f * (by1 - by0);
     const unsigned below = lanemask_lt();
-
-    float ax = 0.f, ay = 0.f;
-    unsigned long long ncell = 0, npair = 0;
+#pragma unroll
+    for (int b = 0; b < kBPL; ++b) {
+        ax[b] = 0.f;
+        ay[b] = 0.f;
+    }
+    ncell = 0;
+    npair = 0;
     int ccount = 0, bcount = 0, size = 1;
-    if (lane == 0) L.stack[0] = s->root;
+    if (lane == 0) L.stack[0] = root;
     __syncwarp();
 
     while (size > 0) {
@@ -186,7 +222,7 @@ force_split(double2* __restrict__ pos, double2* __restrict__ vel, double2* __res
         ccount += __popc(acc_mask);
         __syncwarp();
         if (ccount >= 32) {
-            sum_cells<kQuad>(L, 32, px, py, eps2, ax, ay);
+            sum_cells<kQuad, kBPL>(L, 32, px, py, eps2, ax, ay);
             ncell += 32;
             __syncwarp();
             // entries 32.. move down; source and destination slots never overlap
@@ -203,7 +239,7 @@ force_split(double2* __restrict__ pos, double2* __restrict__ vel, double2* __res
         int pushed;
         const int off = warp_exclusive_sum(nch, pushed);
         if (size + pushed > kStkAlloc) {  // excluded by the batch rule; stop safely
-            if (lane == 0) atomicOr(&s->error, kErrStack);
+            if (lane == 0) atomicOr(err, kErrStack);
             break;
         }
         if (act == 3) {
@@ -233,7 +269,7 @@ force_split(double2* __restrict__ pos, double2* __restrict__ vel, double2* __res
             bcount += added;
             __syncwarp();
             if (bcount >= 32) {
-                sum_bodies(L, 32, px, py, eps2, i, ax, ay);
+                sum_bodies<kBPL>(L, 32, px, py, me, eps2, ax, ay);
                 npair += 32;
                 __syncwarp();
                 if (lane < bcount - 32) L.body[lane] = L.body[32 + lane];
@@ -242,52 +278,105 @@ force_split(double2* __restrict__ pos, double2* __restrict__ vel, double2* __res
             }
         }
     }
-    sum_cells<kQuad>(L, ccount, px, py, eps2, ax, ay);
-    sum_bodies(L, bcount, px, py, eps2, i, ax, ay);
+    sum_cells<kQuad, kBPL>(L, ccount, px, py, eps2, ax, ay);
+    sum_bodies<kBPL>(L, bcount, px, py, me, eps2, ax, ay);
     ncell += ccount;
     npair += bcount;
+    __syncwarp();
+}
 
-    if (valid) {
-        if (acc_out) acc_out[i] = make_double2((double)ax, (double)ay);
-        if (kick) {
-            double2 v = vel[i];
-            v.x += (double)ax * G_dt;
-            v.y += (double)ay * G_dt;
-            vel[i] = v;
-            double2 p = P;
-            p.x += v.x * dt;
-            p.y += v.y * dt;
-            pos[i] = p;
+// Persistent: each warp takes groups from a global ticket until none is left,
+// which balances groups of very different cost.
+template <bool kQuad, int kBPL>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32)
+force_split(double2* __restrict__ pos, double2* __restrict__ vel, double2* __restrict__ acc_out,
+            int n, Tree t, DeviceScalars* __restrict__ s, float eps2, float theta2, int leaf_size,
+            double G_dt, double dt, int kick) {
+    __shared__ WarpLists lists[kWarpsPerBlock];
+    const int lane = threadIdx.x & 31;
+    WarpLists& L = lists[threadIdx.x >> 5];
+    const int ngroups = s->groups;
+    const int root = s->root;
+    const double cx = s->center[0], cy = s->center[1];
+    unsigned long long cells_total = 0, pairs_total = 0;
+    while (true) {
+        int g = 0;
+        if (lane == 0) g = (int)atomicAdd(&s->group_ticket, 1u);
+        g = __shfl_sync(kFull, g, 0);
+        if (g >= ngroups) break;
+        const int2 gr = t.groups[g];
+        const int g0 = gr.x, g1 = min(gr.y, n - 1);
+        int me[kBPL];
+        bool on[kBPL];
+        float px[kBPL], py[kBPL], ax[kBPL], ay[kBPL];
+        double2 P[kBPL];
+#pragma unroll
+        for (int b = 0; b < kBPL; ++b) {
+            on[b] = g0 + 32 * b + lane <= g1;
+            me[b] = min(g0 + 32 * b + lane, g1);
+            P[b] = pos[me[b]];
+            px[b] = (float)(P[b].x - cx);
+            py[b] = (float)(P[b].y - cy);
         }
+        unsigned long long ncell, npair;
+        walk_group<kQuad, kBPL>(L, t, root, n, g0, g1, px, py, me, on, eps2, theta2, leaf_size, ax,
+                                ay, ncell, npair, &s->error);
+#pragma unroll
+        for (int b = 0; b < kBPL; ++b) {
+            if (!on[b]) continue;
+            const int i = me[b];
+            if (acc_out) acc_out[i] = make_double2((double)ax[b], (double)ay[b]);
+            if (kick) {
+                double2 v = vel[i];
+                v.x += (double)ax[b] * G_dt;
+                v.y += (double)ay[b] * G_dt;
+                vel[i] = v;
+                double2 p = P[b];
+                p.x += v.x * dt;
+                p.y += v.y * dt;
+                pos[i] = p;
+            }
+        }
+        // every body of the group summed every entry and skipped itself once
+        const unsigned long long bodies = (unsigned long long)(g1 - g0 + 1);
+        cells_total += ncell * bodies;
+        pairs_total += npair * bodies - bodies;
     }
-    // interaction counts: every valid lane summed every entry (self excluded)
     if (lane == 0) {
-        const unsigned long long lanes = (unsigned long long)(g1 - g0 + 1);
-        atomicAdd(&s->cell_terms, ncell * lanes);
-        atomicAdd(&s->body_terms, npair * lanes - lanes);  // each lane skips itself once
+        atomicAdd(&s->cell_terms, cells_total);
+        atomicAdd(&s->body_terms, pairs_total);
     }
 }
 
-inline unsigned blocks_for(int64_t n, int per) { return (unsigned)((n + per - 1) / per); }
+template <bool kQuad, int kBPL>
+void launch_split_kernel(nb_ctx* c, const BodyBuffers& b, bool kick, bool store_acc) {
+    if (c->split_blocks == 0) {
+        int blocks = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, force_split<kQuad, kBPL>,
+                                                          kWarpsPerBlock * 32, 0) != cudaSuccess ||
+            blocks < 1)
+            blocks = 4;
+        c->split_blocks = c->sm_count * blocks;
+    }
+    const float theta2 = (float)(c->p.theta * c->p.theta);
+    const int leaf = c->p.leaf_size > 0 ? c->p.leaf_size : kDefaultLeaf;
+    force_split<kQuad, kBPL><<<c->split_blocks, 32 * kWarpsPerBlock, 0, c->stream>>>(
+        b.pos, b.vel, store_acc ? c->acc : nullptr, (int)c->n, c->tree, c->scal,
+        (float)c->p.epsilon_squared, theta2, leaf, c->p.G * c->p.timestep, c->p.timestep,
+        kick ? 1 : 0);
+}
 
 }  // namespace
 
+int split_group_size(const nb_ctx* c) { return 32 * kBodiesPerLane; }
+
 void launch_force_split(nb_ctx* c, const BodyBuffers& b, bool kick, bool store_acc) {
-    const float theta2 = (float)(c->p.theta * c->p.theta);
-    const int leaf = c->p.leaf_size > 0 ? c->p.leaf_size : 16;
-    const unsigned blocks = blocks_for(c->n, 32 * kWarpsPerBlock);
     c->launches += 1;
-    const bool quad = (c->p.flags & NB_FLAG_QUADRUPOLE) != 0;
-    if (quad)
-        force_split<true><<<blocks, 32 * kWarpsPerBlock, 0, c->stream>>>(
-            b.pos, b.vel, store_acc ? c->acc : nullptr, (int)c->n, c->tree, c->scal,
-            (float)c->p.epsilon_squared, theta2, leaf, c->p.G * c->p.timestep, c->p.timestep,
-            kick ? 1 : 0);
+    cudaMemsetAsync(&c->scal->group_ticket, 0, sizeof(unsigned), c->stream);
+    if (c->p.flags & NB_FLAG_QUADRUPOLE)
+        launch_split_kernel<true, kBodiesPerLane>(c, b, kick, store_acc);
     else
-        force_split<false><<<blocks, 32 * kWarpsPerBlock, 0, c->stream>>>(
-            b.pos, b.vel, store_acc ? c->acc : nullptr, (int)c->n, c->tree, c->scal,
-            (float)c->p.epsilon_squared, theta2, leaf, c->p.G * c->p.timestep, c->p.timestep,
-            kick ? 1 : 0);
+        launch_split_kernel<false, kBodiesPerLane>(c, b, kick, store_acc);
 }
 
 }  // namespace nb

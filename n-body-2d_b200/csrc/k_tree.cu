@@ -145,7 +145,7 @@ scan_reduce(const int32_t* __restrict__ in, int n, int32_t* __restrict__ block_s
 }
 
 __global__ void __launch_bounds__(kThreads)
-scan_block_sums(int32_t* __restrict__ block_sums, int blocks, DeviceScalars* __restrict__ s) {
+scan_block_sums(int32_t* __restrict__ block_sums, int blocks, int32_t* __restrict__ total_out) {
     __shared__ int wsum[kThreads / 32];
     __shared__ int total;
     int carry = 0;
@@ -157,7 +157,7 @@ scan_block_sums(int32_t* __restrict__ block_sums, int blocks, DeviceScalars* __r
         carry += total;
         __syncthreads();
     }
-    if (threadIdx.x == 0) s->cells = carry;
+    if (threadIdx.x == 0) *total_out = carry;
 }
 
 __global__ void __launch_bounds__(kThreads)
@@ -348,17 +348,20 @@ __global__ void tree_moments(DeviceScalars* __restrict__ s, const double2* __res
                 const int r = refs[q];
                 if (r == INT_MIN) continue;
                 if (r >= 0) {
-                    const double4 sc = __ldcg(t.s64 + r);
-                    sxx += sc.x;
-                    sxy += sc.y;
-                    syy += sc.z;
+                    const double2* sc = reinterpret_cast<const double2*>(t.s64 + r);
+                    const double2 s01 = __ldcg(sc), s2 = __ldcg(sc + 1);
+                    sxx += s01.x;
+                    sxy += s01.y;
+                    syy += s2.x;
                 }
                 const double dx = cmx[q] - com.x, dy = cmy[q] - com.y;
                 sxx += cm[q] * dx * dx;
                 sxy += cm[q] * dx * dy;
                 syy += cm[q] * dy * dy;
             }
-            __stcg(t.s64 + id, make_double4(sxx, sxy, syy, 0.0));
+            double2* so = reinterpret_cast<double2*>(t.s64 + id);
+            __stcg(so, make_double2(sxx, sxy));
+            __stcg(so + 1, make_double2(syy, 0.0));
             t.cell4[id] = make_float4((float)(com.x - s->center[0]), (float)(com.y - s->center[1]),
                                       (float)M, (float)s->wsq[t.level[id]]);
             t.cellq[id] = make_float4((float)sxx, (float)sxy, (float)syy, 0.f);
@@ -377,11 +380,97 @@ __global__ void tree_moments(DeviceScalars* __restrict__ s, const double2* __res
     }
 }
 
+// ---- SPLIT target groups -----------------------------------------------
+// A cell with more than gsize bodies hands its small children (cells or
+// leaves with <= gsize bodies) to groups: consecutive small children are
+// merged while the sum stays <= gsize, so a group never leaves its parent
+// cell and its bounding box stays within one cell width.  Multi-body leaves
+// larger than a group are cut into chunks of gsize.  kWrite = false
+// counts the groups of each cell, kWrite = true writes them at gbase[cell].
+template <bool kWrite>
+__global__ void tree_groups(int n, int gsize, Tree t, const DeviceScalars* __restrict__ s) {
+    const int id = blockIdx.x * blockDim.x + threadIdx.x;
+    const int cells = s->cells;
+    if (id >= n) return;
+    if (id >= cells) {
+        if (!kWrite) t.gcount[id] = 0;
+        if (cells == 0 && id == 0) {  // no cell: the root leaf holds all bodies
+            const int ng = (n + gsize - 1) / gsize;
+            if (!kWrite) {
+                t.gcount[0] = ng;
+            } else {
+                for (int k = 0; k < ng; ++k)
+                    t.groups[k] = make_int2(k * gsize, min(n, (k + 1) * gsize) - 1);
+            }
+        }
+        return;
+    }
+    const int2 rg = t.range[id];
+    int out = kWrite ? t.gbase[id] : 0;
+    int emitted = 0;
+    auto emit = [&](int a, int b) {
+        if (kWrite) t.groups[out + emitted] = make_int2(a, b);
+        ++emitted;
+    };
+    if (rg.y - rg.x + 1 <= gsize) {
+        if (id == s->root) emit(rg.x, rg.y);  // the whole (small) tree is one group
+    } else {
+        const int4 ch = t.child[id];
+        const int refs[4] = {ch.x, ch.y, ch.z, ch.w};
+        int run_a = -1, run_b = -1;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int r = refs[q];
+            if (r == INT_MIN) break;
+            int a, b;
+            if (r >= 0) {
+                const int2 cr = t.range[r];
+                a = cr.x;
+                b = cr.y;
+            } else {
+                a = ~r;
+                b = t.leaf_last[a];
+            }
+            const int cnt = b - a + 1;
+            if (cnt > gsize) {
+                if (run_a >= 0) emit(run_a, run_b);
+                run_a = -1;
+                if (r < 0)  // oversized multi-body leaf: chunks of one group each
+                    for (int k = a; k <= b; k += gsize) emit(k, min(b, k + gsize - 1));
+                continue;
+            }
+            if (run_a >= 0 && b - run_a + 1 > gsize) {
+                emit(run_a, run_b);
+                run_a = -1;
+            }
+            if (run_a < 0) run_a = a;
+            run_b = b;
+        }
+        if (run_a >= 0) emit(run_a, run_b);
+    }
+    if (!kWrite) t.gcount[id] = emitted;
+}
+
 inline unsigned blocks_for(int64_t n, int threads) {
     return (unsigned)((n + threads - 1) / threads);
 }
 
 }  // namespace
+
+void launch_groups(nb_ctx* c) {
+    const int n = (int)c->n;
+    const int sblocks = (int)blocks_for(n, kScanTile);
+    c->launches += 5;
+    const int gsize = split_group_size(c);
+    tree_groups<false><<<blocks_for(n, kThreads), kThreads, 0, c->stream>>>(n, gsize, c->tree,
+                                                                            c->scal);
+    scan_reduce<<<sblocks, kThreads, 0, c->stream>>>(c->tree.gcount, n, c->scan.block_sums);
+    scan_block_sums<<<1, kThreads, 0, c->stream>>>(c->scan.block_sums, sblocks, &c->scal->groups);
+    scan_apply<<<sblocks, kThreads, 0, c->stream>>>(c->tree.gcount, n, c->scan.block_sums,
+                                                     c->tree.gbase);
+    tree_groups<true><<<blocks_for(n, kThreads), kThreads, 0, c->stream>>>(n, gsize, c->tree,
+                                                                           c->scal);
+}
 
 void launch_tree(nb_ctx* c, const BodyBuffers& b) {
     const int n = (int)c->n;
@@ -391,7 +480,7 @@ void launch_tree(nb_ctx* c, const BodyBuffers& b) {
                                                                     c->tree.start_of);
     const int sblocks = (int)blocks_for(n, kScanTile);
     scan_reduce<<<sblocks, kThreads, 0, c->stream>>>(c->tree.flag, n, c->scan.block_sums);
-    scan_block_sums<<<1, kThreads, 0, c->stream>>>(c->scan.block_sums, sblocks, c->scal);
+    scan_block_sums<<<1, kThreads, 0, c->stream>>>(c->scan.block_sums, sblocks, &c->scal->cells);
     scan_apply<<<sblocks, kThreads, 0, c->stream>>>(c->tree.flag, n, c->scan.block_sums,
                                                      c->tree.cell_of);
     tree_link<<<blocks_for(n, kThreads), kThreads, 0, c->stream>>>(key, n, b.pos, b.mass, c->tree,

@@ -83,6 +83,9 @@ int alloc_all(nb_ctx* c) {
         NB_CUDA(c, dalloc(&t.cell4, n));
         NB_CUDA(c, dalloc(&t.cellq, n));
         NB_CUDA(c, dalloc(&t.body4, n));
+        NB_CUDA(c, dalloc(&t.gcount, n));
+        NB_CUDA(c, dalloc(&t.gbase, n));
+        NB_CUDA(c, dalloc(&t.groups, n));
     }
     NB_CUDA(c, dalloc(&t.leaf_last, n));
     NB_CUDA(c, dalloc(&t.leaf_plevel, n));
@@ -118,7 +121,7 @@ void free_all(nb_ctx* c) {
                          t.nint,      t.ready,       t.mass,        t.com,        t.leaf_last,
                          t.leaf_plevel, t.bucket_mass, t.bucket_com, t.flag,      t.cell_of,
                          t.start_of,  t.range,       t.s64,         t.cell4,      t.cellq,
-                         t.body4};
+                         t.body4,     t.gcount,      t.gbase,       t.groups};
     for (void* q : tree_ptrs) cudaFree(q);
     cudaFree(c->scal);
     cudaFree(c->bbox_partials);
@@ -136,7 +139,7 @@ void drop_graphs(nb_ctx* c) {
 }
 
 const char* const kPhaseNames[nb::kPhases] = {"bbox+morton", "sort", "gather", "tree",
-                                              "moments", "force", "drift"};
+                                              "moments", "groups", "force", "drift"};
 
 // Enqueues one step reading the state from buf[parity]; leaves it in the
 // other buffer.  integrate=false stops after the force pass (no kick/drift).
@@ -163,15 +166,17 @@ void enqueue_step(nb_ctx* c, int parity, bool integrate, bool store_acc, bool ti
     mark(4);
     nb::launch_moments(c, B, split);
     mark(5);
+    if (split) nb::launch_groups(c);
+    mark(6);
     if (split) {
         nb::launch_force_split(c, B, integrate, store_acc);  // kick and drift fused
-        mark(6);
+        mark(7);
     } else {
         nb::launch_force_fp64(c, B, integrate, store_acc);
-        mark(6);
+        mark(7);
         if (integrate) nb::launch_drift(c, B);
     }
-    mark(7);
+    mark(8);
 }
 
 int capture_graph(nb_ctx* c, int parity) {

@@ -17,7 +17,7 @@ constexpr int kStackDepth = 96;   // >= 1 + 3 * 30 pending cells of a DFS
 constexpr int kSortTileItems = 8; // keys per thread in a radix tile
 constexpr int kSortThreads = 256;
 constexpr int kSortTile = kSortTileItems * kSortThreads;  // 2048 keys
-constexpr int kPhases = 7;        // morton, sort, gather, tree, moments, force, drift
+constexpr int kPhases = 8;        // morton, sort, gather, tree, moments, groups, force, drift
 
 // Device error flags (bit mask in DeviceScalars::error).
 constexpr unsigned kErrStack = 1u;      // DFS stack bound exceeded
@@ -31,6 +31,8 @@ struct DeviceScalars {
     double wsq[kMaxLevel + 1];// squared cell width per level (root * 0.25^L)
     int32_t root;             // >= 0 cell id, < 0 leaf ~first_body
     int32_t cells;            // internal cells of the current tree
+    int32_t groups;           // SPLIT: target groups of the current tree
+    unsigned group_ticket;    // SPLIT: next group for the persistent traversal
     unsigned error;           // kErr* bits, sticky until read by the host
     unsigned bbox_ticket;     // last-block-done counter of the bbox reduction
     unsigned long long cell_terms;
@@ -63,6 +65,11 @@ struct Tree {
     float4* cell4 = nullptr;     // {com_x - cx, com_y - cy, mass, width^2}
     float4* cellq = nullptr;     // {Sxx, Sxy, Syy, 0}
     float4* body4 = nullptr;     // per body {x - cx, y - cy, mass, index bits}
+    // SPLIT target groups: <= split_group_size() Morton-consecutive bodies in one
+    // parent cell (merged sibling cells/leaves), stored as body ranges
+    int32_t* gcount = nullptr;   // groups each cell emits
+    int32_t* gbase = nullptr;    // exclusive scan of gcount
+    int2* groups = nullptr;      // {first, last} body of each group
     // per-body side tables, only meaningful at leaf starts
     int32_t* leaf_last = nullptr;   // last body of the leaf starting here
     int32_t* leaf_plevel = nullptr; // level of the leaf's parent cell (-1: root leaf)
@@ -105,6 +112,7 @@ struct nb_ctx {
     nb::DeviceScalars* scal = nullptr;   // device
     double* bbox_partials = nullptr;     // [blocks][4]
     int bbox_blocks = 0;
+    int split_blocks = 0;                // persistent grid of the SPLIT traversal
     double2* acc = nullptr;              // optional FP64 accelerations (sorted order)
     double2* stage_pos = nullptr;        // original-order staging for downloads
     double2* stage_vel = nullptr;
@@ -127,6 +135,8 @@ void launch_sort(nb_ctx* c);                                   // result in key[
 void launch_gather(nb_ctx* c, const BodyBuffers& src, const BodyBuffers& dst, float4* body4);
 void launch_tree(nb_ctx* c, const BodyBuffers& b);
 void launch_moments(nb_ctx* c, const BodyBuffers& b, bool split);
+int split_group_size(const nb_ctx* c);   // bodies per SPLIT traversal group
+void launch_groups(nb_ctx* c);
 void launch_force_split(nb_ctx* c, const BodyBuffers& b, bool kick, bool store_acc);
 void launch_force_fp64(nb_ctx* c, const BodyBuffers& b, bool kick, bool store_acc);
 void launch_drift(nb_ctx* c, const BodyBuffers& b);

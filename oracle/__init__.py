@@ -56,6 +56,10 @@ def load():
         lib.orc_ref_step.restype = C.c_int
         lib.orc_allpairs_plummer.argtypes = [C.c_int64, _P, _P, C.c_int64, _P, C.c_double, _P,
                                              C.c_int]
+        lib.orc_allpairs_plummer_abs.argtypes = [C.c_int64, _P, _P, C.c_int64, _P, C.c_double,
+                                                 _P, C.c_int]
+        lib.orc_allpairs_fp32_bound.argtypes = [C.c_int64, _P, _P, C.c_int64, _P, C.c_double,
+                                                C.c_double, C.c_double, _P, C.c_int]
         lib.orc_allpairs_cpulaw.argtypes = [C.c_int64, _P, _P, C.c_int64, _P, C.c_double,
                                             C.c_double, _P, C.c_int]
         _lib = lib
@@ -144,6 +148,28 @@ def allpairs_plummer(mass, pos, targets=None, eps2=1e-4, nthreads=None) -> np.nd
     load().orc_allpairs_plummer(n, _p(mass), _p(pos), tgt.shape[0], _p(tgt), eps2, _p(acc),
                                 _threads(nthreads))
     return acc
+
+
+def allpairs_plummer_abs(mass, pos, targets=None, eps2=1e-4, nthreads=None) -> np.ndarray:
+    mass = np.ascontiguousarray(mass, dtype=np.float64)
+    pos = np.ascontiguousarray(pos, dtype=np.float64)
+    n = mass.shape[0]
+    tgt = np.ascontiguousarray(np.arange(n) if targets is None else targets, dtype=np.int64)
+    out = np.empty(tgt.shape[0])
+    load().orc_allpairs_plummer_abs(n, _p(mass), _p(pos), tgt.shape[0], _p(tgt), eps2, _p(out),
+                                    _threads(nthreads))
+    return out
+
+
+def allpairs_fp32_bound(mass, pos, center, targets=None, eps2=1e-4, nthreads=None) -> np.ndarray:
+    mass = np.ascontiguousarray(mass, dtype=np.float64)
+    pos = np.ascontiguousarray(pos, dtype=np.float64)
+    n = mass.shape[0]
+    tgt = np.ascontiguousarray(np.arange(n) if targets is None else targets, dtype=np.int64)
+    out = np.empty(tgt.shape[0])
+    load().orc_allpairs_fp32_bound(n, _p(mass), _p(pos), tgt.shape[0], _p(tgt), eps2,
+                                   float(center[0]), float(center[1]), _p(out), _threads(nthreads))
+    return out
 
 
 def allpairs_cpulaw(mass, pos, targets=None, G=1.0, eps2=1e-4, nthreads=None) -> np.ndarray:

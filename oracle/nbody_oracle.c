@@ -478,6 +478,65 @@ void orc_allpairs_plummer(int64_t n, const double* mass, const double* pos, int6
     }
 }
 
+void orc_allpairs_plummer_abs(int64_t n, const double* mass, const double* pos, int64_t k,
+                              const int64_t* tgt, double eps2, double* out, int nthreads) {
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#else
+    (void)nthreads;
+#endif
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int64_t t = 0; t < k; ++t) {
+        const int64_t i = tgt[t];
+        const double bx = pos[2 * i], by = pos[2 * i + 1];
+        double s = 0.0;
+        for (int64_t j = 0; j < n; ++j) {
+            if (j == i) continue;
+            const double dx = pos[2 * j] - bx, dy = pos[2 * j + 1] - by;
+            const double r2 = dx * dx + dy * dy;
+            const double d2 = r2 + eps2;
+            s += mass[j] * sqrt(r2) / (d2 * sqrt(d2));
+        }
+        out[t] = s;
+    }
+}
+
+void orc_allpairs_fp32_bound(int64_t n, const double* mass, const double* pos, int64_t k,
+                             const int64_t* tgt, double eps2, double cx, double cy, double* out,
+                             int nthreads) {
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#else
+    (void)nthreads;
+#endif
+    const double u = 5.9604644775390625e-08; /* 2^-24, FP32 unit roundoff */
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int64_t t = 0; t < k; ++t) {
+        const int64_t i = tgt[t];
+        const double bx = pos[2 * i], by = pos[2 * i + 1];
+        const double ri = fabs(bx - cx) + fabs(by - cy);
+        double s = 0.0, abs_sum = 0.0;
+        for (int64_t j = 0; j < n; ++j) {
+            if (j == i) continue;
+            const double dx = pos[2 * j] - bx, dy = pos[2 * j + 1] - by;
+            const double r2 = dx * dx + dy * dy;
+            const double r = sqrt(r2);
+            const double d2 = r2 + eps2;
+            const double term = mass[j] * r / (d2 * sqrt(d2));
+            const double rj = fabs(pos[2 * j] - cx) + fabs(pos[2 * j + 1] - cy);
+            /* rounding of the two coordinates shifts d by up to u (ri + rj);
+             * the term moves by at most 3 of that relative to r, plus 16 u of
+             * per-term arithmetic */
+            s += term * (16.0 * u + (r > 0.0 ? 3.0 * u * (ri + rj) / r : 0.0));
+            abs_sum += term;
+        }
+        /* accumulation: each addition rounds by at most u |partial sum| <=
+         * u abs_sum; independent roundings grow like sqrt(terms), taken with a
+         * margin of 8 */
+        out[t] = s + 8.0 * sqrt((double)n) * u * abs_sum;
+    }
+}
+
 void orc_allpairs_cpulaw(int64_t n, const double* mass, const double* pos, int64_t k,
                          const int64_t* tgt, double G, double eps2, double* acc, int nthreads) {
 #ifdef _OPENMP

@@ -74,6 +74,19 @@ int orc_ref_step(int64_t n, double* mass, double* pos_xy, double* vel_xy, int32_
 void orc_allpairs_plummer(int64_t n, const double* mass, const double* pos_xy, int64_t k,
                           const int64_t* tgt, double eps2, double* acc_xy, int nthreads);
 
+/* Sum of the magnitudes of the pair terms of orc_allpairs_plummer, per target:
+ * the scale that bounds the rounding error of any order of summation. */
+void orc_allpairs_plummer_abs(int64_t n, const double* mass, const double* pos_xy, int64_t k,
+                              const int64_t* tgt, double eps2, double* out, int nthreads);
+
+/* A per-target bound on the error of an FP32 pair sum whose coordinates are
+ * rounded to FP32 relative to (cx, cy): sum_j |a_ij| (16 u + 3 u (|x_i-c| +
+ * |x_j-c|)_1 / |d_ij|) + 8 sqrt(n) u sum_j |a_ij|, u = 2^-24 (the last term
+ * covers accumulation rounding, taken as a random walk). */
+void orc_allpairs_fp32_bound(int64_t n, const double* mass, const double* pos_xy, int64_t k,
+                             const int64_t* tgt, double eps2, double cx, double cy, double* out,
+                             int nthreads);
+
 /*
  * FP64 all-pairs accelerations with the reference CPU pair law
  * (src/Simulation/src/Simulation.cpp:74-80, BarnesHut.cpp:130-135):

@@ -30,7 +30,12 @@ def test_theta_zero_is_allpairs_in_fp32(nbp, orc, n):
     if n == 1:
         assert np.array_equal(a, np.zeros((1, 2)))
         return
-    assert rel_err(a, exact).max() < 2e-4
+    # FP32: coordinates are rounded relative to the box centre, so the bound
+    # grows with |x - centre| / |d| for close pairs
+    box = orc.bbox_squared(p)
+    center = (0.5 * (box[0] + box[1]), 0.5 * (box[2] + box[3]))
+    bound = orc.allpairs_fp32_bound(m, p, center, eps2=EPS2)
+    assert (np.linalg.norm(a - exact, axis=1) <= bound).all()
 
 
 def test_monopole_error_not_worse_than_reference_walk(nbp):
@@ -81,4 +86,7 @@ def test_split_coincident_and_ragged(nbp, orc):
     m = rng.random(n) + 0.5
     a, _ = accel(nbp, m, p, np.zeros((n, 2)), nbp.NB_MODE_SPLIT, 0.0, leaf=1)
     exact = orc.allpairs_plummer(m, p, eps2=EPS2)
-    assert rel_err(a, exact).max() < 2e-4
+    box = orc.bbox_squared(p)
+    center = (0.5 * (box[0] + box[1]), 0.5 * (box[2] + box[3]))
+    bound = orc.allpairs_fp32_bound(m, p, center, eps2=EPS2)
+    assert (np.linalg.norm(a - exact, axis=1) <= bound).all()
