@@ -162,6 +162,34 @@ NB_API int nb_allpairs_accelerations(int32_t device, uint64_t n, const double* m
                               const double* pos_xy, uint64_t k, const int64_t* targets,
                               double epsilon_squared, double* acc_xy);
 
+/* Largest n nb_morton_sort_static accepts (its scratch is sized for it). */
+#define NB_STATIC_SORT_MAX_BODIES 262144
+
+/* The sort stage without any allocation.  No counterpart in the reference:
+ * for callers that cannot let a library allocate device memory -- a renderer
+ * stepping once per frame cannot take the device-wide synchronisation that
+ * cudaMalloc/cudaFree may cause, and host programs that own all device memory
+ * through their own pool hand libraries buffers instead.
+ *
+ * Computes, on the current device and on `stream` (a cudaStream_t; NULL is
+ * the legacy default stream), what nb_debug_morton computes: the squared root
+ * box, the 64-bit Morton codes sorted stably, and the permutation.  All
+ * pointers are DEVICE pointers owned by the caller: pos_xy holds n
+ * interleaved {x, y} doubles; codes receives n uint64, order n int32
+ * (order[r] = input index of the body ranked r); box (nullable) receives
+ * {x_min, x_max, y_min, y_max}.  Returns once the work is enqueued.
+ *
+ * Calls no cudaMalloc/cudaFree: the scratch is a static device array in the
+ * library (NB_STATIC_SORT_MAX_BODIES x 24 bytes + about 20 KB on every GPU
+ * that loads it, held until exit).  n above NB_STATIC_SORT_MAX_BODIES is
+ * rejected with NB_ERR_CAPACITY, n == 0 or a NULL pointer with
+ * NB_ERR_INVALID.  The first call on a device looks up the array's device
+ * address, so make it before any stream capture.  All calls on a device share
+ * the scratch: calls that overlap on the GPU race and must be serialised by
+ * the caller. */
+NB_API int nb_morton_sort_static(const double* pos_xy, uint64_t n, uint64_t* codes,
+                                 int32_t* order, double* box, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -24,13 +24,14 @@ NB_ERR_NOTFOUND = 6
 NB_MODE_FP64 = 0
 NB_MODE_SPLIT = 1
 NB_FLAG_QUADRUPOLE = 1
+NB_STATIC_SORT_MAX_BODIES = 262144  # include/nbody_b200.h
 
 # Every symbol include/nbody_b200.h declares.
 EXPORTS = (
     "nb_params_default", "nb_create", "nb_destroy", "nb_step", "nb_sync", "nb_set_timestep",
     "nb_upload", "nb_download", "nb_accelerations", "nb_debug_morton", "nb_debug_state",
     "nb_debug_tree", "nb_get_stats", "nb_last_error", "nb_status_string",
-    "nb_allpairs_accelerations", "nb_phase_times", "nb_phase_name",
+    "nb_allpairs_accelerations", "nb_phase_times", "nb_phase_name", "nb_morton_sort_static",
 )
 
 
@@ -97,6 +98,7 @@ def load() -> C.CDLL:
     lib.nb_last_error.restype = C.c_char_p
     lib.nb_status_string.argtypes = [C.c_int]
     lib.nb_status_string.restype = C.c_char_p
+    lib.nb_morton_sort_static.argtypes = [_P, C.c_uint64, _P, _P, _P, _P]
     lib.nb_phase_times.argtypes = [_P, _P, C.c_int]
     lib.nb_phase_name.argtypes = [C.c_int]
     lib.nb_phase_name.restype = C.c_char_p

@@ -350,6 +350,25 @@ void launch_sort(nb_ctx* c) {
     }
 }
 
+void launch_morton_sort_raw(const double2* pos, int64_t n, uint64_t* const key[2],
+                            uint32_t* const val[2], uint64_t* key_out, uint32_t* val_out,
+                            uint32_t* counts, uint32_t* totals, double* partials, int bbox_blocks,
+                            DeviceScalars* scal, cudaStream_t st) {
+    const int tiles = (int)((n + kSortTile - 1) / kSortTile);
+    bbox_kernel<<<bbox_blocks, kBoxThreads, 0, st>>>(pos, n, partials, scal);
+    morton_kernel<<<blocks_for(n, 256), 256, 0, st>>>(pos, n, scal, key[0], val[0]);
+    for (int pass = 0; pass < 8; ++pass) {
+        const int src = pass & 1, dst = src ^ 1;
+        const int shift = 8 * pass;
+        uint64_t* kd = pass == 7 ? key_out : key[dst];
+        uint32_t* vd = pass == 7 ? val_out : val[dst];
+        sort_upsweep<<<tiles, kSortThreads, 0, st>>>(key[src], n, shift, counts, tiles);
+        sort_scan_rows<<<256, kSortThreads, 0, st>>>(counts, tiles, totals);
+        sort_downsweep<<<tiles, kSortThreads, 0, st>>>(key[src], val[src], kd, vd, n, shift, counts,
+                                                       totals, tiles);
+    }
+}
+
 void launch_gather(nb_ctx* c, const BodyBuffers& src, const BodyBuffers& dst, float4* body4) {
     c->launches += 1;
     gather_kernel<<<blocks_for(c->n, 256), 256, 0, c->stream>>>(c->sort.val[0], c->n, src, dst,

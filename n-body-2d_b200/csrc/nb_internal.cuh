@@ -144,4 +144,13 @@ void launch_scatter(nb_ctx* c, const BodyBuffers& b, double2* out_pos, double2* 
                     const double2* acc, double2* out_acc);
 void launch_identity(nb_ctx* c, int32_t* orig);
 
+// The bounding-box, Morton and radix-sort stage on caller-provided buffers
+// (no context): key/val ping-pong scratch of n entries each, counts of
+// 256 x ceil(n / kSortTile), totals of 256, partials of 4 x bbox_blocks.  The
+// last pass writes the sorted codes and permutation to key_out / val_out.
+void launch_morton_sort_raw(const double2* pos, int64_t n, uint64_t* const key[2],
+                            uint32_t* const val[2], uint64_t* key_out, uint32_t* val_out,
+                            uint32_t* counts, uint32_t* totals, double* partials, int bbox_blocks,
+                            DeviceScalars* scal, cudaStream_t st);
+
 }  // namespace nb
