@@ -32,7 +32,7 @@ constexpr int kStk = 256;              // stack bound kept by the batch size rul
 constexpr int kStkAlloc = kStk + 96;   // + one depth-first descent (<= 3 x 30 + 1)
 constexpr int kList = 64;
 constexpr int kBodiesPerLane = 2;      // group of 64 bodies per warp
-constexpr int kDefaultLeaf = 16;       // cells this small are summed body by body
+constexpr int kDefaultLeaf = 8;        // cells this small are summed body by body
 
 struct WarpLists {
     int stack[kStkAlloc];
