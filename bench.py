@@ -63,28 +63,41 @@ def _peaks() -> tuple[dict, str]:
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """nvidia-smi clocks and throttle reasons, sampled every 20 ms from before
+    the timed region to after it; samples are kept when their timestamp falls
+    inside the region widened by one interval (a region of a few tens of ms
+    would otherwise see none)."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    FIELDS = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    INTERVAL_MS = 20
 
     def __init__(self, device: int):
         self.device = device
         self.proc = None
+        self.t0 = self.t1 = None
+        self.lines: list[str] = []
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200", "-i", str(self.device)],
+                 "-lms", str(self.INTERVAL_MS), "-i", str(self.device)],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            time.sleep(0.5)  # let the sampler start before the region opens
         except OSError:
             self.proc = None
         return self
 
+    def mark_start(self):
+        self.t0 = time.time()
+
+    def mark_end(self):
+        self.t1 = time.time()
+        time.sleep(2.5 * self.INTERVAL_MS / 1000.0)
+
     def __exit__(self, *exc):
-        self.lines = []
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -95,24 +108,40 @@ class ClockSampler:
             self.lines = [ln for ln in out.splitlines() if ln.strip()]
 
     def summary(self) -> dict:
+        import datetime
+
+        def stamp(text):
+            for fmt in ("%Y/%m/%d %H:%M:%S.%f", "%Y/%m/%d %H:%M:%S", "%Y-%m-%d %H:%M:%S.%f"):
+                try:
+                    return datetime.datetime.strptime(text, fmt).timestamp()
+                except ValueError:
+                    pass
+            return None
+
         sm, smax, reasons = [], [], set()
         names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
-        for ln in getattr(self, "lines", []):
-            parts = [x.strip() for x in ln.split(",")]
-            if len(parts) < 9:
-                continue
+        pad = self.INTERVAL_MS / 1000.0
+        parsed = [[x.strip() for x in ln.split(",")] for ln in self.lines]
+        parsed = [p for p in parsed if len(p) >= 10]
+        stamps = [stamp(p[0]) for p in parsed]
+        windowed = self.t0 is not None and any(t is not None for t in stamps)
+        for parts, ts in zip(parsed, stamps):
             try:
-                sm.append(float(parts[1]))
-                smax.append(float(parts[2]))
+                clk, clk_max = float(parts[2]), float(parts[3])
             except ValueError:
                 continue
-            for name, val in zip(names, parts[5:9]):
+            if windowed and (ts is None or not (self.t0 - pad <= ts <= self.t1 + pad)):
+                continue
+            sm.append(clk)
+            smax.append(clk_max)
+            for name, val in zip(names, parts[6:10]):
                 if val.lower() == "active":
                     reasons.add(name)
         if not sm:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax),
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm),
+                "interval_ms": self.INTERVAL_MS, "windowed": windowed}
 
 
 def _dist():
@@ -237,8 +266,10 @@ def run_ours(args) -> None:
 
     barrier()
     with ClockSampler(local) as clocks:
+        clocks.mark_start()
         ctx.step(args.steps, sync=False)
         ctx.sync()
+        clocks.mark_end()
     barrier()
     st = ctx.stats()
     ms = st.ms_last_step
