@@ -299,6 +299,168 @@ sort_downsweep(const uint64_t* __restrict__ key_in, const uint32_t* __restrict__
     }
 }
 
+// ---------------------------------------------------------------------------
+// Onesweep LSD radix sort (the step's sort).  One pass over the keys builds
+// the histograms of all eight digits; each digit pass is then a single kernel
+// whose tiles learn their global offsets by decoupled look-back: a tile
+// publishes its per-digit count, then sums its predecessors' counts until it
+// meets one that already holds an inclusive prefix.  Tiles take their index
+// from an atomic counter in the order they start, so a tile only ever waits
+// on tiles that are already running.  Every wait is bounded; a wait that runs
+// out sets kErrTimeout and the step reports NB_ERR_TIMEOUT.
+// ---------------------------------------------------------------------------
+constexpr uint32_t kFlagAgg = 1u << 30;
+constexpr uint32_t kFlagPrefix = 2u << 30;
+constexpr uint32_t kCountMask = (1u << 30) - 1;
+constexpr int kSpinLimit = 1 << 22;
+
+__global__ void __launch_bounds__(kSortThreads)
+onesweep_histogram(const uint64_t* __restrict__ key, int64_t n, uint32_t* __restrict__ hist) {
+    __shared__ uint32_t h[8][256];
+    for (int k = threadIdx.x; k < 8 * 256; k += kSortThreads) (&h[0][0])[k] = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    // the loop test uses the warp's first index so the whole warp iterates
+    // together (__match_any_sync needs every lane)
+    for (int64_t i = blockIdx.x * (int64_t)kSortThreads + threadIdx.x; i - lane < n;
+         i += (int64_t)gridDim.x * kSortThreads) {
+        const bool valid = i < n;
+        const uint64_t k = valid ? __ldg(key + i) : 0ull;
+#pragma unroll
+        for (int d = 0; d < 8; ++d) {
+            const uint32_t dig = valid ? (uint32_t)((k >> (8 * d)) & 0xFF) : 0x100u + lane;
+            const unsigned peers = __match_any_sync(kFull, dig);
+            if (valid && lane == __ffs(peers) - 1) atomicAdd(&h[d][dig], (uint32_t)__popc(peers));
+        }
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < 8 * 256; k += kSortThreads) {
+        const uint32_t v = (&h[0][0])[k];
+        if (v) atomicAdd(hist + k, v);
+    }
+}
+
+// Exclusive scan of each digit position's 256 bins (block d = position d).
+__global__ void __launch_bounds__(kSortThreads)
+onesweep_bins(uint32_t* __restrict__ hist) {
+    __shared__ uint32_t warp_tot[kWarps];
+    uint32_t* row = hist + 256 * blockIdx.x;
+    const uint32_t v = row[threadIdx.x];
+    const uint32_t ex = block_exclusive_scan(v, warp_tot, nullptr);
+    row[threadIdx.x] = ex;
+}
+
+__device__ __forceinline__ uint32_t ld_status(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_status(uint32_t* p, uint32_t v) {
+    asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__global__ void __launch_bounds__(kSortThreads)
+onesweep_pass(const uint64_t* __restrict__ key_in, const uint32_t* __restrict__ val_in,
+              uint64_t* __restrict__ key_out, uint32_t* __restrict__ val_out, int64_t n, int shift,
+              const uint32_t* __restrict__ bins, uint32_t* __restrict__ status,
+              unsigned* __restrict__ tile_counter, unsigned* __restrict__ err) {
+    __shared__ uint32_t whist[kWarps][256];
+    __shared__ uint32_t tile_start[256];
+    __shared__ uint32_t goff[256];
+    __shared__ uint32_t warp_tot[kWarps];
+    __shared__ uint64_t skey[kSortTile];
+    __shared__ uint32_t sval[kSortTile];
+    __shared__ int tile_sh;
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) tile_sh = (int)atomicAdd(tile_counter, 1u);
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) whist[w][tid] = 0;
+    __syncthreads();
+    const int tile = tile_sh;
+    const int64_t base = (int64_t)tile * kSortTile;
+    const int64_t seg = base + warp * (32 * kSortTileItems);
+    uint64_t k_reg[kSortTileItems];
+    uint32_t v_reg[kSortTileItems];
+    uint32_t r_reg[kSortTileItems];
+    const unsigned below = lanemask_lt();
+#pragma unroll
+    for (int k = 0; k < kSortTileItems; ++k) {
+        const int64_t i = seg + k * 32 + lane;
+        const bool valid = i < n;
+        k_reg[k] = valid ? key_in[i] : 0ull;
+        v_reg[k] = valid ? val_in[i] : 0u;
+        const uint32_t d = valid ? (uint32_t)((k_reg[k] >> shift) & 0xFF) : 0x100u + lane;
+        const unsigned peers = __match_any_sync(kFull, d);
+        const int leader = __ffs(peers) - 1;
+        uint32_t b = 0;
+        if (valid && lane == leader) {
+            b = whist[warp][d];
+            whist[warp][d] = b + __popc(peers);
+        }
+        b = __shfl_sync(kFull, b, leader);
+        r_reg[k] = b + __popc(peers & below);
+        __syncwarp();
+    }
+    __syncthreads();
+    uint32_t count;
+    {
+        uint32_t run = 0;
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) {
+            const uint32_t c = whist[w][tid];
+            whist[w][tid] = run;
+            run += c;
+        }
+        count = run;
+        tile_start[tid] = block_exclusive_scan(run, warp_tot, nullptr);
+    }
+    // look-back for digit tid
+    uint32_t* st = status + (int64_t)tile * 256 + tid;
+    uint32_t excl = 0;
+    if (tile == 0) {
+        st_status(st, kFlagPrefix | count);
+    } else {
+        st_status(st, kFlagAgg | count);
+        for (int j = tile - 1; j >= 0; --j) {
+            const uint32_t* pj = status + (int64_t)j * 256 + tid;
+            uint32_t v = ld_status(pj);
+            int spins = 0;
+            while ((v & ~kCountMask) == 0) {
+                if (++spins > kSpinLimit) {
+                    atomicOr(err, kErrTimeout);
+                    break;
+                }
+                v = ld_status(pj);
+            }
+            excl += v & kCountMask;
+            if ((v & ~kCountMask) == kFlagPrefix) break;
+        }
+        st_status(st, kFlagPrefix | (excl + count));
+    }
+    goff[tid] = bins[tid] + excl;
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < kSortTileItems; ++k) {
+        const int64_t i = seg + k * 32 + lane;
+        if (i < n) {
+            const uint32_t d = (uint32_t)((k_reg[k] >> shift) & 0xFF);
+            const uint32_t lp = tile_start[d] + whist[warp][d] + r_reg[k];
+            skey[lp] = k_reg[k];
+            sval[lp] = v_reg[k];
+        }
+    }
+    __syncthreads();
+    const int tile_n = (int)min((int64_t)kSortTile, n - base);
+    for (int p = tid; p < tile_n; p += kSortThreads) {
+        const uint64_t kk = skey[p];
+        const uint32_t d = (uint32_t)((kk >> shift) & 0xFF);
+        const uint32_t gp = goff[d] + (uint32_t)p - tile_start[d];
+        key_out[gp] = kk;
+        val_out[gp] = sval[p];
+    }
+}
+
 // CU:135-147: gather the bodies into Morton order.  In SPLIT mode it also
 // writes the FP32 source record of each body relative to the box centre.
 __global__ void gather_kernel(const uint32_t* __restrict__ order, int64_t n, BodyBuffers src,
@@ -337,16 +499,20 @@ void launch_morton(nb_ctx* c, const double2* pos) {
 
 void launch_sort(nb_ctx* c) {
     const int tiles = c->sort.tiles;
-    c->launches += 3 * 8;
+    c->launches += 2 + 8;
+    // histograms, per-pass status words and tile counters start at zero
+    cudaMemsetAsync(c->sort.hist, 0, sizeof(uint32_t) * 8 * 256, c->stream);
+    cudaMemsetAsync(c->sort.status, 0, sizeof(uint32_t) * 8 * 256 * (size_t)tiles, c->stream);
+    cudaMemsetAsync(c->sort.tile_counter, 0, sizeof(unsigned) * 8, c->stream);
+    onesweep_histogram<<<2 * c->sm_count, kSortThreads, 0, c->stream>>>(c->sort.key[0], c->n,
+                                                                        c->sort.hist);
+    onesweep_bins<<<8, kSortThreads, 0, c->stream>>>(c->sort.hist);
     for (int pass = 0; pass < 8; ++pass) {
         const int src = pass & 1, dst = src ^ 1;
-        const int shift = 8 * pass;
-        sort_upsweep<<<tiles, kSortThreads, 0, c->stream>>>(c->sort.key[src], c->n, shift,
-                                                             c->sort.counts, tiles);
-        sort_scan_rows<<<256, kSortThreads, 0, c->stream>>>(c->sort.counts, tiles, c->sort.totals);
-        sort_downsweep<<<tiles, kSortThreads, 0, c->stream>>>(
-            c->sort.key[src], c->sort.val[src], c->sort.key[dst], c->sort.val[dst], c->n, shift,
-            c->sort.counts, c->sort.totals, tiles);
+        onesweep_pass<<<tiles, kSortThreads, 0, c->stream>>>(
+            c->sort.key[src], c->sort.val[src], c->sort.key[dst], c->sort.val[dst], c->n, 8 * pass,
+            c->sort.hist + 256 * pass, c->sort.status + (size_t)pass * 256 * tiles,
+            c->sort.tile_counter + pass, &c->scal->error);
     }
 }
 

@@ -162,7 +162,7 @@ scan_block_sums(int32_t* __restrict__ block_sums, int blocks, int32_t* __restric
 
 __global__ void __launch_bounds__(kThreads)
 scan_apply(const int32_t* __restrict__ in, int n, const int32_t* __restrict__ block_sums,
-           int32_t* __restrict__ out) {
+           int32_t* __restrict__ out, int32_t* __restrict__ index_of) {
     __shared__ int wsum[kThreads / 32];
     __shared__ int total;
     // Items of a thread are consecutive so one block scan covers the tile.
@@ -177,7 +177,11 @@ scan_apply(const int32_t* __restrict__ in, int n, const int32_t* __restrict__ bl
     int run = block_exclusive(sum, wsum, &total) + block_sums[blockIdx.x];
 #pragma unroll
     for (int k = 0; k < kScanItems; ++k) {
-        if (base + k < n) out[base + k] = run;
+        if (base + k < n) {
+            out[base + k] = run;
+            // with 0/1 inputs, index_of lists the flagged positions in order
+            if (index_of && v[k]) index_of[run] = base + k;
+        }
         run += v[k];
     }
 }
@@ -220,9 +224,10 @@ __device__ void bucket_moments(const double2* __restrict__ pos, const double* __
 __global__ void tree_link(const uint64_t* __restrict__ key, int n,
                           const double2* __restrict__ pos, const double* __restrict__ mass,
                           Tree t, DeviceScalars* __restrict__ s) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n - 1 || !t.flag[i]) return;
-    const int id = t.cell_of[i];
+    // one thread per cell, so every lane of a warp builds a cell
+    const int id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= s->cells) return;
+    const int i = t.rep_of[id];
     const int c = lcp_digits(key[i], key[i + 1]);
     const int first = t.start_of[i];
     const int last = c == 0 ? n - 1 : gallop_right(key, i + 1, n - 1, c);
@@ -286,14 +291,81 @@ __global__ void tree_trivial_root(const double2* __restrict__ pos, const double*
     if (n > 1) bucket_moments(pos, mass, 0, n - 1, t.bucket_mass, t.bucket_com);
 }
 
-// Bottom-up FP64 moments.  Threads start at cells without internal children
-// and climb; the last child to arrive at a parent (atomic counter) computes
-// it.  Sums run over the children in quadrant order with the reference's
-// arithmetic (CU:329-343): M += m; R = fma(m, com, R); com = R / M.
+// Moments of one cell from its children, in quadrant order, with the
+// reference's arithmetic (CU:329-343): M += m; R = fma(m, com, R); com = R / M.
 // kSplit also accumulates second moments about the COM by the parallel-axis
 // rule, S = sum_c [S_c + m_c d_c d_c^T] with d_c = com_c - com, in FP64, and
 // packs the FP32 records the group traversal reads.  Leaves have S = 0 (a
 // multi-body leaf spans less than width / 2^30, so its own S is negligible).
+// Children are read with L2-coherent loads: they were written by other
+// threads of this launch (climb) or of an earlier launch (per level).
+template <bool kSplit>
+__device__ __forceinline__ void cell_moments(int id, const DeviceScalars* __restrict__ s,
+                                             const double2* __restrict__ pos,
+                                             const double* __restrict__ mass, const Tree& t) {
+    const int4 ch = t.child[id];
+    const int refs[4] = {ch.x, ch.y, ch.z, ch.w};
+    double cm[4], cmx[4], cmy[4];
+    double M = 0.0, Rx = 0.0, Ry = 0.0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int r = refs[q];
+        cm[q] = 0.0;
+        cmx[q] = 0.0;
+        cmy[q] = 0.0;
+        if (r == INT_MIN) continue;
+        double2 cc;
+        if (r >= 0) {
+            cm[q] = __ldcg(t.mass + r);
+            cc = __ldcg(t.com + r);
+        } else {
+            const int b = ~r;
+            if (t.leaf_last[b] == b) {
+                cm[q] = mass[b];
+                cc = pos[b];
+            } else {
+                cm[q] = t.bucket_mass[b];
+                cc = t.bucket_com[b];
+            }
+        }
+        cmx[q] = cc.x;
+        cmy[q] = cc.y;
+        M += cm[q];
+        Rx = fma(cm[q], cc.x, Rx);
+        Ry = fma(cm[q], cc.y, Ry);
+    }
+    const double2 com = make_double2(Rx / M, Ry / M);
+    __stcg(t.mass + id, M);
+    __stcg(t.com + id, com);
+    if (kSplit) {
+        double sxx = 0.0, sxy = 0.0, syy = 0.0;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int r = refs[q];
+            if (r == INT_MIN) continue;
+            if (r >= 0) {
+                const double2* sc = reinterpret_cast<const double2*>(t.s64 + r);
+                const double2 s01 = __ldcg(sc), s2 = __ldcg(sc + 1);
+                sxx += s01.x;
+                sxy += s01.y;
+                syy += s2.x;
+            }
+            const double dx = cmx[q] - com.x, dy = cmy[q] - com.y;
+            sxx += cm[q] * dx * dx;
+            sxy += cm[q] * dx * dy;
+            syy += cm[q] * dy * dy;
+        }
+        double2* so = reinterpret_cast<double2*>(t.s64 + id);
+        __stcg(so, make_double2(sxx, sxy));
+        __stcg(so + 1, make_double2(syy, 0.0));
+        t.cell4[id] = make_float4((float)(com.x - s->center[0]), (float)(com.y - s->center[1]),
+                                  (float)M, (float)s->wsq[t.level[id]]);
+        t.cellq[id] = make_float4((float)sxx, (float)sxy, (float)syy, 0.f);
+    }
+}
+
+// Bottom-up pass: threads start at cells without internal children and
+// climb; the last child to arrive at a parent (atomic counter) computes it.
 template <bool kSplit>
 __global__ void tree_moments(DeviceScalars* __restrict__ s, const double2* __restrict__ pos,
                              const double* __restrict__ mass, Tree t) {
@@ -307,65 +379,7 @@ __global__ void tree_moments(DeviceScalars* __restrict__ s, const double2* __res
             atomicOr(&s->error, kErrTree);
             return;
         }
-        const int4 ch = t.child[id];
-        const int refs[4] = {ch.x, ch.y, ch.z, ch.w};
-        double cm[4], cmx[4], cmy[4];
-        double M = 0.0, Rx = 0.0, Ry = 0.0;
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int r = refs[q];
-            cm[q] = 0.0;
-            cmx[q] = 0.0;
-            cmy[q] = 0.0;
-            if (r == INT_MIN) continue;
-            double2 cc;
-            if (r >= 0) {
-                cm[q] = __ldcg(t.mass + r);
-                cc = __ldcg(t.com + r);
-            } else {
-                const int b = ~r;
-                if (t.leaf_last[b] == b) {
-                    cm[q] = mass[b];
-                    cc = pos[b];
-                } else {
-                    cm[q] = t.bucket_mass[b];
-                    cc = t.bucket_com[b];
-                }
-            }
-            cmx[q] = cc.x;
-            cmy[q] = cc.y;
-            M += cm[q];
-            Rx = fma(cm[q], cc.x, Rx);
-            Ry = fma(cm[q], cc.y, Ry);
-        }
-        const double2 com = make_double2(Rx / M, Ry / M);
-        __stcg(t.mass + id, M);
-        __stcg(t.com + id, com);
-        if (kSplit) {
-            double sxx = 0.0, sxy = 0.0, syy = 0.0;
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const int r = refs[q];
-                if (r == INT_MIN) continue;
-                if (r >= 0) {
-                    const double2* sc = reinterpret_cast<const double2*>(t.s64 + r);
-                    const double2 s01 = __ldcg(sc), s2 = __ldcg(sc + 1);
-                    sxx += s01.x;
-                    sxy += s01.y;
-                    syy += s2.x;
-                }
-                const double dx = cmx[q] - com.x, dy = cmy[q] - com.y;
-                sxx += cm[q] * dx * dx;
-                sxy += cm[q] * dx * dy;
-                syy += cm[q] * dy * dy;
-            }
-            double2* so = reinterpret_cast<double2*>(t.s64 + id);
-            __stcg(so, make_double2(sxx, sxy));
-            __stcg(so + 1, make_double2(syy, 0.0));
-            t.cell4[id] = make_float4((float)(com.x - s->center[0]), (float)(com.y - s->center[1]),
-                                      (float)M, (float)s->wsq[t.level[id]]);
-            t.cellq[id] = make_float4((float)sxx, (float)sxy, (float)syy, 0.f);
-        }
+        cell_moments<kSplit>(id, s, pos, mass, t);
         __threadfence();
         const int par = t.parent[id];
         if (par < 0) return;
@@ -467,7 +481,7 @@ void launch_groups(nb_ctx* c) {
     scan_reduce<<<sblocks, kThreads, 0, c->stream>>>(c->tree.gcount, n, c->scan.block_sums);
     scan_block_sums<<<1, kThreads, 0, c->stream>>>(c->scan.block_sums, sblocks, &c->scal->groups);
     scan_apply<<<sblocks, kThreads, 0, c->stream>>>(c->tree.gcount, n, c->scan.block_sums,
-                                                     c->tree.gbase);
+                                                     c->tree.gbase, nullptr);
     tree_groups<true><<<blocks_for(n, kThreads), kThreads, 0, c->stream>>>(n, gsize, c->tree,
                                                                            c->scal);
 }
@@ -482,7 +496,7 @@ void launch_tree(nb_ctx* c, const BodyBuffers& b) {
     scan_reduce<<<sblocks, kThreads, 0, c->stream>>>(c->tree.flag, n, c->scan.block_sums);
     scan_block_sums<<<1, kThreads, 0, c->stream>>>(c->scan.block_sums, sblocks, &c->scal->cells);
     scan_apply<<<sblocks, kThreads, 0, c->stream>>>(c->tree.flag, n, c->scan.block_sums,
-                                                     c->tree.cell_of);
+                                                     c->tree.cell_of, c->tree.rep_of);
     tree_link<<<blocks_for(n, kThreads), kThreads, 0, c->stream>>>(key, n, b.pos, b.mass, c->tree,
                                                                     c->scal);
     tree_trivial_root<<<1, 1, 0, c->stream>>>(b.pos, b.mass, n, c->tree, c->scal);

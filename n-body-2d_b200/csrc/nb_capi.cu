@@ -65,6 +65,9 @@ int alloc_all(nb_ctx* c) {
     c->sort.tiles = (int)((n + nb::kSortTile - 1) / nb::kSortTile);
     NB_CUDA(c, dalloc(&c->sort.counts, (size_t)256 * c->sort.tiles));
     NB_CUDA(c, dalloc(&c->sort.totals, 256));
+    NB_CUDA(c, dalloc(&c->sort.hist, 8 * 256));
+    NB_CUDA(c, dalloc(&c->sort.status, (size_t)8 * 256 * c->sort.tiles));
+    NB_CUDA(c, dalloc(&c->sort.tile_counter, 8));
     c->scan.blocks = (int)((n + 2047) / 2048);
     NB_CUDA(c, dalloc(&c->scan.block_sums, (size_t)c->scan.blocks));
     nb::Tree& t = c->tree;
@@ -93,6 +96,7 @@ int alloc_all(nb_ctx* c) {
     NB_CUDA(c, dalloc(&t.bucket_com, n));
     NB_CUDA(c, dalloc(&t.flag, n));
     NB_CUDA(c, dalloc(&t.cell_of, n));
+    NB_CUDA(c, dalloc(&t.rep_of, n));
     NB_CUDA(c, dalloc(&t.start_of, n));
     NB_CUDA(c, dalloc(&c->scal, 1));
     NB_CUDA(c, cudaMemset(c->scal, 0, sizeof(nb::DeviceScalars)));
@@ -115,13 +119,16 @@ void free_all(nb_ctx* c) {
     }
     cudaFree(c->sort.counts);
     cudaFree(c->sort.totals);
+    cudaFree(c->sort.hist);
+    cudaFree(c->sort.status);
+    cudaFree(c->sort.tile_counter);
     cudaFree(c->scan.block_sums);
     nb::Tree& t = c->tree;
     void* tree_ptrs[] = {t.first,     t.last,        t.level,       t.child,      t.parent,
                          t.nint,      t.ready,       t.mass,        t.com,        t.leaf_last,
                          t.leaf_plevel, t.bucket_mass, t.bucket_com, t.flag,      t.cell_of,
                          t.start_of,  t.range,       t.s64,         t.cell4,      t.cellq,
-                         t.body4,     t.gcount,      t.gbase,       t.groups};
+                         t.body4,     t.gcount,      t.gbase,       t.groups,     t.rep_of};
     for (void* q : tree_ptrs) cudaFree(q);
     cudaFree(c->scal);
     cudaFree(c->bbox_partials);

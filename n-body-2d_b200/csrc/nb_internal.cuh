@@ -78,6 +78,7 @@ struct Tree {
     // build scratch (per boundary i between bodies i and i+1)
     int32_t* flag = nullptr;
     int32_t* cell_of = nullptr;     // exclusive scan of flag
+    int32_t* rep_of = nullptr;      // cell id -> the boundary that creates it
     int32_t* start_of = nullptr;    // first body of the cell owning boundary i
 };
 
@@ -86,6 +87,9 @@ struct SortBuffers {
     uint32_t* val[2] = {nullptr, nullptr};
     uint32_t* counts = nullptr;   // [256][tiles]
     uint32_t* totals = nullptr;   // [256]
+    uint32_t* hist = nullptr;     // [8][256] digit histograms -> exclusive bin offsets
+    uint32_t* status = nullptr;   // [8][tiles][256] look-back status words
+    unsigned* tile_counter = nullptr;  // [8]
     int tiles = 0;
 };
 
