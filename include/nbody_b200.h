@@ -56,6 +56,12 @@ extern "C" {
 
 /* nb_params.flags bits */
 #define NB_FLAG_QUADRUPOLE 1u  /* SPLIT: add the cells' second-moment term */
+#define NB_FLAG_LEARNED 2u     /* SPLIT: learned far-field correction (set weights first) */
+
+/* Learned correction: parameters of the 12 -> 64 -> 64 -> 2 MLP as one FP32
+ * vector: W1[64][12], b1[64], W2[64][64], b2[64], W3[2][64], b3[2], then the
+ * output scale (residuals are predicted in units of that scale). */
+#define NB_MLP_PARAMS 5123
 
 typedef struct nb_params {
     double G;               /* gravitational constant (Constants::Simulation::G)    */
@@ -161,6 +167,51 @@ NB_API const char* nb_status_string(int status);
 NB_API int nb_allpairs_accelerations(int32_t device, uint64_t n, const double* mass,
                               const double* pos_xy, uint64_t k, const int64_t* targets,
                               double epsilon_squared, double* acc_xy);
+
+/* ---- learned far-field correction (no counterpart in the reference: the
+ * reference's force pass is the plain monopole walk, BarnesHutCuda.cu:382-486).
+ * A context created with NB_MODE_SPLIT | NB_FLAG_LEARNED accepts cells at
+ * theta; for each cell that plain theta = 0.5 would have opened, a small MLP
+ * predicts the residual between the cell's exact pull and its monopole. */
+
+typedef struct nb_mlp_train_params {
+    uint32_t epochs;      /* passes over the samples                           */
+    uint32_t batch;       /* samples per Adam step                             */
+    float lr;             /* Adam learning rate                                */
+    uint64_t seed;        /* shuffling and (when params is zero) initialisation */
+} nb_mlp_train_params;
+
+/* Installs the MLP parameters (NB_MLP_PARAMS floats) into a learned context. */
+NB_API int nb_set_mlp_weights(nb_ctx* ctx, const float* params);
+
+/* Residual samples from the context's current bodies: for ntargets random
+ * bodies, every cell accepted at the context's theta but opened at 0.5 gives
+ * features[12] and the exact-minus-monopole residual[2] (units of M / d^2,
+ * summed over the cell's bodies in FP64).  Features: (p - c)/d (2), w/d,
+ * heaviest child's mass fraction, S/(M w^2) (3), T/(M w^3) (4),
+ * eps^2/(d^2 + eps^2).  Host arrays of capacity rows;
+ * *count receives the rows written. Does not change the bodies. */
+NB_API int nb_mlp_samples(nb_ctx* ctx, uint64_t ntargets, uint64_t seed, uint64_t capacity,
+                          float* features, float* residuals, uint64_t* count);
+
+/* Batched MLP on the GPU: out[n][2] = network(features[n][12]) (without the
+ * output scale).  Host arrays. */
+NB_API int nb_mlp_forward(int32_t device, const float* params, uint64_t n, const float* features,
+                          float* out);
+
+/* Mean squared error of network(features) against targets[n][2] and its
+ * gradient with respect to the parameters (grad has NB_MLP_PARAMS entries; the
+ * output-scale entry is zero).  Host arrays. */
+NB_API int nb_mlp_loss_grad(int32_t device, const float* params, uint64_t n, const float* features,
+                            const float* targets, float* grad, float* loss);
+
+/* Trains on the GPU with Adam on BF16 tensor-core forward/backward kernels.
+ * residuals are raw (units of M / d^2); params[NB_MLP_PARAMS - 1] <= 0 asks
+ * for the output scale to be set to the residuals' RMS, and all-zero params
+ * ask for a seeded initialisation.  loss_per_epoch (nullable) gets one mean
+ * loss per epoch. */
+NB_API int nb_mlp_train(int32_t device, uint64_t n, const float* features, const float* residuals,
+                        const nb_mlp_train_params* tp, float* params, float* loss_per_epoch);
 
 /* Largest n nb_morton_sort_static accepts (its scratch is sized for it). */
 #define NB_STATIC_SORT_MAX_BODIES 262144

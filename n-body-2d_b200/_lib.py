@@ -24,6 +24,8 @@ NB_ERR_NOTFOUND = 6
 NB_MODE_FP64 = 0
 NB_MODE_SPLIT = 1
 NB_FLAG_QUADRUPOLE = 1
+NB_FLAG_LEARNED = 2
+NB_MLP_PARAMS = 5123  # include/nbody_b200.h
 NB_STATIC_SORT_MAX_BODIES = 262144  # include/nbody_b200.h
 
 # Every symbol include/nbody_b200.h declares.
@@ -32,6 +34,7 @@ EXPORTS = (
     "nb_upload", "nb_download", "nb_accelerations", "nb_debug_morton", "nb_debug_state",
     "nb_debug_tree", "nb_get_stats", "nb_last_error", "nb_status_string",
     "nb_allpairs_accelerations", "nb_phase_times", "nb_phase_name", "nb_morton_sort_static",
+    "nb_set_mlp_weights", "nb_mlp_samples", "nb_mlp_forward", "nb_mlp_loss_grad", "nb_mlp_train",
 )
 
 
@@ -58,6 +61,15 @@ class NbStats(C.Structure):
         ("ms_last_step", C.c_double),
         ("root_width", C.c_double),
         ("kernels_per_step", C.c_uint64),
+    ]
+
+
+class NbMlpTrainParams(C.Structure):
+    _fields_ = [
+        ("epochs", C.c_uint32),
+        ("batch", C.c_uint32),
+        ("lr", C.c_float),
+        ("seed", C.c_uint64),
     ]
 
 
@@ -99,6 +111,11 @@ def load() -> C.CDLL:
     lib.nb_status_string.argtypes = [C.c_int]
     lib.nb_status_string.restype = C.c_char_p
     lib.nb_morton_sort_static.argtypes = [_P, C.c_uint64, _P, _P, _P, _P]
+    lib.nb_set_mlp_weights.argtypes = [_P, _P]
+    lib.nb_mlp_samples.argtypes = [_P, C.c_uint64, C.c_uint64, C.c_uint64, _P, _P, _P]
+    lib.nb_mlp_forward.argtypes = [C.c_int32, _P, C.c_uint64, _P, _P]
+    lib.nb_mlp_loss_grad.argtypes = [C.c_int32, _P, C.c_uint64, _P, _P, _P, _P]
+    lib.nb_mlp_train.argtypes = [C.c_int32, C.c_uint64, _P, _P, C.POINTER(NbMlpTrainParams), _P, _P]
     lib.nb_phase_times.argtypes = [_P, _P, C.c_int]
     lib.nb_phase_name.argtypes = [C.c_int]
     lib.nb_phase_name.restype = C.c_char_p

@@ -142,13 +142,13 @@ __device__ __forceinline__ void sum_bodies(const WarpLists& L, int cnt, const fl
 
 // Walk the tree for one group [g0, g1] of <= 32 kBPL bodies (lane l owns
 // g0 + l, g0 + 32 + l, ...) and accumulate the FP32 accelerations.
-template <bool kQuad, int kBPL>
+template <bool kQuad, int kBPL, bool kLearned>
 __device__ __forceinline__ void walk_group(WarpLists& L, const Tree& t, int root, int n, int g0,
                                            int g1, const float* px, const float* py, const int* me,
                                            const bool* act_body, float eps2, float theta2,
                                            int leaf_size, float* ax, float* ay,
                                            unsigned long long& ncell, unsigned long long& npair,
-                                           unsigned* err) {
+                                           unsigned* err, int* band, int& nband, int band_cap) {
     const int lane = threadIdx.x & 31;
     float bx0 = INFINITY, bx1 = -INFINITY, by0 = INFINITY, by1 = -INFINITY;
 #pragma unroll
@@ -187,6 +187,7 @@ __device__ __forceinline__ void walk_group(WarpLists& L, const Tree& t, int root
         int bfirst = 0, bcnt = 0;
         int4 ch = make_int4(INT_MIN, INT_MIN, INT_MIN, INT_MIN);
         float4 c4 = make_float4(0.f, 0.f, 0.f, 0.f);
+        float band_d2 = 0.f;
         if (lane < k) {
             if (ref >= 0) {
                 c4 = t.cell4[ref];
@@ -195,6 +196,7 @@ __device__ __forceinline__ void walk_group(WarpLists& L, const Tree& t, int root
                 const float dx = fmaxf(fabsf(c4.x - gcx) - ghx, 0.f);
                 const float dy = fmaxf(fabsf(c4.y - gcy) - ghy, 0.f);
                 const float d2 = fmaf(dx, dx, dy * dy);
+                band_d2 = d2;
                 if (!overlap && c4.w < theta2 * d2) {
                     act = 1;
                 } else if (rg.y - rg.x < leaf_size) {
@@ -218,6 +220,16 @@ __device__ __forceinline__ void walk_group(WarpLists& L, const Tree& t, int root
             const int slot = ccount + __popc(acc_mask & below);
             L.cell[slot] = c4;
             if (kQuad) L.quad[slot] = t.cellq[ref];
+        }
+        if (kLearned) {
+            // band: accepted here but opened by the plain theta_B walk
+            const bool in_band = act == 1 && c4.w >= kThetaBand * kThetaBand * band_d2;
+            const unsigned bm = __ballot_sync(kFull, in_band);
+            if (in_band) {
+                const int slot = nband + __popc(bm & below);
+                if (slot < band_cap) band[slot] = ref;
+            }
+            nband += __popc(bm);
         }
         ccount += __popc(acc_mask);
         __syncwarp();
@@ -287,11 +299,11 @@ __device__ __forceinline__ void walk_group(WarpLists& L, const Tree& t, int root
 
 // Persistent: each warp takes groups from a global ticket until none is left,
 // which balances groups of very different cost.
-template <bool kQuad, int kBPL>
+template <bool kQuad, int kBPL, bool kLearned>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32)
 force_split(double2* __restrict__ pos, double2* __restrict__ vel, double2* __restrict__ acc_out,
-            int n, Tree t, DeviceScalars* __restrict__ s, float eps2, float theta2, int leaf_size,
-            double G_dt, double dt, int kick) {
+            float2* __restrict__ acc32, int n, Tree t, DeviceScalars* __restrict__ s, float eps2,
+            float theta2, int leaf_size, double G_dt, double dt, int kick) {
     __shared__ WarpLists lists[kWarpsPerBlock];
     const int lane = threadIdx.x & 31;
     WarpLists& L = lists[threadIdx.x >> 5];
@@ -319,11 +331,21 @@ force_split(double2* __restrict__ pos, double2* __restrict__ vel, double2* __res
             py[b] = (float)(P[b].y - cy);
         }
         unsigned long long ncell, npair;
-        walk_group<kQuad, kBPL>(L, t, root, n, g0, g1, px, py, me, on, eps2, theta2, leaf_size, ax,
-                                ay, ncell, npair, &s->error);
+        int nband = 0;
+        int* band = kLearned ? t.band + (int64_t)kBandPerBody * g0 : nullptr;
+        walk_group<kQuad, kBPL, kLearned>(L, t, root, n, g0, g1, px, py, me, on, eps2, theta2,
+                                          leaf_size, ax, ay, ncell, npair, &s->error, band, nband,
+                                          kBandPerBody * (g1 - g0 + 1));
+        if (kLearned) {
+            // the correction kernel adds the learned term, then kicks and drifts
+            if (lane == 0) t.band_count[g] = nband;
+#pragma unroll
+            for (int b = 0; b < kBPL; ++b)
+                if (on[b]) acc32[me[b]] = make_float2(ax[b], ay[b]);
+        }
 #pragma unroll
         for (int b = 0; b < kBPL; ++b) {
-            if (!on[b]) continue;
+            if (kLearned || !on[b]) continue;
             const int i = me[b];
             if (acc_out) acc_out[i] = make_double2((double)ax[b], (double)ay[b]);
             if (kick) {
@@ -348,20 +370,21 @@ force_split(double2* __restrict__ pos, double2* __restrict__ vel, double2* __res
     }
 }
 
-template <bool kQuad, int kBPL>
+template <bool kQuad, int kBPL, bool kLearned>
 void launch_split_kernel(nb_ctx* c, const BodyBuffers& b, bool kick, bool store_acc) {
-    if (c->split_blocks == 0) {
+    int& grid = c->split_blocks[(kQuad ? 1 : 0) + (kLearned ? 2 : 0)];
+    if (grid == 0) {
         int blocks = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, force_split<kQuad, kBPL>,
-                                                          kWarpsPerBlock * 32, 0) != cudaSuccess ||
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                &blocks, force_split<kQuad, kBPL, kLearned>, kWarpsPerBlock * 32, 0) != cudaSuccess ||
             blocks < 1)
             blocks = 4;
-        c->split_blocks = c->sm_count * blocks;
+        grid = c->sm_count * blocks;
     }
     const float theta2 = (float)(c->p.theta * c->p.theta);
     const int leaf = c->p.leaf_size > 0 ? c->p.leaf_size : kDefaultLeaf;
-    force_split<kQuad, kBPL><<<c->split_blocks, 32 * kWarpsPerBlock, 0, c->stream>>>(
-        b.pos, b.vel, store_acc ? c->acc : nullptr, (int)c->n, c->tree, c->scal,
+    force_split<kQuad, kBPL, kLearned><<<grid, 32 * kWarpsPerBlock, 0, c->stream>>>(
+        b.pos, b.vel, store_acc ? c->acc : nullptr, c->acc32, (int)c->n, c->tree, c->scal,
         (float)c->p.epsilon_squared, theta2, leaf, c->p.G * c->p.timestep, c->p.timestep,
         kick ? 1 : 0);
 }
@@ -373,10 +396,12 @@ int split_group_size(const nb_ctx* c) { return 32 * kBodiesPerLane; }
 void launch_force_split(nb_ctx* c, const BodyBuffers& b, bool kick, bool store_acc) {
     c->launches += 1;
     cudaMemsetAsync(&c->scal->group_ticket, 0, sizeof(unsigned), c->stream);
-    if (c->p.flags & NB_FLAG_QUADRUPOLE)
-        launch_split_kernel<true, kBodiesPerLane>(c, b, kick, store_acc);
+    if (c->p.flags & NB_FLAG_LEARNED)
+        launch_split_kernel<false, kBodiesPerLane, true>(c, b, kick, store_acc);
+    else if (c->p.flags & NB_FLAG_QUADRUPOLE)
+        launch_split_kernel<true, kBodiesPerLane, false>(c, b, kick, store_acc);
     else
-        launch_split_kernel<false, kBodiesPerLane>(c, b, kick, store_acc);
+        launch_split_kernel<false, kBodiesPerLane, false>(c, b, kick, store_acc);
 }
 
 }  // namespace nb

@@ -1,0 +1,710 @@
+// k_mlp.cu -- learned far-field correction (SPLIT mode, NB_FLAG_LEARNED).
+//
+// A 12 -> 64 -> 64 -> 2 MLP (tanh hidden layers, BF16 weights and activations,
+// FP32 accumulation) predicts, for a cell accepted at theta_L = theta but that
+// plain theta_B = 0.5 would have opened, the residual between the cell's exact
+// pull and its monopole, in units of M / d^2:
+//   r = (sum_j m_j (x_j - p)(|x_j - p|^2 + eps^2)^-3/2
+//        - M (c - p)(|c - p|^2 + eps^2)^-3/2) * d^2 / M,    d = |p - c|.
+// Features of (point p, cell): u = (p - c) / d (2), w / d, the heaviest child's
+// mass fraction, S / (M w^2) (3), T / (M w^3) (4), and eps^2 / (d^2 + eps^2):
+// the softening ratio takes the last of the eight moment slots because near
+// cells (d ~ eps) have residuals that depend on it far more than on any
+// higher moment.
+//
+// Tensor-core layout: mma.sync m16n8k16 BF16 with FP32 accumulators.  A 16-row
+// tile (16 samples, or 16 cells of one target group) runs through the three
+// layers in registers; the accumulator fragment of one layer is, element for
+// element, the A fragment of the next, so no shuffles are needed.
+//
+// Inference is per target group: the traversal lists each group's band cells;
+// mlp_correct_kick evaluates the MLP at the group's centre for all of them in
+// tiles of 16, adds the summed correction to every body's acceleration, and
+// applies the FP64 kick and drift.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <climits>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "nb_internal.cuh"
+
+namespace nb {
+
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kH = 64;
+constexpr int kNin = 12;
+
+// FP32 parameter vector layout (also the ABI layout of the weights).
+constexpr int kW1 = 0;                    // [64][12]
+constexpr int kB1 = kW1 + kH * kNin;      // [64]
+constexpr int kW2 = kB1 + kH;             // [64][64]  (out, in)
+constexpr int kB2 = kW2 + kH * kH;        // [64]
+constexpr int kW3 = kB2 + kH;             // [2][64]
+constexpr int kB3 = kW3 + 2 * kH;         // [2]
+constexpr int kYS = kB3 + 2;              // output scale
+constexpr int kParams = kYS + 1;
+static_assert(kParams == NB_MLP_PARAMS, "weight layout and header disagree");
+
+// BF16 images of the weights in the layouts the fragments read.
+struct MlpWeights {
+    __nv_bfloat16 w1[kH][16];    // B of layer 1: [n = hidden][k = input, padded]
+    __nv_bfloat16 w2[kH][kH];    // B of layer 2: [n = out][k = in]
+    __nv_bfloat16 w3[8][kH];     // B of layer 3: [n = out, padded][k = hidden]
+    __nv_bfloat16 w2t[kH][kH];   // backward: [n = in][k = out]
+    __nv_bfloat16 w3t[kH][16];   // backward: [n = hidden][k = out, padded]
+    float b1[kH], b2[kH], b3[8];
+    float yscale;
+};
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+    const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<const uint32_t*>(&v);
+}
+
+__device__ __forceinline__ void mma16816(float c[4], const uint32_t a[4], uint32_t b0, uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+        "{%8,%9}, {%0,%1,%2,%3};"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// B fragment of an [n][k] row-major BF16 matrix (leading dimension ld), for
+// the 8 columns starting at nb and the 16 k starting at kb.
+__device__ __forceinline__ void load_b(const __nv_bfloat16* m, int ld, int nb, int kb, uint32_t& b0,
+                                       uint32_t& b1) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
+    const __nv_bfloat16* row = m + (nb + g) * ld + kb + 2 * q;
+    b0 = *reinterpret_cast<const uint32_t*>(row);
+    b1 = *reinterpret_cast<const uint32_t*>(row + 8);
+}
+
+// A fragment of a 16 x 16 tile of a row-major BF16 matrix.
+__device__ __forceinline__ void load_a(const __nv_bfloat16* m, int ld, int kb, uint32_t a[4]) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
+    a[0] = *reinterpret_cast<const uint32_t*>(m + g * ld + kb + 2 * q);
+    a[1] = *reinterpret_cast<const uint32_t*>(m + (g + 8) * ld + kb + 2 * q);
+    a[2] = *reinterpret_cast<const uint32_t*>(m + g * ld + kb + 2 * q + 8);
+    a[3] = *reinterpret_cast<const uint32_t*>(m + (g + 8) * ld + kb + 2 * q + 8);
+}
+
+// Accumulators of n-tiles 2kt and 2kt+1 -> A fragment of k-tile kt.
+__device__ __forceinline__ void c_to_a(const float c0[4], const float c1[4], uint32_t a[4]) {
+    a[0] = pack_bf16(c0[0], c0[1]);
+    a[1] = pack_bf16(c0[2], c0[3]);
+    a[2] = pack_bf16(c1[0], c1[1]);
+    a[3] = pack_bf16(c1[2], c1[3]);
+}
+
+// Activations kept for the backward pass (the BF16-rounded values the next
+// layer consumed).
+struct Fwd {
+    float h1[8][4];
+    float h2[8][4];
+    float y[4];   // n-tile 0 of the output: columns 2q, 2q+1 of rows g, g+8
+};
+
+__device__ __forceinline__ float bf16_round(float v) {
+    return __bfloat162float(__float2bfloat16_rn(v));
+}
+
+// Forward pass of one 16-row tile whose inputs are the A fragment `x`.
+__device__ __forceinline__ void mlp_forward(const MlpWeights& W, const uint32_t x[4], Fwd& f) {
+    const int q = threadIdx.x & 3;
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt) {
+        const float bl = W.b1[8 * nt + 2 * q], bh = W.b1[8 * nt + 2 * q + 1];
+        float c[4] = {bl, bh, bl, bh};
+        uint32_t b0, b1;
+        load_b(&W.w1[0][0], 16, 8 * nt, 0, b0, b1);
+        mma16816(c, x, b0, b1);
+#pragma unroll
+        for (int e = 0; e < 4; ++e) f.h1[nt][e] = bf16_round(tanhf(c[e]));
+    }
+    uint32_t a1[4][4];
+#pragma unroll
+    for (int kt = 0; kt < 4; ++kt) c_to_a(f.h1[2 * kt], f.h1[2 * kt + 1], a1[kt]);
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt) {
+        const float bl = W.b2[8 * nt + 2 * q], bh = W.b2[8 * nt + 2 * q + 1];
+        float c[4] = {bl, bh, bl, bh};
+#pragma unroll
+        for (int kt = 0; kt < 4; ++kt) {
+            uint32_t b0, b1;
+            load_b(&W.w2[0][0], kH, 8 * nt, 16 * kt, b0, b1);
+            mma16816(c, a1[kt], b0, b1);
+        }
+#pragma unroll
+        for (int e = 0; e < 4; ++e) f.h2[nt][e] = bf16_round(tanhf(c[e]));
+    }
+    uint32_t a2[4][4];
+#pragma unroll
+    for (int kt = 0; kt < 4; ++kt) c_to_a(f.h2[2 * kt], f.h2[2 * kt + 1], a2[kt]);
+    {
+        const float bl = W.b3[2 * q], bh = W.b3[2 * q + 1];
+        float c[4] = {bl, bh, bl, bh};
+#pragma unroll
+        for (int kt = 0; kt < 4; ++kt) {
+            uint32_t b0, b1;
+            load_b(&W.w3[0][0], kH, 0, 16 * kt, b0, b1);
+            mma16816(c, a2[kt], b0, b1);
+        }
+#pragma unroll
+        for (int e = 0; e < 4; ++e) f.y[e] = c[e];
+    }
+}
+
+// FP32 master parameters -> BF16 fragment images (one block).
+__device__ void fill_weights(const float* __restrict__ p, MlpWeights& W) {
+    for (int k = threadIdx.x; k < kH * 16; k += blockDim.x) {
+        const int o = k / 16, i = k % 16;
+        W.w1[o][i] = __float2bfloat16_rn(i < kNin ? p[kW1 + o * kNin + i] : 0.f);
+        W.w3t[o][i] = __float2bfloat16_rn(i < 2 ? p[kW3 + i * kH + o] : 0.f);
+    }
+    for (int k = threadIdx.x; k < kH * kH; k += blockDim.x) {
+        const int o = k / kH, i = k % kH;
+        W.w2[o][i] = __float2bfloat16_rn(p[kW2 + k]);
+        W.w2t[i][o] = __float2bfloat16_rn(p[kW2 + k]);
+    }
+    for (int k = threadIdx.x; k < 8 * kH; k += blockDim.x) {
+        const int o = k / kH, i = k % kH;
+        W.w3[o][i] = __float2bfloat16_rn(o < 2 ? p[kW3 + o * kH + i] : 0.f);
+    }
+    for (int k = threadIdx.x; k < kH; k += blockDim.x) {
+        W.b1[k] = p[kB1 + k];
+        W.b2[k] = p[kB2 + k];
+    }
+    if (threadIdx.x < 8) W.b3[threadIdx.x] = threadIdx.x < 2 ? p[kB3 + threadIdx.x] : 0.f;
+    if (threadIdx.x == 0) W.yscale = p[kYS];
+}
+
+// One 16 x 16 BF16 input tile staged in shared memory per warp.
+struct XTile {
+    __nv_bfloat16 x[16][16];
+};
+
+// ---- batched forward (tests and offline evaluation) --------------------
+constexpr int kWarps = 4;
+
+__global__ void __launch_bounds__(kWarps * 32)
+mlp_forward_kernel(const float* __restrict__ params, const float* __restrict__ X, int64_t n,
+                   float* __restrict__ Y) {
+    __shared__ MlpWeights W;
+    __shared__ XTile tiles[kWarps];
+    fill_weights(params, W);
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    XTile& T = tiles[warp];
+    const int64_t ntiles = (n + 15) / 16;
+    for (int64_t tile = blockIdx.x * (int64_t)kWarps + warp; tile < ntiles;
+         tile += (int64_t)gridDim.x * kWarps) {
+        for (int e = lane; e < 256; e += 32) {
+            const int r = e >> 4, k = e & 15;
+            const int64_t s = tile * 16 + r;
+            T.x[r][k] = __float2bfloat16_rn(s < n && k < kNin ? X[s * kNin + k] : 0.f);
+        }
+        __syncwarp();
+        uint32_t a[4];
+        load_a(&T.x[0][0], 16, 0, a);
+        Fwd f;
+        mlp_forward(W, a, f);
+        const int g = lane >> 2, q = lane & 3;
+        if (q == 0) {
+            const int64_t s0 = tile * 16 + g, s1 = s0 + 8;
+            if (s0 < n) {
+                Y[2 * s0] = f.y[0];
+                Y[2 * s0 + 1] = f.y[1];
+            }
+            if (s1 < n) {
+                Y[2 * s1] = f.y[2];
+                Y[2 * s1 + 1] = f.y[3];
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// ---- training: loss and gradients of a batch ---------------------------
+// Loss = mean over the batch of |y - t|^2 (t already divided by yscale).
+// Each warp takes 16-sample tiles; the backward GEMMs run on the tensor cores:
+//   dh2 = dy W3, dh1 = dp2 W2 (A from the accumulators, B = transposed
+//   weights), and the weight gradients dW = dp^T h with the batch as the K
+//   dimension (A and B staged transposed in shared memory).  Gradients sum in
+//   per-block shared memory and then in the global FP32 gradient vector.
+struct TrainSmem {
+    MlpWeights W;
+    float g[kParams];                // block-local gradient sums
+    __nv_bfloat16 xt[kWarps][16][16];    // inputs  [s][k]
+    __nv_bfloat16 p2t[kWarps][kH][16];   // dp2^T   [o][s]
+    __nv_bfloat16 p1t[kWarps][kH][16];   // dp1^T   [o][s]
+    __nv_bfloat16 h1t[kWarps][kH][16];   // h1^T    [i][s]
+    __nv_bfloat16 h2t[kWarps][kH][16];   // h2^T    [i][s]
+    __nv_bfloat16 dyt[kWarps][16][16];   // dy^T    [o][s] (rows >= 2 zero)
+    __nv_bfloat16 xtt[kWarps][16][16];   // x^T     [k][s]
+    float loss;
+};
+
+__device__ __forceinline__ void atomic_tile(float* dst, int ld, int mb, int nb, const float c[4]) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
+    atomicAdd(dst + (mb + g) * ld + nb + 2 * q, c[0]);
+    atomicAdd(dst + (mb + g) * ld + nb + 2 * q + 1, c[1]);
+    atomicAdd(dst + (mb + g + 8) * ld + nb + 2 * q, c[2]);
+    atomicAdd(dst + (mb + g + 8) * ld + nb + 2 * q + 1, c[3]);
+}
+
+__global__ void __launch_bounds__(kWarps * 32)
+mlp_grad_kernel(const float* __restrict__ params, const float* __restrict__ X,
+                const float* __restrict__ Yt, const int64_t* __restrict__ idx, int64_t n,
+                float inv_n, float* __restrict__ grad, float* __restrict__ loss) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    TrainSmem& S = *reinterpret_cast<TrainSmem*>(smem_raw);
+    fill_weights(params, S.W);
+    for (int k = threadIdx.x; k < kParams; k += blockDim.x) S.g[k] = 0.f;
+    if (threadIdx.x == 0) S.loss = 0.f;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, q = lane & 3;
+    const int64_t ntiles = (n + 15) / 16;
+    for (int64_t tile = blockIdx.x * (int64_t)kWarps + warp; tile < ntiles;
+         tile += (int64_t)gridDim.x * kWarps) {
+        // stage the inputs (row-major for the forward, transposed for dW1)
+        for (int e = lane; e < 256; e += 32) {
+            const int r = e >> 4, k = e & 15;
+            const int64_t s = tile * 16 + r;
+            const int64_t src = s < n ? (idx ? idx[s] : s) : -1;
+            const __nv_bfloat16 v = __float2bfloat16_rn(src >= 0 && k < kNin ? X[src * kNin + k] : 0.f);
+            S.xt[warp][r][k] = v;
+            S.xtt[warp][k][r] = v;
+        }
+        __syncwarp();
+        uint32_t a[4];
+        load_a(&S.xt[warp][0][0], 16, 0, a);
+        Fwd f;
+        mlp_forward(S.W, a, f);
+        // dy = 2 (y - t) / n on valid rows and the two output columns
+        float dy[4];
+        float l = 0.f;
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const int row = g + (e >= 2 ? 8 : 0), col = 2 * q + (e & 1);
+            const int64_t s = tile * 16 + row;
+            float d = 0.f;
+            if (s < n && col < 2) {
+                const int64_t src = idx ? idx[s] : s;
+                d = f.y[e] - Yt[2 * src + col];
+                l += d * d;
+            }
+            dy[e] = 2.f * d * inv_n;
+        }
+        for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(kFull, l, o);
+        if (lane == 0) atomicAdd(&S.loss, l * inv_n);
+        // dh2 = dy W3 -> dp2 = dh2 (1 - h2^2)
+        uint32_t ady[4] = {pack_bf16(dy[0], dy[1]), pack_bf16(dy[2], dy[3]), 0u, 0u};
+        float dp2[8][4];
+#pragma unroll
+        for (int nt = 0; nt < 8; ++nt) {
+            float c[4] = {0.f, 0.f, 0.f, 0.f};
+            uint32_t b0, b1;
+            load_b(&S.W.w3t[0][0], 16, 8 * nt, 0, b0, b1);
+            mma16816(c, ady, b0, b1);
+#pragma unroll
+            for (int e = 0; e < 4; ++e) dp2[nt][e] = c[e] * (1.f - f.h2[nt][e] * f.h2[nt][e]);
+        }
+        // dh1 = dp2 W2 -> dp1 = dh1 (1 - h1^2)
+        uint32_t ap2[4][4];
+#pragma unroll
+        for (int kt = 0; kt < 4; ++kt) c_to_a(dp2[2 * kt], dp2[2 * kt + 1], ap2[kt]);
+        float dp1[8][4];
+#pragma unroll
+        for (int nt = 0; nt < 8; ++nt) {
+            float c[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+            for (int kt = 0; kt < 4; ++kt) {
+                uint32_t b0, b1;
+                load_b(&S.W.w2t[0][0], kH, 8 * nt, 16 * kt, b0, b1);
+                mma16816(c, ap2[kt], b0, b1);
+            }
+#pragma unroll
+            for (int e = 0; e < 4; ++e) dp1[nt][e] = c[e] * (1.f - f.h1[nt][e] * f.h1[nt][e]);
+        }
+        // stage the transposes: element (row s, col o) -> [o][s]
+#pragma unroll
+        for (int nt = 0; nt < 8; ++nt)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const int s = g + (e >= 2 ? 8 : 0), o = 8 * nt + 2 * q + (e & 1);
+                S.p2t[warp][o][s] = __float2bfloat16_rn(dp2[nt][e]);
+                S.p1t[warp][o][s] = __float2bfloat16_rn(dp1[nt][e]);
+                S.h1t[warp][o][s] = __float2bfloat16_rn(f.h1[nt][e]);
+                S.h2t[warp][o][s] = __float2bfloat16_rn(f.h2[nt][e]);
+            }
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const int s = g + (e >= 2 ? 8 : 0), o = 2 * q + (e & 1);
+            S.dyt[warp][o][s] = __float2bfloat16_rn(o < 2 ? dy[e] : 0.f);
+            S.dyt[warp][o + 8][s] = __float2bfloat16(0.f);
+        }
+        __syncwarp();
+        // bias gradients: column sums
+#pragma unroll
+        for (int nt = 0; nt < 8; ++nt)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const int o = 8 * nt + 2 * q + (e & 1);
+                atomicAdd(&S.g[kB2 + o], dp2[nt][e]);
+                atomicAdd(&S.g[kB1 + o], dp1[nt][e]);
+            }
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+            if (2 * q + (e & 1) < 2) atomicAdd(&S.g[kB3 + 2 * q + (e & 1)], dy[e]);
+        // dW2[o][i] = sum_s dp2[s][o] h1[s][i]: A = dp2^T (m = o), B = h1 (k = s)
+#pragma unroll
+        for (int mt = 0; mt < 4; ++mt) {
+            uint32_t am[4];
+            load_a(&S.p2t[warp][16 * mt][0], 16, 0, am);
+#pragma unroll
+            for (int nt = 0; nt < 8; ++nt) {
+                float c[4] = {0.f, 0.f, 0.f, 0.f};
+                uint32_t b0, b1;
+                load_b(&S.h1t[warp][0][0], 16, 8 * nt, 0, b0, b1);
+                mma16816(c, am, b0, b1);
+                atomic_tile(S.g + kW2, kH, 16 * mt, 8 * nt, c);
+            }
+        }
+        // dW1[o][k] = sum_s dp1[s][o] x[s][k]
+#pragma unroll
+        for (int mt = 0; mt < 4; ++mt) {
+            uint32_t am[4];
+            load_a(&S.p1t[warp][16 * mt][0], 16, 0, am);
+#pragma unroll
+            for (int nt = 0; nt < 2; ++nt) {
+                float c[4] = {0.f, 0.f, 0.f, 0.f};
+                uint32_t b0, b1;
+                load_b(&S.xtt[warp][0][0], 16, 8 * nt, 0, b0, b1);
+                mma16816(c, am, b0, b1);
+                // columns >= 12 are padding
+                const int o0 = 16 * mt + g, k0 = 8 * nt + 2 * q;
+                if (k0 < kNin) {
+                    atomicAdd(&S.g[kW1 + o0 * kNin + k0], c[0]);
+                    atomicAdd(&S.g[kW1 + (o0 + 8) * kNin + k0], c[2]);
+                }
+                if (k0 + 1 < kNin) {
+                    atomicAdd(&S.g[kW1 + o0 * kNin + k0 + 1], c[1]);
+                    atomicAdd(&S.g[kW1 + (o0 + 8) * kNin + k0 + 1], c[3]);
+                }
+            }
+        }
+        // dW3[o][i] = sum_s dy[s][o] h2[s][i] (rows o >= 2 are padding)
+        {
+            uint32_t am[4];
+            load_a(&S.dyt[warp][0][0], 16, 0, am);
+#pragma unroll
+            for (int nt = 0; nt < 8; ++nt) {
+                float c[4] = {0.f, 0.f, 0.f, 0.f};
+                uint32_t b0, b1;
+                load_b(&S.h2t[warp][0][0], 16, 8 * nt, 0, b0, b1);
+                mma16816(c, am, b0, b1);
+                if (g < 2) {
+                    atomicAdd(&S.g[kW3 + g * kH + 8 * nt + 2 * q], c[0]);
+                    atomicAdd(&S.g[kW3 + g * kH + 8 * nt + 2 * q + 1], c[1]);
+                }
+            }
+        }
+        __syncwarp();
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < kYS; k += blockDim.x) {
+        const float v = S.g[k];
+        if (v != 0.f) atomicAdd(grad + k, v);
+    }
+    if (threadIdx.x == 0) atomicAdd(loss, S.loss);
+}
+
+// Adam on the FP32 master parameters (the output scale is not trained).
+__global__ void mlp_adam_kernel(float* __restrict__ p, const float* __restrict__ g,
+                                float* __restrict__ m, float* __restrict__ v, float lr, float b1,
+                                float b2, float eps, float c1, float c2) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= kYS) return;
+    const float gk = g[k];
+    const float mk = b1 * m[k] + (1.f - b1) * gk;
+    const float vk = b2 * v[k] + (1.f - b2) * gk * gk;
+    m[k] = mk;
+    v[k] = vk;
+    p[k] -= lr * (mk / c1) / (sqrtf(vk / c2) + eps);
+}
+
+}  // namespace
+
+int mlp_smem_bytes() { return (int)sizeof(TrainSmem); }
+
+namespace {
+
+// ---- features shared by sampling and inference -------------------------
+// (p - c), d and the cell record -> the 12 features (see the file header).
+__device__ __forceinline__ void mlp_features(float ux, float uy, float d, float eps2,
+                                             const float4 f0, const float4 f1, const float4 f2,
+                                             float* x) {
+    const float inv = 1.f / d;
+    x[0] = ux * inv;
+    x[1] = uy * inv;
+    x[2] = f2.y * inv;  // w / d
+    x[3] = f0.x;        // heaviest child's mass fraction
+    x[4] = f0.y;        // S / (M w^2)
+    x[5] = f0.z;
+    x[6] = f0.w;
+    x[7] = f1.x;        // T / (M w^3)
+    x[8] = f1.y;
+    x[9] = f1.z;
+    x[10] = f1.w;
+    x[11] = eps2 / (d * d + eps2);
+}
+
+// ---- residual samples (training data) ----------------------------------
+// One warp per target body: a depth-first walk with the per-body test at
+// theta_L; every cell accepted at theta_L but not at theta_B is a band cell
+// and yields one sample, its exact pull summed over its bodies in FP64.
+constexpr int kSampleStack = 128;
+
+__global__ void __launch_bounds__(kWarps * 32)
+mlp_samples_kernel(Tree t, const DeviceScalars* __restrict__ s, const double2* __restrict__ pos,
+                   const double* __restrict__ mass, int n, const int* __restrict__ slots, int nslots,
+                   double thL2, double thB2, double eps2, float* __restrict__ X,
+                   float* __restrict__ Y, unsigned* __restrict__ count, unsigned cap) {
+    __shared__ int stacks[kWarps][kSampleStack];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int* stk = stacks[warp];
+    const int cells = s->cells;
+    for (int w = blockIdx.x * kWarps + warp; w < nslots; w += gridDim.x * kWarps) {
+        const int i = slots[w];
+        const double2 p = pos[i];
+        int top = 0;
+        if (lane == 0) stk[0] = s->root;
+        __syncwarp();
+        while (top >= 0) {
+            const int ref = stk[top];
+            --top;
+            __syncwarp();
+            if (ref < 0 || ref >= cells) continue;  // leaves are summed exactly: no correction
+            const double M = t.mass[ref];
+            const double2 c = t.com[ref];
+            const int2 rg = t.range[ref];
+            const double w2 = s->wsq[t.level[ref]];
+            const double ux = p.x - c.x, uy = p.y - c.y;
+            const double d2 = ux * ux + uy * uy;
+            const bool holds = rg.x <= i && i <= rg.y;
+            if (holds || !(w2 < thL2 * d2)) {
+                const int4 ch = t.child[ref];
+                const int refs[4] = {ch.x, ch.y, ch.z, ch.w};
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    if (refs[q] >= 0 && top + 1 < kSampleStack) {
+                        ++top;
+                        if (lane == 0) stk[top] = refs[q];
+                    }
+                __syncwarp();
+                continue;
+            }
+            if (!(w2 >= thB2 * d2)) continue;  // accepted by plain theta_B too
+            double ax = 0.0, ay = 0.0;
+            for (int j = rg.x + lane; j <= rg.y; j += 32) {
+                const double2 q = pos[j];
+                const double dx = q.x - p.x, dy = q.y - p.y;
+                const double r2 = dx * dx + dy * dy + eps2;
+                const double a = mass[j] / (r2 * sqrt(r2));
+                ax += dx * a;
+                ay += dy * a;
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                ax += __shfl_xor_sync(kFull, ax, o);
+                ay += __shfl_xor_sync(kFull, ay, o);
+            }
+            if (lane == 0) {
+                const double r2 = d2 + eps2;
+                const double am = M / (r2 * sqrt(r2));
+                const double scale = d2 / M;
+                const unsigned slot = atomicAdd(count, 1u);
+                if (slot < cap) {
+                    float x[kNin];
+                    mlp_features((float)ux, (float)uy, (float)sqrt(d2), (float)eps2,
+                                 t.cellf[3 * ref], t.cellf[3 * ref + 1], t.cellf[3 * ref + 2], x);
+#pragma unroll
+                    for (int k = 0; k < kNin; ++k) X[(int64_t)slot * kNin + k] = x[k];
+                    Y[2 * (int64_t)slot] = (float)((ax - (-ux) * am) * scale);
+                    Y[2 * (int64_t)slot + 1] = (float)((ay - (-uy) * am) * scale);
+                }
+            }
+        }
+    }
+}
+
+// ---- inference: per-group correction, then kick and drift --------------
+// acc32 holds the traversal's FP32 accelerations (monopoles of every
+// accepted cell and the direct sums); band[] lists, per group, the cells
+// accepted at theta but not at theta_B (capacity kBandPerBody per body of the
+// group, starting at kBandPerBody * first body).
+struct CorrSmem {
+    MlpWeights W;
+    __nv_bfloat16 x[kWarps][16][16];
+    float scale[kWarps][16][2];  // per tile row: M / d^2 and the row's validity
+};
+
+__global__ void __launch_bounds__(kWarps * 32)
+mlp_correct_kick(const float* __restrict__ params, Tree t, const DeviceScalars* __restrict__ s,
+                 double2* __restrict__ pos, double2* __restrict__ vel,
+                 const float2* __restrict__ acc32, double2* __restrict__ acc_out, int n,
+                 float eps2, double G_dt, double dt, int kick) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    CorrSmem& S = *reinterpret_cast<CorrSmem*>(smem_raw);
+    fill_weights(params, S.W);
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, q = lane & 3;
+    const double cx = s->center[0], cy = s->center[1];
+    const int ngroups = s->groups;
+    const float ys = S.W.yscale;
+    for (int gi = blockIdx.x * kWarps + warp; gi < ngroups; gi += gridDim.x * kWarps) {
+        const int2 gr = t.groups[gi];
+        const int g0 = gr.x, g1 = min(gr.y, n - 1);
+        double2 P[2];
+        bool on[2];
+        float bx0 = INFINITY, bx1 = -INFINITY, by0 = INFINITY, by1 = -INFINITY;
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+            const int i = min(g0 + 32 * b + lane, g1);
+            on[b] = g0 + 32 * b + lane <= g1;
+            P[b] = pos[i];
+            if (on[b]) {
+                const float px = (float)(P[b].x - cx), py = (float)(P[b].y - cy);
+                bx0 = fminf(bx0, px);
+                bx1 = fmaxf(bx1, px);
+                by0 = fminf(by0, py);
+                by1 = fmaxf(by1, py);
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            bx0 = fminf(bx0, __shfl_xor_sync(kFull, bx0, o));
+            bx1 = fmaxf(bx1, __shfl_xor_sync(kFull, bx1, o));
+            by0 = fminf(by0, __shfl_xor_sync(kFull, by0, o));
+            by1 = fmaxf(by1, __shfl_xor_sync(kFull, by1, o));
+        }
+        const float gx = 0.5f * (bx0 + bx1), gy = 0.5f * (by0 + by1);
+        const int nband = min(t.band_count[gi], kBandPerBody * (g1 - g0 + 1));
+        const int* band = t.band + (int64_t)kBandPerBody * g0;
+        float cxs = 0.f, cys = 0.f;
+        for (int base = 0; base < nband; base += 16) {
+            // lanes 0..15 build the features of one band cell each
+            if (lane < 16) {
+                const int r = base + lane;
+                float x[kNin];
+                float sc = 0.f;
+                if (r < nband) {
+                    const int ref = band[r];
+                    const float4 c4 = t.cell4[ref];
+                    const float ux = gx - c4.x, uy = gy - c4.y;
+                    const float d2 = fmaxf(ux * ux + uy * uy, 1e-30f);
+                    mlp_features(ux, uy, sqrtf(d2), eps2, t.cellf[3 * ref], t.cellf[3 * ref + 1],
+                                 t.cellf[3 * ref + 2], x);
+                    sc = c4.z / d2;
+                } else {
+#pragma unroll
+                    for (int k = 0; k < kNin; ++k) x[k] = 0.f;
+                }
+#pragma unroll
+                for (int k = 0; k < 16; ++k) S.x[warp][lane][k] = __float2bfloat16_rn(k < kNin ? x[k] : 0.f);
+                S.scale[warp][lane][0] = sc;
+            }
+            __syncwarp();
+            uint32_t a[4];
+            load_a(&S.x[warp][0][0], 16, 0, a);
+            Fwd f;
+            mlp_forward(S.W, a, f);
+            if (q == 0) {
+                cxs += ys * (f.y[0] * S.scale[warp][g][0] + f.y[2] * S.scale[warp][g + 8][0]);
+                cys += ys * (f.y[1] * S.scale[warp][g][0] + f.y[3] * S.scale[warp][g + 8][0]);
+            }
+            __syncwarp();
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            cxs += __shfl_xor_sync(kFull, cxs, o);
+            cys += __shfl_xor_sync(kFull, cys, o);
+        }
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+            if (!on[b]) continue;
+            const int i = g0 + 32 * b + lane;
+            const float2 a32 = acc32[i];
+            const double ax = (double)a32.x + (double)cxs, ay = (double)a32.y + (double)cys;
+            if (acc_out) acc_out[i] = make_double2(ax, ay);
+            if (kick) {
+                double2 v = vel[i];
+                v.x += ax * G_dt;
+                v.y += ay * G_dt;
+                vel[i] = v;
+                double2 p = P[b];
+                p.x += v.x * dt;
+                p.y += v.y * dt;
+                pos[i] = p;
+            }
+        }
+    }
+}
+
+inline unsigned blocks_for(int64_t n, int per) { return (unsigned)((n + per - 1) / per); }
+
+}  // namespace
+
+void launch_mlp_correct(nb_ctx* c, const BodyBuffers& b, bool kick, bool store_acc) {
+    c->launches += 1;
+    const int smem = (int)sizeof(CorrSmem);
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(mlp_correct_kick, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        attr_set = true;
+    }
+    mlp_correct_kick<<<c->sm_count * 8, kWarps * 32, smem, c->stream>>>(
+        c->mlp_params, c->tree, c->scal, b.pos, b.vel, c->acc32, store_acc ? c->acc : nullptr,
+        (int)c->n, (float)c->p.epsilon_squared, c->p.G * c->p.timestep, c->p.timestep, kick ? 1 : 0);
+}
+
+void launch_mlp_samples(nb_ctx* c, const BodyBuffers& b, const int* slots, int nslots, float* X,
+                        float* Y, unsigned* count, unsigned cap) {
+    const double thL = c->p.theta, thB = kThetaBand;
+    mlp_samples_kernel<<<c->sm_count * 8, kWarps * 32, 0, c->stream>>>(
+        c->tree, c->scal, b.pos, b.mass, (int)c->n, slots, nslots, thL * thL, thB * thB,
+        c->p.epsilon_squared, X, Y, count, cap);
+}
+
+int mlp_forward_device(const float* params, const float* X, int64_t n, float* Y,
+                       cudaStream_t st) {
+    mlp_forward_kernel<<<(unsigned)std::min<int64_t>((n + 63) / 64, 4096), kWarps * 32, 0, st>>>(
+        params, X, n, Y);
+    return cudaGetLastError() == cudaSuccess ? NB_OK : NB_ERR_CUDA;
+}
+
+int mlp_grad_device(const float* params, const float* X, const float* Yt, const int64_t* idx,
+                    int64_t n, float* grad, float* loss, int blocks, cudaStream_t st) {
+    const int smem = (int)sizeof(TrainSmem);
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(mlp_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        attr_set = true;
+    }
+    mlp_grad_kernel<<<blocks, kWarps * 32, smem, st>>>(params, X, Yt, idx, n, 1.f / (float)n, grad,
+                                                       loss);
+    return cudaGetLastError() == cudaSuccess ? NB_OK : NB_ERR_CUDA;
+}
+
+int mlp_adam_device(float* p, const float* g, float* m, float* v, float lr, int step,
+                    cudaStream_t st) {
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = 1.f - powf(b1, (float)step), c2 = 1.f - powf(b2, (float)step);
+    mlp_adam_kernel<<<blocks_for(kYS, 256), 256, 0, st>>>(p, g, m, v, lr, b1, b2, 1e-8f, c1, c2);
+    return cudaGetLastError() == cudaSuccess ? NB_OK : NB_ERR_CUDA;
+}
+
+}  // namespace nb

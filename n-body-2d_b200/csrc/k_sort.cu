@@ -314,30 +314,62 @@ constexpr uint32_t kFlagPrefix = 2u << 30;
 constexpr uint32_t kCountMask = (1u << 30) - 1;
 constexpr int kSpinLimit = 1 << 22;
 
+// Histograms of all eight digits.  Each thread counts a run of kHistRun
+// consecutive keys and flushes a digit's count to shared memory only when the
+// digit changes: the keys arrive nearly sorted (the bodies keep last step's
+// order), so the high digits change rarely and the low ones hit random bins.
+constexpr int kHistRun = 16;
+
 __global__ void __launch_bounds__(kSortThreads)
 onesweep_histogram(const uint64_t* __restrict__ key, int64_t n, uint32_t* __restrict__ hist) {
     __shared__ uint32_t h[8][256];
     for (int k = threadIdx.x; k < 8 * 256; k += kSortThreads) (&h[0][0])[k] = 0;
     __syncthreads();
-    const int lane = threadIdx.x & 31;
-    // the loop test uses the warp's first index so the whole warp iterates
-    // together (__match_any_sync needs every lane)
-    for (int64_t i = blockIdx.x * (int64_t)kSortThreads + threadIdx.x; i - lane < n;
-         i += (int64_t)gridDim.x * kSortThreads) {
-        const bool valid = i < n;
-        const uint64_t k = valid ? __ldg(key + i) : 0ull;
+    const int64_t stride = (int64_t)gridDim.x * kSortThreads * kHistRun;
+    for (int64_t first = ((int64_t)blockIdx.x * kSortThreads + threadIdx.x) * kHistRun; first < n;
+         first += stride) {
+        const int cnt = (int)min((int64_t)kHistRun, n - first);
+        uint64_t prev = __ldg(key + first);
+        uint32_t run[8];
 #pragma unroll
-        for (int d = 0; d < 8; ++d) {
-            const uint32_t dig = valid ? (uint32_t)((k >> (8 * d)) & 0xFF) : 0x100u + lane;
-            const unsigned peers = __match_any_sync(kFull, dig);
-            if (valid && lane == __ffs(peers) - 1) atomicAdd(&h[d][dig], (uint32_t)__popc(peers));
+        for (int d = 0; d < 8; ++d) run[d] = 1;
+        for (int j = 1; j < cnt; ++j) {
+            const uint64_t k = __ldg(key + first + j);
+#pragma unroll
+            for (int d = 0; d < 8; ++d) {
+                const uint32_t a = (uint32_t)(prev >> (8 * d)) & 0xFF;
+                const uint32_t b = (uint32_t)(k >> (8 * d)) & 0xFF;
+                if (a != b) {
+                    atomicAdd(&h[d][a], run[d]);
+                    run[d] = 1;
+                } else {
+                    ++run[d];
+                }
+            }
+            prev = k;
         }
+#pragma unroll
+        for (int d = 0; d < 8; ++d) atomicAdd(&h[d][(uint32_t)(prev >> (8 * d)) & 0xFF], run[d]);
     }
     __syncthreads();
     for (int k = threadIdx.x; k < 8 * 256; k += kSortThreads) {
         const uint32_t v = (&h[0][0])[k];
         if (v) atomicAdd(hist + k, v);
     }
+}
+
+// Lanes holding the same 8-bit digit, from eight ballots (the ballot path
+// keeps this off the pipe that serialises __match_any_sync).
+__device__ __forceinline__ unsigned digit_peers(uint32_t d, bool valid) {
+    unsigned peers = __ballot_sync(kFull, valid);
+    if (!valid) peers = 0;
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+        const bool bit = (d >> b) & 1u;
+        const unsigned m = __ballot_sync(kFull, bit);
+        peers &= bit ? m : ~m;
+    }
+    return valid ? peers : (1u << (threadIdx.x & 31));
 }
 
 // Exclusive scan of each digit position's 256 bins (block d = position d).
@@ -390,8 +422,8 @@ onesweep_pass(const uint64_t* __restrict__ key_in, const uint32_t* __restrict__ 
         const bool valid = i < n;
         k_reg[k] = valid ? key_in[i] : 0ull;
         v_reg[k] = valid ? val_in[i] : 0u;
-        const uint32_t d = valid ? (uint32_t)((k_reg[k] >> shift) & 0xFF) : 0x100u + lane;
-        const unsigned peers = __match_any_sync(kFull, d);
+        const uint32_t d = (uint32_t)((k_reg[k] >> shift) & 0xFF);
+        const unsigned peers = digit_peers(d, valid);
         const int leader = __ffs(peers) - 1;
         uint32_t b = 0;
         if (valid && lane == leader) {

@@ -299,7 +299,7 @@ __global__ void tree_trivial_root(const double2* __restrict__ pos, const double*
 // multi-body leaf spans less than width / 2^30, so its own S is negligible).
 // Children are read with L2-coherent loads: they were written by other
 // threads of this launch (climb) or of an earlier launch (per level).
-template <bool kSplit>
+template <bool kSplit, bool kFeat>
 __device__ __forceinline__ void cell_moments(int id, const DeviceScalars* __restrict__ s,
                                              const double2* __restrict__ pos,
                                              const double* __restrict__ mass, const Tree& t) {
@@ -358,6 +358,50 @@ __device__ __forceinline__ void cell_moments(int id, const DeviceScalars* __rest
         double2* so = reinterpret_cast<double2*>(t.s64 + id);
         __stcg(so, make_double2(sxx, sxy));
         __stcg(so + 1, make_double2(syy, 0.0));
+        if (kFeat) {
+            // Third moments T_ijk about the COM, by the same shift rule
+            // (u = u_child + d):
+            //   T += T_c + (d_i S_c,jk + d_j S_c,ik + d_k S_c,ij) + m d_i d_j d_k
+            double txxx = 0.0, txxy = 0.0, txyy = 0.0, tyyy = 0.0, mmax = 0.0;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int r = refs[q];
+                if (r == INT_MIN) continue;
+                const double m = cm[q];
+                mmax = fmax(mmax, m);
+                const double dx = cmx[q] - com.x, dy = cmy[q] - com.y;
+                double cxx = 0.0, cxy = 0.0, cyy = 0.0;
+                double c3[4] = {0.0, 0.0, 0.0, 0.0};
+                if (r >= 0) {
+                    const double2* sc = reinterpret_cast<const double2*>(t.s64 + r);
+                    const double2 s01 = __ldcg(sc), s2 = __ldcg(sc + 1);
+                    cxx = s01.x;
+                    cxy = s01.y;
+                    cyy = s2.x;
+                    const double2* tc = reinterpret_cast<const double2*>(t.t64 + r);
+                    const double2 t01 = __ldcg(tc), t23 = __ldcg(tc + 1);
+                    c3[0] = t01.x;
+                    c3[1] = t01.y;
+                    c3[2] = t23.x;
+                    c3[3] = t23.y;
+                }
+                txxx += c3[0] + 3.0 * dx * cxx + m * dx * dx * dx;
+                txxy += c3[1] + 2.0 * dx * cxy + dy * cxx + m * dx * dx * dy;
+                txyy += c3[2] + dx * cyy + 2.0 * dy * cxy + m * dx * dy * dy;
+                tyyy += c3[3] + 3.0 * dy * cyy + m * dy * dy * dy;
+            }
+            double2* to = reinterpret_cast<double2*>(t.t64 + id);
+            __stcg(to, make_double2(txxx, txxy));
+            __stcg(to + 1, make_double2(txyy, tyyy));
+            // the MLP's cell features, normalised by M and the cell width
+            const double w2 = s->wsq[t.level[id]], w = sqrt(w2);
+            const double im2 = 1.0 / (M * w2), im3 = im2 / w;
+            t.cellf[3 * id + 0] = make_float4((float)(mmax / M), (float)(sxx * im2),
+                                              (float)(sxy * im2), (float)(syy * im2));
+            t.cellf[3 * id + 1] = make_float4((float)(txxx * im3), (float)(txxy * im3),
+                                              (float)(txyy * im3), (float)(tyyy * im3));
+            t.cellf[3 * id + 2] = make_float4(0.f, (float)w, 0.f, 0.f);
+        }
         t.cell4[id] = make_float4((float)(com.x - s->center[0]), (float)(com.y - s->center[1]),
                                   (float)M, (float)s->wsq[t.level[id]]);
         t.cellq[id] = make_float4((float)sxx, (float)sxy, (float)syy, 0.f);
@@ -366,7 +410,7 @@ __device__ __forceinline__ void cell_moments(int id, const DeviceScalars* __rest
 
 // Bottom-up pass: threads start at cells without internal children and
 // climb; the last child to arrive at a parent (atomic counter) computes it.
-template <bool kSplit>
+template <bool kSplit, bool kFeat>
 __global__ void tree_moments(DeviceScalars* __restrict__ s, const double2* __restrict__ pos,
                              const double* __restrict__ mass, Tree t) {
     int id = blockIdx.x * blockDim.x + threadIdx.x;
@@ -379,7 +423,7 @@ __global__ void tree_moments(DeviceScalars* __restrict__ s, const double2* __res
             atomicOr(&s->error, kErrTree);
             return;
         }
-        cell_moments<kSplit>(id, s, pos, mass, t);
+        cell_moments<kSplit, kFeat>(id, s, pos, mass, t);
         __threadfence();
         const int par = t.parent[id];
         if (par < 0) return;
@@ -505,13 +549,17 @@ void launch_tree(nb_ctx* c, const BodyBuffers& b) {
 void launch_moments(nb_ctx* c, const BodyBuffers& b, bool split) {
     // Cells never exceed n - 1; threads beyond the live count exit at once.
     const int cap = (int)(c->n > 1 ? c->n - 1 : 1);
+    const bool feat = split && c->tree.cellf != nullptr;
     c->launches += 1;
-    if (split)
-        tree_moments<true><<<blocks_for(cap, kThreads), kThreads, 0, c->stream>>>(c->scal, b.pos,
-                                                                                  b.mass, c->tree);
+    const unsigned blocks = blocks_for(cap, kThreads);
+    if (feat)
+        tree_moments<true, true><<<blocks, kThreads, 0, c->stream>>>(c->scal, b.pos, b.mass, c->tree);
+    else if (split)
+        tree_moments<true, false><<<blocks, kThreads, 0, c->stream>>>(c->scal, b.pos, b.mass,
+                                                                      c->tree);
     else
-        tree_moments<false><<<blocks_for(cap, kThreads), kThreads, 0, c->stream>>>(c->scal, b.pos,
-                                                                                   b.mass, c->tree);
+        tree_moments<false, false><<<blocks, kThreads, 0, c->stream>>>(c->scal, b.pos, b.mass,
+                                                                       c->tree);
 }
 
 }  // namespace nb

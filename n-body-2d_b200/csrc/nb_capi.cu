@@ -12,6 +12,8 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <vector>
+#include <algorithm>
 
 #include "nb_internal.cuh"
 
@@ -48,7 +50,9 @@ int check_params(const nb_params* p) {
         return NB_ERR_INVALID;
     if (p->theta < 0.0 || p->epsilon_squared < 0.0) return NB_ERR_INVALID;
     if (p->mode != NB_MODE_FP64 && p->mode != NB_MODE_SPLIT) return NB_ERR_INVALID;
-    if (p->leaf_size < 0 || (p->flags & ~(int32_t)NB_FLAG_QUADRUPOLE) != 0) return NB_ERR_INVALID;
+    if (p->leaf_size < 0 || (p->flags & ~(int32_t)(NB_FLAG_QUADRUPOLE | NB_FLAG_LEARNED)) != 0)
+        return NB_ERR_INVALID;
+    if ((p->flags & NB_FLAG_LEARNED) && p->mode != NB_MODE_SPLIT) return NB_ERR_INVALID;
     return NB_OK;
 }
 
@@ -90,6 +94,14 @@ int alloc_all(nb_ctx* c) {
         NB_CUDA(c, dalloc(&t.gbase, n));
         NB_CUDA(c, dalloc(&t.groups, n));
     }
+    if (c->p.flags & NB_FLAG_LEARNED) {
+        NB_CUDA(c, dalloc(&t.t64, n));
+        NB_CUDA(c, dalloc(&t.cellf, 3 * n));
+        NB_CUDA(c, dalloc(&t.band, (size_t)nb::kBandPerBody * n));
+        NB_CUDA(c, dalloc(&t.band_count, n));
+        NB_CUDA(c, dalloc(&c->acc32, n));
+        NB_CUDA(c, dalloc(&c->mlp_params, NB_MLP_PARAMS));
+    }
     NB_CUDA(c, dalloc(&t.leaf_last, n));
     NB_CUDA(c, dalloc(&t.leaf_plevel, n));
     NB_CUDA(c, dalloc(&t.bucket_mass, n));
@@ -128,13 +140,16 @@ void free_all(nb_ctx* c) {
                          t.nint,      t.ready,       t.mass,        t.com,        t.leaf_last,
                          t.leaf_plevel, t.bucket_mass, t.bucket_com, t.flag,      t.cell_of,
                          t.start_of,  t.range,       t.s64,         t.cell4,      t.cellq,
-                         t.body4,     t.gcount,      t.gbase,       t.groups,     t.rep_of};
+                         t.body4,     t.gcount,      t.gbase,       t.groups,     t.rep_of,
+                         t.t64,       t.cellf,       t.band,        t.band_count};
     for (void* q : tree_ptrs) cudaFree(q);
     cudaFree(c->scal);
     cudaFree(c->bbox_partials);
     cudaFree(c->acc);
     cudaFree(c->stage_pos);
     cudaFree(c->stage_vel);
+    cudaFree(c->acc32);
+    cudaFree(c->mlp_params);
 }
 
 void drop_graphs(nb_ctx* c) {
@@ -145,6 +160,8 @@ void drop_graphs(nb_ctx* c) {
         }
 }
 
+// "drift": the FP64 drift kernel; in learned mode the correction kernel, which
+// also kicks and drifts (plain SPLIT fuses both into the force kernel).
 const char* const kPhaseNames[nb::kPhases] = {"bbox+morton", "sort", "gather", "tree",
                                               "moments", "groups", "force", "drift"};
 
@@ -175,7 +192,11 @@ void enqueue_step(nb_ctx* c, int parity, bool integrate, bool store_acc, bool ti
     mark(5);
     if (split) nb::launch_groups(c);
     mark(6);
-    if (split) {
+    if (split && (c->p.flags & NB_FLAG_LEARNED)) {
+        nb::launch_force_split(c, B, integrate, store_acc);  // FP32 accelerations + band lists
+        mark(7);
+        nb::launch_mlp_correct(c, B, integrate, store_acc);  // learned term, kick, drift
+    } else if (split) {
         nb::launch_force_split(c, B, integrate, store_acc);  // kick and drift fused
         mark(7);
     } else {
@@ -222,6 +243,36 @@ struct DeviceGuard {
     ~DeviceGuard() {
         if (prev >= 0) cudaSetDevice(prev);
     }
+};
+
+}  // namespace
+
+namespace {
+
+struct DeviceScope {
+    int prev = -1;
+    int rc = NB_OK;
+    explicit DeviceScope(int dev) {
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || dev < 0 || dev >= ndev) {
+            rc = NB_ERR_NOTFOUND;
+            return;
+        }
+        cudaGetDevice(&prev);
+        cudaSetDevice(dev);
+    }
+    ~DeviceScope() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+template <typename T>
+struct DBuf {
+    T* p = nullptr;
+    explicit DBuf(size_t count) {
+        if (cudaMalloc(&p, sizeof(T) * (count ? count : 1)) != cudaSuccess) p = nullptr;
+    }
+    ~DBuf() { cudaFree(p); }
 };
 
 }  // namespace
@@ -334,6 +385,8 @@ int nb_set_timestep(nb_ctx* c, double dt) {
 int nb_step(nb_ctx* c, uint32_t nsteps) {
     if (!c) return NB_ERR_INVALID;
     if (nsteps == 0) return NB_OK;
+    if ((c->p.flags & NB_FLAG_LEARNED) && !c->mlp_ready)
+        return fail(c, NB_ERR_INVALID, "learned mode: call nb_set_mlp_weights first");
     DeviceGuard guard(c->device);
     for (int par = 0; par < 2; ++par)
         if (!c->graph[par]) {
@@ -381,6 +434,8 @@ int nb_download(nb_ctx* c, double* pos_xy, double* vel_xy) {
 
 int nb_accelerations(nb_ctx* c, double* acc_xy) {
     if (!c || !acc_xy) return NB_ERR_INVALID;
+    if ((c->p.flags & NB_FLAG_LEARNED) && !c->mlp_ready)
+        return fail(c, NB_ERR_INVALID, "learned mode: call nb_set_mlp_weights first");
     DeviceGuard guard(c->device);
     enqueue_step(c, c->parity, false, true);
     NB_CUDA(c, cudaGetLastError());
@@ -476,5 +531,203 @@ int nb_phase_times(nb_ctx* c, double* ms, int max) {
 }
 
 const char* nb_phase_name(int k) { return k >= 0 && k < nb::kPhases ? kPhaseNames[k] : ""; }
+
+int nb_set_mlp_weights(nb_ctx* c, const float* params) {
+    if (!c || !params) return NB_ERR_INVALID;
+    if (!(c->p.flags & NB_FLAG_LEARNED))
+        return fail(c, NB_ERR_INVALID, "context was not created with NB_FLAG_LEARNED");
+    for (int k = 0; k < NB_MLP_PARAMS; ++k)
+        if (!std::isfinite(params[k])) return fail(c, NB_ERR_INVALID, "non-finite MLP parameter");
+    DeviceGuard guard(c->device);
+    NB_CUDA(c, cudaMemcpyAsync(c->mlp_params, params, sizeof(float) * NB_MLP_PARAMS,
+                               cudaMemcpyHostToDevice, c->stream));
+    NB_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->mlp_ready = true;
+    return NB_OK;
+}
+
+int nb_mlp_samples(nb_ctx* c, uint64_t ntargets, uint64_t seed, uint64_t capacity, float* features,
+                   float* residuals, uint64_t* count) {
+    if (!c || !features || !residuals || !count || ntargets == 0 || capacity == 0)
+        return NB_ERR_INVALID;
+    if (!(c->p.flags & NB_FLAG_LEARNED))
+        return fail(c, NB_ERR_INVALID, "context was not created with NB_FLAG_LEARNED");
+    if (capacity > 0xffffffffull || ntargets > (uint64_t)INT32_MAX) return NB_ERR_INVALID;
+    DeviceGuard guard(c->device);
+    // sorted bodies, tree and moments of the current state, without integrating
+    const nb::BodyBuffers& A = c->buf[c->parity];
+    const nb::BodyBuffers& B = c->buf[c->parity ^ 1];
+    nb::launch_bbox(c, A.pos);
+    nb::launch_morton(c, A.pos);
+    nb::launch_sort(c);
+    nb::launch_gather(c, A, B, c->tree.body4);
+    nb::launch_tree(c, B);
+    nb::launch_moments(c, B, true);
+    NB_CUDA(c, cudaGetLastError());
+    c->parity ^= 1;
+    // targets: a seeded uniform choice of body slots (splitmix64)
+    std::vector<int> slots(ntargets);
+    uint64_t z = seed + 0x9e3779b97f4a7c15ull;
+    for (auto& sl : slots) {
+        z += 0x9e3779b97f4a7c15ull;
+        uint64_t x = z;
+        x = (x ^ (x >> 30)) * 0xbf58476d1ce4e5b9ull;
+        x = (x ^ (x >> 27)) * 0x94d049bb133111ebull;
+        x ^= x >> 31;
+        sl = (int)(x % (uint64_t)c->n);
+    }
+    int* dslots = nullptr;
+    float *dX = nullptr, *dY = nullptr;
+    unsigned* dcount = nullptr;
+    int rc = NB_OK;
+    if (cudaMalloc(&dslots, sizeof(int) * ntargets) != cudaSuccess ||
+        cudaMalloc(&dX, sizeof(float) * 12 * capacity) != cudaSuccess ||
+        cudaMalloc(&dY, sizeof(float) * 2 * capacity) != cudaSuccess ||
+        cudaMalloc(&dcount, sizeof(unsigned)) != cudaSuccess)
+        rc = fail(c, NB_ERR_NOMEM, "sample buffers");
+    unsigned hcount = 0;
+    if (rc == NB_OK) {
+        cudaMemcpyAsync(dslots, slots.data(), sizeof(int) * ntargets, cudaMemcpyHostToDevice,
+                        c->stream);
+        cudaMemsetAsync(dcount, 0, sizeof(unsigned), c->stream);
+        nb::launch_mlp_samples(c, B, dslots, (int)ntargets, dX, dY, dcount, (unsigned)capacity);
+        cudaMemcpyAsync(&hcount, dcount, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream);
+        if (cudaStreamSynchronize(c->stream) != cudaSuccess)
+            rc = fail(c, NB_ERR_CUDA, "sample kernel failed");
+    }
+    if (rc == NB_OK) {
+        const uint64_t rows = hcount < capacity ? hcount : capacity;
+        cudaMemcpy(features, dX, sizeof(float) * 12 * rows, cudaMemcpyDeviceToHost);
+        cudaMemcpy(residuals, dY, sizeof(float) * 2 * rows, cudaMemcpyDeviceToHost);
+        *count = rows;
+    }
+    cudaFree(dslots);
+    cudaFree(dX);
+    cudaFree(dY);
+    cudaFree(dcount);
+    if (rc == NB_OK) rc = read_device_error(c);
+    return rc;
+}
+
+int nb_mlp_forward(int32_t device, const float* params, uint64_t n, const float* features,
+                   float* out) {
+    if (!params || !features || !out || n == 0) return NB_ERR_INVALID;
+    DeviceScope scope(device);
+    if (scope.rc != NB_OK) return scope.rc;
+    DBuf<float> p(NB_MLP_PARAMS), x(12 * n), y(2 * n);
+    if (!p.p || !x.p || !y.p) return NB_ERR_NOMEM;
+    cudaMemcpy(p.p, params, sizeof(float) * NB_MLP_PARAMS, cudaMemcpyHostToDevice);
+    cudaMemcpy(x.p, features, sizeof(float) * 12 * n, cudaMemcpyHostToDevice);
+    if (nb::mlp_forward_device(p.p, x.p, (int64_t)n, y.p, nullptr) != NB_OK) return NB_ERR_CUDA;
+    if (cudaMemcpy(out, y.p, sizeof(float) * 2 * n, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return NB_ERR_CUDA;
+    return NB_OK;
+}
+
+int nb_mlp_loss_grad(int32_t device, const float* params, uint64_t n, const float* features,
+                     const float* targets, float* grad, float* loss) {
+    if (!params || !features || !targets || !grad || !loss || n == 0) return NB_ERR_INVALID;
+    DeviceScope scope(device);
+    if (scope.rc != NB_OK) return scope.rc;
+    DBuf<float> p(NB_MLP_PARAMS), x(12 * n), y(2 * n), g(NB_MLP_PARAMS), l(1);
+    if (!p.p || !x.p || !y.p || !g.p || !l.p) return NB_ERR_NOMEM;
+    cudaMemcpy(p.p, params, sizeof(float) * NB_MLP_PARAMS, cudaMemcpyHostToDevice);
+    cudaMemcpy(x.p, features, sizeof(float) * 12 * n, cudaMemcpyHostToDevice);
+    cudaMemcpy(y.p, targets, sizeof(float) * 2 * n, cudaMemcpyHostToDevice);
+    cudaMemset(g.p, 0, sizeof(float) * NB_MLP_PARAMS);
+    cudaMemset(l.p, 0, sizeof(float));
+    const int blocks = (int)std::min<uint64_t>((n + 63) / 64, 592);
+    if (nb::mlp_grad_device(p.p, x.p, y.p, nullptr, (int64_t)n, g.p, l.p, blocks, nullptr) != NB_OK)
+        return NB_ERR_CUDA;
+    if (cudaMemcpy(grad, g.p, sizeof(float) * NB_MLP_PARAMS, cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(loss, l.p, sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return NB_ERR_CUDA;
+    return NB_OK;
+}
+
+int nb_mlp_train(int32_t device, uint64_t n, const float* features, const float* residuals,
+                 const nb_mlp_train_params* tp, float* params, float* loss_per_epoch) {
+    if (!features || !residuals || !tp || !params || n == 0 || tp->batch == 0 || tp->epochs == 0 ||
+        !(tp->lr > 0.f))
+        return NB_ERR_INVALID;
+    DeviceScope scope(device);
+    if (scope.rc != NB_OK) return scope.rc;
+    // host-side set-up: output scale and seeded initialisation
+    std::vector<float> P(params, params + NB_MLP_PARAMS);
+    bool all_zero = true;
+    for (int k = 0; k < NB_MLP_PARAMS - 1; ++k) all_zero = all_zero && P[k] == 0.f;
+    uint64_t z = tp->seed * 0x9e3779b97f4a7c15ull + 1;
+    auto uniform = [&z]() {
+        z += 0x9e3779b97f4a7c15ull;
+        uint64_t x = z;
+        x = (x ^ (x >> 30)) * 0xbf58476d1ce4e5b9ull;
+        x = (x ^ (x >> 27)) * 0x94d049bb133111ebull;
+        x ^= x >> 31;
+        return (double)(x >> 11) * (1.0 / 9007199254740992.0);
+    };
+    if (all_zero) {  // uniform(-a, a), a = sqrt(6 / (fan_in + fan_out))
+        const int w1 = 0, w2 = 64 * 12 + 64, w3 = w2 + 64 * 64 + 64;
+        const double a1 = std::sqrt(6.0 / (12 + 64)), a2 = std::sqrt(6.0 / 128.0),
+                     a3 = std::sqrt(6.0 / 66.0);
+        for (int k = 0; k < 64 * 12; ++k) P[w1 + k] = (float)((2 * uniform() - 1) * a1);
+        for (int k = 0; k < 64 * 64; ++k) P[w2 + k] = (float)((2 * uniform() - 1) * a2);
+        for (int k = 0; k < 2 * 64; ++k) P[w3 + k] = (float)((2 * uniform() - 1) * a3);
+    }
+    if (!(P[NB_MLP_PARAMS - 1] > 0.f)) {
+        double ss = 0.0;
+        for (uint64_t k = 0; k < 2 * n; ++k) ss += (double)residuals[k] * residuals[k];
+        P[NB_MLP_PARAMS - 1] = (float)std::sqrt(ss / (2.0 * n) + 1e-30);
+    }
+    const float inv_scale = 1.f / P[NB_MLP_PARAMS - 1];
+    std::vector<float> T(2 * n);
+    for (uint64_t k = 0; k < 2 * n; ++k) T[k] = residuals[k] * inv_scale;
+    DBuf<float> p(NB_MLP_PARAMS), x(12 * n), y(2 * n), g(NB_MLP_PARAMS), m(NB_MLP_PARAMS),
+        v(NB_MLP_PARAMS), l(1);
+    DBuf<int64_t> idx(n);
+    if (!p.p || !x.p || !y.p || !g.p || !m.p || !v.p || !l.p || !idx.p) return NB_ERR_NOMEM;
+    cudaStream_t st = nullptr;
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return NB_ERR_CUDA;
+    cudaMemcpyAsync(p.p, P.data(), sizeof(float) * NB_MLP_PARAMS, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(x.p, features, sizeof(float) * 12 * n, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(y.p, T.data(), sizeof(float) * 2 * n, cudaMemcpyHostToDevice, st);
+    cudaMemsetAsync(m.p, 0, sizeof(float) * NB_MLP_PARAMS, st);
+    cudaMemsetAsync(v.p, 0, sizeof(float) * NB_MLP_PARAMS, st);
+    std::vector<int64_t> perm(n);
+    for (uint64_t k = 0; k < n; ++k) perm[k] = (int64_t)k;
+    int rc = NB_OK;
+    int step = 0;
+    const uint64_t B = tp->batch;
+    for (uint32_t e = 0; e < tp->epochs && rc == NB_OK; ++e) {
+        for (uint64_t k = n - 1; k > 0; --k) {  // Fisher-Yates
+            const uint64_t j = (uint64_t)(uniform() * (double)(k + 1)) % (k + 1);
+            std::swap(perm[k], perm[j]);
+        }
+        cudaMemcpyAsync(idx.p, perm.data(), sizeof(int64_t) * n, cudaMemcpyHostToDevice, st);
+        cudaMemsetAsync(l.p, 0, sizeof(float), st);
+        uint64_t nbatches = 0;
+        for (uint64_t b0 = 0; b0 < n; b0 += B, ++nbatches) {
+            const uint64_t cnt = std::min<uint64_t>(B, n - b0);
+            cudaMemsetAsync(g.p, 0, sizeof(float) * NB_MLP_PARAMS, st);
+            const int blocks = (int)std::min<uint64_t>((cnt + 63) / 64, 592);
+            if (nb::mlp_grad_device(p.p, x.p, y.p, idx.p + b0, (int64_t)cnt, g.p, l.p, blocks, st) !=
+                    NB_OK ||
+                nb::mlp_adam_device(p.p, g.p, m.p, v.p, tp->lr, ++step, st) != NB_OK) {
+                rc = NB_ERR_CUDA;
+                break;
+            }
+        }
+        float lsum = 0.f;
+        cudaMemcpyAsync(&lsum, l.p, sizeof(float), cudaMemcpyDeviceToHost, st);
+        if (cudaStreamSynchronize(st) != cudaSuccess) rc = NB_ERR_CUDA;
+        if (loss_per_epoch) loss_per_epoch[e] = lsum / (float)nbatches;
+    }
+    if (rc == NB_OK) {
+        cudaMemcpyAsync(P.data(), p.p, sizeof(float) * (NB_MLP_PARAMS - 1), cudaMemcpyDeviceToHost, st);
+        if (cudaStreamSynchronize(st) != cudaSuccess) rc = NB_ERR_CUDA;
+        else std::memcpy(params, P.data(), sizeof(float) * NB_MLP_PARAMS);
+    }
+    cudaStreamDestroy(st);
+    return rc;
+}
 
 }  // extern "C"

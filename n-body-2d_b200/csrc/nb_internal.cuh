@@ -18,6 +18,8 @@ constexpr int kSortTileItems = 8; // keys per thread in a radix tile
 constexpr int kSortThreads = 256;
 constexpr int kSortTile = kSortTileItems * kSortThreads;  // 2048 keys
 constexpr int kPhases = 8;        // morton, sort, gather, tree, moments, groups, force, drift
+constexpr float kThetaBand = 0.5f; // learned mode: cells the plain 0.5 walk would open get the MLP
+constexpr int kBandPerBody = 16;   // learned mode: band-list capacity per body of a group
 
 // Device error flags (bit mask in DeviceScalars::error).
 constexpr unsigned kErrStack = 1u;      // DFS stack bound exceeded
@@ -65,6 +67,12 @@ struct Tree {
     float4* cell4 = nullptr;     // {com_x - cx, com_y - cy, mass, width^2}
     float4* cellq = nullptr;     // {Sxx, Sxy, Syy, 0}
     float4* body4 = nullptr;     // per body {x - cx, y - cy, mass, index bits}
+    // learned correction: third moments (FP64, bottom-up) and the
+    // packed per-cell MLP features (3 float4 per cell, see k_mlp.cu)
+    double4* t64 = nullptr;      // {Txxx, Txxy, Txyy, Tyyy}
+    float4* cellf = nullptr;
+    int32_t* band = nullptr;       // per group: band cells, kBandPerBody x first body onwards
+    int32_t* band_count = nullptr; // per group: band cells found
     // SPLIT target groups: <= split_group_size() Morton-consecutive bodies in one
     // parent cell (merged sibling cells/leaves), stored as body ranges
     int32_t* gcount = nullptr;   // groups each cell emits
@@ -116,7 +124,10 @@ struct nb_ctx {
     nb::DeviceScalars* scal = nullptr;   // device
     double* bbox_partials = nullptr;     // [blocks][4]
     int bbox_blocks = 0;
-    int split_blocks = 0;                // persistent grid of the SPLIT traversal
+    int split_blocks[4] = {0, 0, 0, 0};  // persistent grids of the SPLIT traversal variants
+    float* mlp_params = nullptr;         // learned mode: FP32 MLP parameters (device)
+    bool mlp_ready = false;
+    float2* acc32 = nullptr;             // learned mode: traversal accelerations
     double2* acc = nullptr;              // optional FP64 accelerations (sorted order)
     double2* stage_pos = nullptr;        // original-order staging for downloads
     double2* stage_vel = nullptr;
@@ -140,6 +151,14 @@ void launch_gather(nb_ctx* c, const BodyBuffers& src, const BodyBuffers& dst, fl
 void launch_tree(nb_ctx* c, const BodyBuffers& b);
 void launch_moments(nb_ctx* c, const BodyBuffers& b, bool split);
 int split_group_size(const nb_ctx* c);   // bodies per SPLIT traversal group
+void launch_mlp_correct(nb_ctx* c, const BodyBuffers& b, bool kick, bool store_acc);
+void launch_mlp_samples(nb_ctx* c, const BodyBuffers& b, const int* slots, int nslots, float* X,
+                        float* Y, unsigned* count, unsigned cap);
+int mlp_forward_device(const float* params, const float* X, int64_t n, float* Y, cudaStream_t st);
+int mlp_grad_device(const float* params, const float* X, const float* Yt, const int64_t* idx,
+                    int64_t n, float* grad, float* loss, int blocks, cudaStream_t st);
+int mlp_adam_device(float* p, const float* g, float* m, float* v, float lr, int step,
+                    cudaStream_t st);
 void launch_groups(nb_ctx* c);
 void launch_force_split(nb_ctx* c, const BodyBuffers& b, bool kick, bool store_acc);
 void launch_force_fp64(nb_ctx* c, const BodyBuffers& b, bool kick, bool store_acc);

@@ -67,6 +67,7 @@ class SimConfig:
     leaf_size: int = 0
     device: int = 0
     quadrupole: bool = False
+    learned: bool = False
 
     def params(self) -> NbParams:
         p = NbParams()
@@ -78,7 +79,8 @@ class SimConfig:
         p.mode = self.mode
         p.leaf_size = self.leaf_size
         p.device = self.device
-        p.flags = _lib.NB_FLAG_QUADRUPOLE if self.quadrupole else 0
+        p.flags = ((_lib.NB_FLAG_QUADRUPOLE if self.quadrupole else 0)
+                   | (_lib.NB_FLAG_LEARNED if self.learned else 0))
         return p
 
 
@@ -192,6 +194,23 @@ class NbContext:
             check(-k, self._h)
         return {self._lib.nb_phase_name(i).decode(): float(ms[i]) for i in range(k)}
 
+    # -- learned correction -----------------------------------------------
+    def set_mlp_weights(self, params: np.ndarray) -> None:
+        params = np.ascontiguousarray(params, dtype=np.float32)
+        if params.shape != (_lib.NB_MLP_PARAMS,):
+            raise ValueError(f"expected {_lib.NB_MLP_PARAMS} parameters")
+        check(self._lib.nb_set_mlp_weights(self.handle, ptr(params)), self._h)
+
+    def mlp_samples(self, ntargets: int, seed: int = 0, capacity: int | None = None):
+        """Residual samples (features[k,12], residuals[k,2]) of the current bodies."""
+        capacity = capacity or 256 * ntargets
+        X = np.empty((capacity, 12), dtype=np.float32)
+        Y = np.empty((capacity, 2), dtype=np.float32)
+        cnt = C.c_uint64()
+        check(self._lib.nb_mlp_samples(self.handle, ntargets, seed, capacity, ptr(X), ptr(Y),
+                                       C.byref(cnt)), self._h)
+        return X[:cnt.value], Y[:cnt.value]
+
     def stats(self) -> NbStats:
         s = NbStats()
         check(self._lib.nb_get_stats(self.handle, C.byref(s)), self._h)
@@ -209,6 +228,43 @@ def allpairs_accelerations(mass, pos, targets, epsilon_squared: float, device: i
     check(lib.nb_allpairs_accelerations(device, n, ptr(mass), ptr(pos), tgt.shape[0], ptr(tgt),
                                         epsilon_squared, ptr(acc)))
     return acc
+
+
+def mlp_forward(params, features, device: int = 0) -> np.ndarray:
+    """Raw network outputs [n, 2] (without the output scale) on the GPU."""
+    lib = load()
+    params = np.ascontiguousarray(params, dtype=np.float32)
+    X = np.ascontiguousarray(features, dtype=np.float32)
+    out = np.empty((X.shape[0], 2), dtype=np.float32)
+    check(lib.nb_mlp_forward(device, ptr(params), X.shape[0], ptr(X), ptr(out)))
+    return out
+
+
+def mlp_loss_grad(params, features, targets, device: int = 0):
+    """(mean squared error, gradient[NB_MLP_PARAMS]) on the GPU."""
+    lib = load()
+    params = np.ascontiguousarray(params, dtype=np.float32)
+    X = np.ascontiguousarray(features, dtype=np.float32)
+    T = np.ascontiguousarray(targets, dtype=np.float32)
+    grad = np.empty(_lib.NB_MLP_PARAMS, dtype=np.float32)
+    loss = np.zeros(1, dtype=np.float32)
+    check(lib.nb_mlp_loss_grad(device, ptr(params), X.shape[0], ptr(X), ptr(T), ptr(grad),
+                               ptr(loss)))
+    return float(loss[0]), grad
+
+
+def mlp_train(features, residuals, *, epochs: int = 4, batch: int = 4096, lr: float = 2e-3,
+              seed: int = 0, params=None, device: int = 0):
+    """Trains the correction MLP on the GPU; returns (params, loss per epoch)."""
+    lib = load()
+    X = np.ascontiguousarray(features, dtype=np.float32)
+    Y = np.ascontiguousarray(residuals, dtype=np.float32)
+    P = (np.zeros(_lib.NB_MLP_PARAMS, dtype=np.float32) if params is None
+         else np.array(params, dtype=np.float32))
+    losses = np.zeros(epochs, dtype=np.float32)
+    tp = _lib.NbMlpTrainParams(epochs=epochs, batch=batch, lr=lr, seed=seed)
+    check(lib.nb_mlp_train(device, X.shape[0], ptr(X), ptr(Y), C.byref(tp), ptr(P), ptr(losses)))
+    return P, losses
 
 
 class State(enum.Enum):
