@@ -351,9 +351,11 @@ def run_ours(args) -> None:
         "clocks": clk,
         "accuracy": accuracy,
     }
+    ctx.close()
+    if rank == 0 and args.variants:
+        line["variants"] = run_variants(args, nb, m, p, v, local, value, accuracy)
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.n, args.theta, m, p, v)
-    ctx.close()
     if world > 1:
         import torch.distributed as dist
 
@@ -361,6 +363,47 @@ def run_ours(args) -> None:
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def run_variants(args, nb, m, p, v, device, plain_value, plain_accuracy) -> dict:
+    """The learned theta = 1.0 step next to the plain theta = 0.5 one (same
+    workload, same timing method), plus the analytic-quadrupole and plain
+    theta = 1.0 walks, each with its p50/p99 force error against FP64
+    all-pairs.  The learned step falls back to plain theta = 0.5 when its p99
+    is worse than the plain step's (the judge of the learned mode)."""
+    from nbody_b200 import accuracy as acc_mod
+
+    weights = PKG / "weights" / "correction_theta1.npy"
+    out = {}
+    specs = [("mono_theta1.0", dict(theta=1.0)),
+             ("quad_theta0.7", dict(theta=0.7, quadrupole=True)),
+             ("quad_theta1.0", dict(theta=1.0, quadrupole=True))]
+    if weights.exists():
+        specs.insert(0, ("learned_theta1.0", dict(theta=1.0, learned=True)))
+    for name, kw in specs:
+        cfg = nb.SimConfig(timestep=1e-4, epsilon_squared=1e-4, G=1.0, mode=nb.NB_MODE_SPLIT,
+                           device=device, **kw)
+        with nb.NbContext(cfg, m, p, v) as ctx:
+            if kw.get("learned"):
+                ctx.set_mlp_weights(np.load(weights))
+            ctx.step(args.warmup)
+            ctx.step(args.steps, sync=False)
+            ctx.sync()
+            ms = ctx.stats().ms_last_step
+            phases = ctx.phase_times()
+            acc_now = ctx.accelerations()
+            pos_now, _ = ctx.download()
+        err = acc_mod.force_errors(acc_now, m, pos_now, 1e-4, k=args.error_sample, device=device)
+        val = args.n / (ms * 1e-3)
+        out[name] = {"value": val, "ms_per_step": ms, "speedup_vs_plain": val / plain_value,
+                     "p50": err["p50"], "p99": err["p99"],
+                     "force_ms": round(phases.get("force", 0.0), 4),
+                     "correction_ms": round(phases.get("drift", 0.0), 4)}
+    if "learned_theta1.0" in out and plain_accuracy:
+        lv = out["learned_theta1.0"]
+        lv["judge"] = ("kept" if lv["p99"] <= plain_accuracy["p99"]
+                       else "falls back to plain theta=0.5 (p99 above the plain step's)")
+    return out
 
 
 WORKLOADS = {
@@ -385,6 +428,8 @@ def main(argv=None):
     ap.add_argument("--leaf", type=int, default=0, help="SPLIT: direct-sum cell size (0=default)")
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--error-sample", type=int, default=65536)
+    ap.add_argument("--variants", action="store_true",
+                    help="also time the learned, quadrupole and plain theta=1.0 walks")
     args = ap.parse_args(argv)
     kind, n, theta = WORKLOADS[args.workload]
     args.kind = kind

@@ -184,12 +184,14 @@ typedef struct nb_mlp_train_params {
 /* Installs the MLP parameters (NB_MLP_PARAMS floats) into a learned context. */
 NB_API int nb_set_mlp_weights(nb_ctx* ctx, const float* params);
 
-/* Residual samples from the context's current bodies: for ntargets random
- * bodies, every cell accepted at the context's theta but opened at 0.5 gives
- * features[12] and the exact-minus-monopole residual[2] (units of M / d^2,
- * summed over the cell's bodies in FP64).  Features: (p - c)/d (2), w/d,
- * heaviest child's mass fraction, S/(M w^2) (3), T/(M w^3) (4),
- * eps^2/(d^2 + eps^2).  Host arrays of capacity rows;
+/* Residual samples from the context's current bodies, drawn the way the
+ * traversal uses the network: for ntargets random target groups, every cell
+ * the group accepts at the context's theta but would open at 0.5 gives
+ * features[12] at the group's centre and, as residual[2], the mean over the
+ * group's bodies of the exact-minus-monopole pull (FP64 sums over the cell's
+ * bodies) in units of M / d^2, d the centre's distance to the cell's COM.
+ * Features: (p - c)/d (2), w/d, heaviest child's mass fraction,
+ * S/(M w^2) (3), T/(M w^3) (4), eps^2/(d^2 + eps^2).  Host arrays of capacity rows;
  * *count receives the rows written. Does not change the bodies. */
 NB_API int nb_mlp_samples(nb_ctx* ctx, uint64_t ntargets, uint64_t seed, uint64_t capacity,
                           float* features, float* residuals, uint64_t* count);

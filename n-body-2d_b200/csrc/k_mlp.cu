@@ -114,7 +114,18 @@ __device__ __forceinline__ float bf16_round(float v) {
     return __bfloat162float(__float2bfloat16_rn(v));
 }
 
+// Hardware tanh (one MUFU op, relative error about 2^-11, below the BF16
+// rounding the activations get next); training and inference both use it.
+__device__ __forceinline__ float tanh_fast(float x) {
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 // Forward pass of one 16-row tile whose inputs are the A fragment `x`.
+// kKeep stores the BF16-rounded activations the backward pass needs; without
+// it the rounding happens once, in the conversion to the next A fragment.
+template <bool kKeep = true>
 __device__ __forceinline__ void mlp_forward(const MlpWeights& W, const uint32_t x[4], Fwd& f) {
     const int q = threadIdx.x & 3;
 #pragma unroll
@@ -125,7 +136,7 @@ __device__ __forceinline__ void mlp_forward(const MlpWeights& W, const uint32_t 
         load_b(&W.w1[0][0], 16, 8 * nt, 0, b0, b1);
         mma16816(c, x, b0, b1);
 #pragma unroll
-        for (int e = 0; e < 4; ++e) f.h1[nt][e] = bf16_round(tanhf(c[e]));
+        for (int e = 0; e < 4; ++e) f.h1[nt][e] = kKeep ? bf16_round(tanh_fast(c[e])) : tanh_fast(c[e]);
     }
     uint32_t a1[4][4];
 #pragma unroll
@@ -141,7 +152,7 @@ __device__ __forceinline__ void mlp_forward(const MlpWeights& W, const uint32_t 
             mma16816(c, a1[kt], b0, b1);
         }
 #pragma unroll
-        for (int e = 0; e < 4; ++e) f.h2[nt][e] = bf16_round(tanhf(c[e]));
+        for (int e = 0; e < 4; ++e) f.h2[nt][e] = kKeep ? bf16_round(tanh_fast(c[e])) : tanh_fast(c[e]);
     }
     uint32_t a2[4][4];
 #pragma unroll
@@ -466,23 +477,57 @@ __device__ __forceinline__ void mlp_features(float ux, float uy, float d, float 
 }
 
 // ---- residual samples (training data) ----------------------------------
-// One warp per target body: a depth-first walk with the per-body test at
-// theta_L; every cell accepted at theta_L but not at theta_B is a band cell
-// and yields one sample, its exact pull summed over its bodies in FP64.
+// Samples are drawn exactly as inference uses the network: one warp per target
+// group, the group's bounding box and acceptance tests in the traversal's FP32
+// arithmetic (cell accepted when it holds no body of the group and
+// w^2 < theta_L^2 d^2, band when also w^2 >= theta_B^2 d^2, d = distance from
+// the cell's COM to the box), and for every band cell one sample: the features
+// at the group's centre and, as target, the mean over the group's bodies of
+// the exact-minus-monopole pull (FP64 sums over the cell's bodies), in units
+// of M / d_c^2 with d_c the centre's distance.  That mean is the best single
+// correction for the whole group, which is what inference applies.
 constexpr int kSampleStack = 128;
 
 __global__ void __launch_bounds__(kWarps * 32)
 mlp_samples_kernel(Tree t, const DeviceScalars* __restrict__ s, const double2* __restrict__ pos,
-                   const double* __restrict__ mass, int n, const int* __restrict__ slots, int nslots,
-                   double thL2, double thB2, double eps2, float* __restrict__ X,
+                   const double* __restrict__ mass, int n, const int* __restrict__ pick, int npick,
+                   float thL2, float thB2, double eps2, float* __restrict__ X,
                    float* __restrict__ Y, unsigned* __restrict__ count, unsigned cap) {
     __shared__ int stacks[kWarps][kSampleStack];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int* stk = stacks[warp];
-    const int cells = s->cells;
-    for (int w = blockIdx.x * kWarps + warp; w < nslots; w += gridDim.x * kWarps) {
-        const int i = slots[w];
-        const double2 p = pos[i];
+    const int cells = s->cells, ngroups = s->groups;
+    const double cx = s->center[0], cy = s->center[1];
+    for (int w = blockIdx.x * kWarps + warp; w < npick; w += gridDim.x * kWarps) {
+        const int gi = pick[w] % max(ngroups, 1);
+        if (gi >= ngroups) continue;
+        const int2 gr = t.groups[gi];
+        const int g0 = gr.x, g1 = min(gr.y, n - 1);
+        const int nb = g1 - g0 + 1;
+        double2 P[2];
+        bool on[2];
+        float bx0 = INFINITY, bx1 = -INFINITY, by0 = INFINITY, by1 = -INFINITY;
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+            const int i = min(g0 + 32 * b + lane, g1);
+            on[b] = g0 + 32 * b + lane <= g1;
+            P[b] = pos[i];
+            if (on[b]) {
+                const float px = (float)(P[b].x - cx), py = (float)(P[b].y - cy);
+                bx0 = fminf(bx0, px);
+                bx1 = fmaxf(bx1, px);
+                by0 = fminf(by0, py);
+                by1 = fmaxf(by1, py);
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            bx0 = fminf(bx0, __shfl_xor_sync(kFull, bx0, o));
+            bx1 = fmaxf(bx1, __shfl_xor_sync(kFull, bx1, o));
+            by0 = fminf(by0, __shfl_xor_sync(kFull, by0, o));
+            by1 = fmaxf(by1, __shfl_xor_sync(kFull, by1, o));
+        }
+        const float gcx = 0.5f * (bx0 + bx1), gcy = 0.5f * (by0 + by1);
+        const float ghx = 0.5f * (bx1 - bx0), ghy = 0.5f * (by1 - by0);
         int top = 0;
         if (lane == 0) stk[0] = s->root;
         __syncwarp();
@@ -491,14 +536,13 @@ mlp_samples_kernel(Tree t, const DeviceScalars* __restrict__ s, const double2* _
             --top;
             __syncwarp();
             if (ref < 0 || ref >= cells) continue;  // leaves are summed exactly: no correction
-            const double M = t.mass[ref];
-            const double2 c = t.com[ref];
+            const float4 c4 = t.cell4[ref];
             const int2 rg = t.range[ref];
-            const double w2 = s->wsq[t.level[ref]];
-            const double ux = p.x - c.x, uy = p.y - c.y;
-            const double d2 = ux * ux + uy * uy;
-            const bool holds = rg.x <= i && i <= rg.y;
-            if (holds || !(w2 < thL2 * d2)) {
+            const bool overlap = !(rg.y < g0 || rg.x > g1);
+            const float dx = fmaxf(fabsf(c4.x - gcx) - ghx, 0.f);
+            const float dy = fmaxf(fabsf(c4.y - gcy) - ghy, 0.f);
+            const float d2 = fmaf(dx, dx, dy * dy);
+            if (overlap || !(c4.w < thL2 * d2)) {
                 const int4 ch = t.child[ref];
                 const int refs[4] = {ch.x, ch.y, ch.z, ch.w};
 #pragma unroll
@@ -510,35 +554,49 @@ mlp_samples_kernel(Tree t, const DeviceScalars* __restrict__ s, const double2* _
                 __syncwarp();
                 continue;
             }
-            if (!(w2 >= thB2 * d2)) continue;  // accepted by plain theta_B too
-            double ax = 0.0, ay = 0.0;
-            for (int j = rg.x + lane; j <= rg.y; j += 32) {
-                const double2 q = pos[j];
-                const double dx = q.x - p.x, dy = q.y - p.y;
-                const double r2 = dx * dx + dy * dy + eps2;
-                const double a = mass[j] / (r2 * sqrt(r2));
-                ax += dx * a;
-                ay += dy * a;
+            if (!(c4.w >= thB2 * d2)) continue;  // accepted by the plain theta_B walk too
+            // mean over the group's bodies of (exact - monopole), FP64
+            const double M = t.mass[ref];
+            const double2 c = t.com[ref];
+            double rx = 0.0, ry = 0.0;
+#pragma unroll
+            for (int b = 0; b < 2; ++b) {
+                if (!on[b]) continue;
+                double ax = 0.0, ay = 0.0;
+                for (int j = rg.x; j <= rg.y; ++j) {
+                    const double2 q = pos[j];
+                    const double ex = q.x - P[b].x, ey = q.y - P[b].y;
+                    const double r2 = ex * ex + ey * ey + eps2;
+                    const double a = mass[j] / (r2 * sqrt(r2));
+                    ax += ex * a;
+                    ay += ey * a;
+                }
+                const double mx = c.x - P[b].x, my = c.y - P[b].y;
+                const double r2 = mx * mx + my * my + eps2;
+                const double am = M / (r2 * sqrt(r2));
+                rx += ax - mx * am;
+                ry += ay - my * am;
             }
             for (int o = 16; o > 0; o >>= 1) {
-                ax += __shfl_xor_sync(kFull, ax, o);
-                ay += __shfl_xor_sync(kFull, ay, o);
+                rx += __shfl_xor_sync(kFull, rx, o);
+                ry += __shfl_xor_sync(kFull, ry, o);
             }
             if (lane == 0) {
-                const double r2 = d2 + eps2;
-                const double am = M / (r2 * sqrt(r2));
-                const double scale = d2 / M;
+                const float ux = gcx - c4.x, uy = gcy - c4.y;
+                const float dc2 = fmaxf(ux * ux + uy * uy, 1e-30f);
+                const double scale = (double)dc2 / (M * nb);
                 const unsigned slot = atomicAdd(count, 1u);
                 if (slot < cap) {
                     float x[kNin];
-                    mlp_features((float)ux, (float)uy, (float)sqrt(d2), (float)eps2,
-                                 t.cellf[3 * ref], t.cellf[3 * ref + 1], t.cellf[3 * ref + 2], x);
+                    mlp_features(ux, uy, sqrtf(dc2), (float)eps2, t.cellf[3 * ref],
+                                 t.cellf[3 * ref + 1], t.cellf[3 * ref + 2], x);
 #pragma unroll
                     for (int k = 0; k < kNin; ++k) X[(int64_t)slot * kNin + k] = x[k];
-                    Y[2 * (int64_t)slot] = (float)((ax - (-ux) * am) * scale);
-                    Y[2 * (int64_t)slot + 1] = (float)((ay - (-uy) * am) * scale);
+                    Y[2 * (int64_t)slot] = (float)(rx * scale);
+                    Y[2 * (int64_t)slot + 1] = (float)(ry * scale);
                 }
             }
+            __syncwarp();
         }
     }
 }
@@ -614,15 +672,18 @@ mlp_correct_kick(const float* __restrict__ params, Tree t, const DeviceScalars* 
 #pragma unroll
                     for (int k = 0; k < kNin; ++k) x[k] = 0.f;
                 }
+                uint32_t* row = reinterpret_cast<uint32_t*>(&S.x[warp][lane][0]);
 #pragma unroll
-                for (int k = 0; k < 16; ++k) S.x[warp][lane][k] = __float2bfloat16_rn(k < kNin ? x[k] : 0.f);
+                for (int k = 0; k < kNin; k += 2) row[k / 2] = pack_bf16(x[k], x[k + 1]);
+                row[6] = 0u;
+                row[7] = 0u;
                 S.scale[warp][lane][0] = sc;
             }
             __syncwarp();
             uint32_t a[4];
             load_a(&S.x[warp][0][0], 16, 0, a);
             Fwd f;
-            mlp_forward(S.W, a, f);
+            mlp_forward<false>(S.W, a, f);
             if (q == 0) {
                 cxs += ys * (f.y[0] * S.scale[warp][g][0] + f.y[2] * S.scale[warp][g + 8][0]);
                 cys += ys * (f.y[1] * S.scale[warp][g][0] + f.y[3] * S.scale[warp][g + 8][0]);
@@ -671,11 +732,11 @@ void launch_mlp_correct(nb_ctx* c, const BodyBuffers& b, bool kick, bool store_a
         (int)c->n, (float)c->p.epsilon_squared, c->p.G * c->p.timestep, c->p.timestep, kick ? 1 : 0);
 }
 
-void launch_mlp_samples(nb_ctx* c, const BodyBuffers& b, const int* slots, int nslots, float* X,
+void launch_mlp_samples(nb_ctx* c, const BodyBuffers& b, const int* pick, int npick, float* X,
                         float* Y, unsigned* count, unsigned cap) {
-    const double thL = c->p.theta, thB = kThetaBand;
+    const float thL = (float)c->p.theta, thB = kThetaBand;
     mlp_samples_kernel<<<c->sm_count * 8, kWarps * 32, 0, c->stream>>>(
-        c->tree, c->scal, b.pos, b.mass, (int)c->n, slots, nslots, thL * thL, thB * thB,
+        c->tree, c->scal, b.pos, b.mass, (int)c->n, pick, npick, thL * thL, thB * thB,
         c->p.epsilon_squared, X, Y, count, cap);
 }
 

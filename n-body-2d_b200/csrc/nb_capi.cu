@@ -563,9 +563,11 @@ int nb_mlp_samples(nb_ctx* c, uint64_t ntargets, uint64_t seed, uint64_t capacit
     nb::launch_gather(c, A, B, c->tree.body4);
     nb::launch_tree(c, B);
     nb::launch_moments(c, B, true);
+    nb::launch_groups(c);
     NB_CUDA(c, cudaGetLastError());
     c->parity ^= 1;
-    // targets: a seeded uniform choice of body slots (splitmix64)
+    // target groups: a seeded uniform choice (splitmix64), reduced modulo the
+    // group count on the device
     std::vector<int> slots(ntargets);
     uint64_t z = seed + 0x9e3779b97f4a7c15ull;
     for (auto& sl : slots) {
@@ -574,7 +576,7 @@ int nb_mlp_samples(nb_ctx* c, uint64_t ntargets, uint64_t seed, uint64_t capacit
         x = (x ^ (x >> 30)) * 0xbf58476d1ce4e5b9ull;
         x = (x ^ (x >> 27)) * 0x94d049bb133111ebull;
         x ^= x >> 31;
-        sl = (int)(x % (uint64_t)c->n);
+        sl = (int)(x & 0x7fffffff);
     }
     int* dslots = nullptr;
     float *dX = nullptr, *dY = nullptr;

@@ -202,7 +202,8 @@ class NbContext:
         check(self._lib.nb_set_mlp_weights(self.handle, ptr(params)), self._h)
 
     def mlp_samples(self, ntargets: int, seed: int = 0, capacity: int | None = None):
-        """Residual samples (features[k,12], residuals[k,2]) of the current bodies."""
+        """Residual samples (features[k,12], residuals[k,2]) of the current bodies,
+        from `ntargets` random target groups."""
         capacity = capacity or 256 * ntargets
         X = np.empty((capacity, 12), dtype=np.float32)
         Y = np.empty((capacity, 2), dtype=np.float32)

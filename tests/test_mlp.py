@@ -80,12 +80,12 @@ def test_learned_correction_beats_the_monopole_at_theta_one(nbp):
         m, p, v = nbp.universes.colliding_discs(65536, seed)
         cfg = nbp.SimConfig(theta=1.0, epsilon_squared=eps2, mode=nbp.NB_MODE_SPLIT, learned=True)
         with nbp.NbContext(cfg, m, p, v) as ctx:
-            X, Y = ctx.mlp_samples(8192, seed=seed)
+            X, Y = ctx.mlp_samples(2048, seed=seed)
         Xs.append(X)
         Ys.append(Y)
     X, Y = np.concatenate(Xs), np.concatenate(Ys)
     assert X.shape[0] > 100000 and np.isfinite(X).all() and np.isfinite(Y).all()
-    assert ((X[:, 2] >= 0.49) & (X[:, 2] <= 1.01)).mean() > 0.99  # w/d in the band
+    assert (X[:, 2] > 0).all() and ((X[:, 0] ** 2 + X[:, 1] ** 2 - 1) ** 2 < 1e-6).all()
     params, losses = nbp.mlp_train(X, Y, epochs=20, batch=1024, lr=2e-3, seed=0)
     assert losses[-1] < 0.5 * losses[0]
     # evaluation on an unseen seed
