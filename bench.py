@@ -55,6 +55,18 @@ def _package():
     return mod
 
 
+def _force_traffic(n: int):
+    """DRAM bytes per launch of the SPLIT force kernel, from the committed ncu
+    summary (captured at 1M bodies, scaled linearly to 4M there), scaled to n."""
+    f = ROOT / "profiles" / "force_split_collision1m.md"
+    if not f.exists():
+        return None
+    for ln in f.read_text().splitlines():
+        if ln.startswith("traffic_bytes_per_launch_4m:"):
+            return float(ln.split(":")[1]) * n / 4194304
+    return None
+
+
 def _peaks() -> tuple[dict, str]:
     f = ROOT / "MEASURED_PEAKS.json"
     if f.exists():
@@ -149,6 +161,20 @@ def _dist():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     return world, rank, local
+
+
+def max_over_ranks(value: float) -> float:
+    """Largest value over the ranks of the default process group (the job's
+    time is its slowest replica's); the value itself without one."""
+    import torch
+    import torch.distributed as dist
+
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return value
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
 
 
 def _workload(kind: str, n: int, seed: int = 0):
@@ -274,12 +300,7 @@ def run_ours(args) -> None:
     st = ctx.stats()
     ms = st.ms_last_step
     phases = ctx.phase_times()
-    if world > 1:
-        import torch.distributed as dist
-
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms)
     value = world * args.n / (ms * 1e-3)
 
     # e2e through the C ABI: host buffers, copies inside the timed region
@@ -294,11 +315,7 @@ def run_ours(args) -> None:
         ctx.upload(hm, hp, hv)
         ctx.step(1, sync=False)
         ctx.download(op, ov)
-    e2e_t = (time.perf_counter() - t0) / e2e_steps
-    if world > 1:
-        t = torch.tensor([e2e_t], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_t = float(t.item())
+    e2e_t = max_over_ranks((time.perf_counter() - t0) / e2e_steps)
 
     accuracy = None
     if not args.no_accuracy:
@@ -335,7 +352,10 @@ def run_ours(args) -> None:
         "config": _config(args),
         "roofline": {"kernel": "force", "bound": "fp64" if args.mode == "fp64" else "fp32",
                      "achieved": round(achieved, 3), "peak": round(fp_peak, 2),
-                     "unit": "TFLOP/s", "frac": round(achieved / fp_peak, 4), "traffic": None,
+                     "unit": "TFLOP/s", "frac": round(achieved / fp_peak, 4),
+                     "traffic": _force_traffic(args.n) if args.mode == "split" else None,
+                     "traffic_source": "ncu dram__bytes_read+write of force_split at 1M bodies "
+                                       "(profiles/force_split_collision1m.md), scaled by n",
                      "peak_source": f"nominal {lanes} FMA/clk/SM x 148 SMs at the sampled "
                                     f"median SM clock {sm_mhz} MHz",
                      "interactions_per_s": interactions / (force_ms * 1e-3),
