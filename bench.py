@@ -219,10 +219,13 @@ def run_reference(args) -> None:
         return
     if str(ROOT) not in sys.path:
         sys.path.insert(0, str(ROOT))
-    m, p, v = _workload(args.kind, args.n)
     cores = os.cpu_count() or 1
     from oracle import refcpu
 
+    if args.kind == "ensemble":
+        run_reference_ensemble(args, refcpu, cores, world)
+        return
+    m, p, v = _workload(args.kind, args.n)
     if refcpu.available():
         t = refcpu.time_steps(m, p, v, theta=args.theta, steps=args.steps, warmup=args.warmup,
                               threads=cores)
@@ -248,6 +251,56 @@ def run_reference(args) -> None:
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic", "config": _config(args),
+        "cpu_baseline": {"value": value, "unit": "body-steps/s", "cores": cores, "kind": kind,
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "body-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_reference_ensemble(args, refcpu, cores: int, world: int) -> None:
+    """Reference arm of the ensemble: the reference CPU backend holds one
+    universe per process, so it steps the universes one after another.  A
+    bounded sample: the first universes of the ensemble up to about one
+    million bodies, each for W untimed and K timed steps."""
+    nb = _package()
+    m, p, v, counts = nb.universes.ensemble_batch(args.universes, seed=0)
+    off = np.concatenate([[0], np.cumsum(counts.astype(np.int64))])
+    bodies, seconds, used = 0, 0.0, 0
+    for u in range(len(counts)):
+        sl = slice(off[u], off[u + 1])
+        if refcpu.available():
+            t = refcpu.time_steps(m[sl], p[sl], v[sl], theta=args.theta, steps=args.steps,
+                                  warmup=args.warmup, threads=cores)
+            kind = "reference"
+        else:
+            import oracle
+
+            st = oracle.RefState(m[sl], p[sl], v[sl])
+            for _ in range(args.warmup):
+                st.step(theta=args.theta, eps2=1e-4, dt=1e-4, G=1.0, nthreads=cores)
+            t0 = time.perf_counter()
+            for _ in range(args.steps):
+                st.step(theta=args.theta, eps2=1e-4, dt=1e-4, G=1.0, nthreads=cores)
+            t = (time.perf_counter() - t0) / args.steps
+            kind = "port"
+        bodies += int(counts[u])
+        seconds += t
+        used += 1
+        if bodies >= 1_000_000:
+            break
+    value = bodies / seconds
+    sample = (f"universes 0..{used - 1} of the {len(counts)}-universe ensemble ({bodies} bodies), "
+              f"each {args.steps} timed steps after {args.warmup} untimed, one after another, "
+              f"{cores} threads")
+    line = {
+        "impl": "reference", "metric": "body-steps/s", "value": value, "unit": "body-steps/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": seconds * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "universes": int(len(counts)),
+                   "n": int(m.shape[0]), "theta": args.theta},
         "cpu_baseline": {"value": value, "unit": "body-steps/s", "cores": cores, "kind": kind,
                          "sample": sample},
         "e2e": {"value": value, "unit": "body-steps/s", "h2d_bytes_per_step": 0,
@@ -385,6 +438,149 @@ def run_ours(args) -> None:
         print(json.dumps(line), flush=True)
 
 
+def run_ensemble(args) -> None:
+    """Batched ensemble: 512 exponential discs of 1,024..262,144 bodies
+    (log-uniform), advanced together by one batched context (one graph per
+    step, one persistent traversal launch) after the autotuner picked the leaf
+    and group sizes.  The same universes are then stepped as one context each,
+    launched one after another every step, for the comparison."""
+    world, rank, local = _dist()
+    nb = _package()
+    import torch
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    m, p, v, counts = nb.universes.ensemble_batch(args.universes, seed=rank)
+    n = int(m.shape[0])
+    args.n = n
+    cfg = nb.SimConfig(timestep=1e-4, theta=args.theta, epsilon_squared=1e-4, G=1.0,
+                       mode=nb.NB_MODE_SPLIT, device=local, quadrupole=args.quad,
+                       leaf_size=args.leaf)
+    ctx = nb.NbContext(cfg, m, p, v, counts=counts)
+    leaf, bpl = ctx.autotune(2) if not args.leaf else (args.leaf, 2)
+    ctx.step(args.warmup)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+            torch.cuda.synchronize()
+
+    barrier()
+    with ClockSampler(local) as clocks:
+        clocks.mark_start()
+        t0 = time.perf_counter()
+        ctx.step(args.steps, sync=False)
+        ctx.sync()
+        wall = (time.perf_counter() - t0) / args.steps
+        clocks.mark_end()
+    barrier()
+    st = ctx.stats()
+    ms = max_over_ranks(st.ms_last_step)
+    phases = ctx.phase_times()
+    value = world * n / (ms * 1e-3)
+
+    pin = lambda shape: torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy()
+    hm, hp, hv = pin((n,)), pin((n, 2)), pin((n, 2))
+    hm[:], hp[:], hv[:] = m, p, v
+    op, ov = pin((n, 2)), pin((n, 2))
+    e2e_steps = max(1, min(args.steps, 5))
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        ctx.upload(hm, hp, hv)
+        ctx.step(1, sync=False)
+        ctx.download(op, ov)
+    e2e_t = max_over_ranks((time.perf_counter() - t0) / e2e_steps)
+
+    accuracy = None
+    if not args.no_accuracy:
+        from nbody_b200 import accuracy as acc_mod
+
+        acc_now = ctx.accelerations()
+        pos_now, _ = ctx.download()
+        accuracy = acc_mod.ensemble_force_errors(acc_now, m, pos_now, counts, 1e-4,
+                                                 k=args.error_sample, device=local)
+        accuracy["oracle"] = "FP64 all-pairs within each universe (GPU kernel)"
+    ctx.close()
+
+    # one context per universe, each step launched universe after universe
+    looped = None
+    if rank == 0:
+        off = np.concatenate([[0], np.cumsum(counts.astype(np.int64))])
+        cfg1 = nb.SimConfig(timestep=1e-4, theta=args.theta, epsilon_squared=1e-4, G=1.0,
+                            mode=nb.NB_MODE_SPLIT, device=local, quadrupole=args.quad,
+                            leaf_size=leaf)
+        ctxs = [nb.NbContext(cfg1, m[off[u]:off[u + 1]], p[off[u]:off[u + 1]],
+                             v[off[u]:off[u + 1]]) for u in range(len(counts))]
+        for c in ctxs:
+            c.step(args.warmup)
+        torch.cuda.synchronize()
+        lsteps = max(1, min(args.steps, 5))
+        t0 = time.perf_counter()
+        for _ in range(lsteps):
+            for c in ctxs:
+                c.step(1, sync=False)
+        for c in ctxs:
+            c.sync()
+        lt = (time.perf_counter() - t0) / lsteps
+        dev_ms = sum(c.stats().ms_last_step for c in ctxs)
+        for c in ctxs:
+            c.close()
+        looped = {"value": n / lt, "unit": "body-steps/s", "ms_per_step_wall": lt * 1e3,
+                  "sum_of_device_ms": dev_ms, "steps": lsteps,
+                  "batched_wall_ms_per_step": wall * 1e3,
+                  "speedup_batched_vs_looped": (n / wall) / (n / lt),
+                  "how": f"{len(counts)} contexts (one graph each, own streams), every step "
+                         "launches them one after another; wall clock from the first launch "
+                         "to the last sync"}
+
+    peaks, peak_kind = _peaks()
+    clk = clocks.summary()
+    sm_mhz = clk["sm_mhz"] or peaks.get("sm_max_mhz", 1965.0)
+    interactions = st.cell_interactions + st.body_interactions
+    force_ms = phases.get("force", ms)
+    fp_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
+    achieved = FLOPS_PER_INTERACTION * interactions / (force_ms * 1e-3) / 1e12
+    line = {
+        "metric": "body-steps/s", "value": value, "unit": "body-steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64", "data": "synthetic",
+        "config": {"workload": args.workload, "universes": int(len(counts)), "n": n,
+                   "n_min": int(counts.min()), "n_max": int(counts.max()), "theta": args.theta,
+                   "mode": "split", "leaf_size": leaf, "bodies_per_lane": bpl,
+                   "autotuned": not args.leaf, "softening": 0.01, "dt": 1e-4, "G": 1.0,
+                   "l2": "inputs larger than L2"},
+        "roofline": {"kernel": "force", "bound": "fp32", "achieved": round(achieved, 3),
+                     "peak": round(fp_peak, 2), "unit": "TFLOP/s",
+                     "frac": round(achieved / fp_peak, 4), "traffic": None,
+                     "peak_source": f"nominal 128 FMA/clk/SM x 148 SMs at the sampled median "
+                                    f"SM clock {sm_mhz} MHz",
+                     "interactions_per_body": interactions / n,
+                     "flops_per_interaction": FLOPS_PER_INTERACTION},
+        "phases_ms": {k: round(v, 4) for k, v in phases.items()},
+        "e2e": {"value": world * n / e2e_t, "unit": "body-steps/s",
+                "h2d_bytes_per_step": 40 * n, "d2h_bytes_per_step": 32 * n, "steps": e2e_steps},
+        "gpu_launches": int(st.kernels_per_step) * args.steps,
+        "clocks": clk, "accuracy": accuracy, "looped_single_universe": looped,
+    }
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def run_variants(args, nb, m, p, v, device, plain_value, plain_accuracy) -> dict:
     """The learned theta = 1.0 step next to the plain theta = 0.5 one (same
     workload, same timing method), plus the analytic-quadrupole and plain
@@ -430,6 +626,7 @@ WORKLOADS = {
     "collision4m": ("collision", 4194304, 0.5),
     "disc16k": ("disc", 16384, 0.5),
     "plummer16m": ("plummer", 16777216, 0.5),
+    "ensemble512": ("ensemble", 0, 0.5),
 }
 
 
@@ -450,6 +647,7 @@ def main(argv=None):
     ap.add_argument("--error-sample", type=int, default=65536)
     ap.add_argument("--variants", action="store_true",
                     help="also time the learned, quadrupole and plain theta=1.0 walks")
+    ap.add_argument("--universes", type=int, default=512, help="ensemble512: universe count")
     args = ap.parse_args(argv)
     kind, n, theta = WORKLOADS[args.workload]
     args.kind = kind
@@ -459,6 +657,8 @@ def main(argv=None):
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif kind == "ensemble":
+        run_ensemble(args)
     else:
         run_ours(args)
 

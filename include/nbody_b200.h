@@ -97,6 +97,24 @@ NB_API int nb_params_default(nb_params* p);
 NB_API int nb_create(const nb_params* p, uint64_t n, const double* mass, const double* pos_xy,
               const double* vel_xy, nb_ctx** out);
 
+/* Batched universes (no counterpart in the reference, which holds one
+ * universe per process): nuniverses independent universes of counts[u]
+ * bodies each, concatenated in universe order in mass/pos_xy/vel_xy.  They
+ * are advanced together: one sort, one tree (a universe never sees
+ * another's bodies) and one persistent traversal launch per step, in one
+ * captured graph.  NB_MODE_SPLIT only (no learned correction); at most 1024
+ * universes.  Every other call works on the batch as one body array in the
+ * concatenated order. */
+NB_API int nb_batch_create(const nb_params* p, uint32_t nuniverses, const uint64_t* counts,
+                           const double* mass, const double* pos_xy, const double* vel_xy,
+                           nb_ctx** out);
+
+/* Picks the SPLIT traversal's bodies per lane (1 or 2: target groups of 32
+ * or 64) and leaf size (4, 8, 16, 32) by timing `steps` steps of each on a
+ * copy of the bodies, which are restored afterwards; the choice stays set.
+ * Either output pointer may be NULL. */
+NB_API int nb_autotune(nb_ctx* ctx, uint32_t steps, int32_t* leaf_out, int32_t* bpl_out);
+
 /* Replaces ~BarnesHutCuda + release_device_resources (BarnesHutCuda.cpp:13-18,
  * BarnesHutCuda.cu:608-630). Accepts NULL. */
 NB_API int nb_destroy(nb_ctx* ctx);

@@ -33,3 +33,20 @@ def force_errors(acc_all: np.ndarray, mass: np.ndarray, pos: np.ndarray, epsilon
     tgt = sample_targets(mass.shape[0], k, seed)
     exact = allpairs_accelerations(mass, pos, tgt, epsilon_squared, device)
     return summary(relative_errors(acc_all[tgt], exact))
+
+
+def ensemble_force_errors(acc_all: np.ndarray, mass: np.ndarray, pos: np.ndarray,
+                          counts: np.ndarray, epsilon_squared: float, k: int = 65536,
+                          device: int = 0, seed: int = 12345) -> dict:
+    """Batched universes: each sampled target against all-pairs over its own
+    universe only (universes do not interact)."""
+    tgt = sample_targets(mass.shape[0], k, seed)
+    off = np.concatenate([[0], np.cumsum(counts.astype(np.int64))])
+    uni = np.searchsorted(off, tgt, side="right") - 1
+    err = np.empty(tgt.shape[0])
+    for u in np.unique(uni):
+        sel = np.nonzero(uni == u)[0]
+        a, b = off[u], off[u + 1]
+        exact = allpairs_accelerations(mass[a:b], pos[a:b], tgt[sel] - a, epsilon_squared, device)
+        err[sel] = relative_errors(acc_all[tgt[sel]], exact)
+    return summary(err)

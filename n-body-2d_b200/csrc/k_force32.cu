@@ -100,16 +100,20 @@ __device__ __forceinline__ void cell_terms(const float4 e, const float4 q, const
     }
 }
 
+// A body's own entry has dx = dy = 0 exactly (body4 and px/py round the same
+// double difference), so with eps2 > 0 it adds 0 * finite = 0 and needs no
+// index test.  d2 == 0 (eps2 = 0 and the same FP32 coordinates: the body
+// itself, or a body that coincides with it at FP32 resolution) contributes
+// nothing instead of 0 * inf.
 template <int kBPL>
 __device__ __forceinline__ void body_terms(const float4 e, const float* px, const float* py,
-                                           const int* me, float eps2, float* ax, float* ay) {
+                                           float eps2, float* ax, float* ay) {
 #pragma unroll
     for (int b = 0; b < kBPL; ++b) {
-        const bool self = __float_as_int(e.w) == me[b];
         const float dx = e.x - px[b], dy = e.y - py[b];
-        const float d2 = self ? 1.f : fmaf(dx, dx, fmaf(dy, dy, eps2));
+        const float d2 = fmaf(dx, dx, fmaf(dy, dy, eps2));
         const float inv = rsqrtf(d2);
-        const float a = (self ? 0.f : e.z) * (inv * inv) * inv;
+        const float a = d2 == 0.f ? 0.f : e.z * (inv * inv) * inv;
         ax[b] = fmaf(dx, a, ax[b]);
         ay[b] = fmaf(dy, a, ay[b]);
     }
@@ -130,13 +134,12 @@ __device__ __forceinline__ void sum_cells(const WarpLists& L, int cnt, const flo
 
 template <int kBPL>
 __device__ __forceinline__ void sum_bodies(const WarpLists& L, int cnt, const float* px,
-                                           const float* py, const int* me, float eps2, float* ax,
-                                           float* ay) {
+                                           const float* py, float eps2, float* ax, float* ay) {
     if (cnt == 32) {
 #pragma unroll 4
-        for (int j = 0; j < 32; ++j) body_terms<kBPL>(L.body[j], px, py, me, eps2, ax, ay);
+        for (int j = 0; j < 32; ++j) body_terms<kBPL>(L.body[j], px, py, eps2, ax, ay);
     } else {
-        for (int j = 0; j < cnt; ++j) body_terms<kBPL>(L.body[j], px, py, me, eps2, ax, ay);
+        for (int j = 0; j < cnt; ++j) body_terms<kBPL>(L.body[j], px, py, eps2, ax, ay);
     }
 }
 
@@ -144,7 +147,7 @@ __device__ __forceinline__ void sum_bodies(const WarpLists& L, int cnt, const fl
 // g0 + l, g0 + 32 + l, ...) and accumulate the FP32 accelerations.
 template <bool kQuad, int kBPL, bool kLearned>
 __device__ __forceinline__ void walk_group(WarpLists& L, const Tree& t, int root, int n, int g0,
-                                           int g1, const float* px, const float* py, const int* me,
+                                           int g1, const float* px, const float* py,
                                            const bool* act_body, float eps2, float theta2,
                                            int leaf_size, float* ax, float* ay,
                                            unsigned long long& ncell, unsigned long long& npair,
@@ -281,7 +284,7 @@ __device__ __forceinline__ void walk_group(WarpLists& L, const Tree& t, int root
             bcount += added;
             __syncwarp();
             if (bcount >= 32) {
-                sum_bodies<kBPL>(L, 32, px, py, me, eps2, ax, ay);
+                sum_bodies<kBPL>(L, 32, px, py, eps2, ax, ay);
                 npair += 32;
                 __syncwarp();
                 if (lane < bcount - 32) L.body[lane] = L.body[32 + lane];
@@ -291,7 +294,7 @@ __device__ __forceinline__ void walk_group(WarpLists& L, const Tree& t, int root
         }
     }
     sum_cells<kQuad, kBPL>(L, ccount, px, py, eps2, ax, ay);
-    sum_bodies<kBPL>(L, bcount, px, py, me, eps2, ax, ay);
+    sum_bodies<kBPL>(L, bcount, px, py, eps2, ax, ay);
     ncell += ccount;
     npair += bcount;
     __syncwarp();
@@ -302,14 +305,12 @@ __device__ __forceinline__ void walk_group(WarpLists& L, const Tree& t, int root
 template <bool kQuad, int kBPL, bool kLearned>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32)
 force_split(double2* __restrict__ pos, double2* __restrict__ vel, double2* __restrict__ acc_out,
-            float2* __restrict__ acc32, int n, Tree t, DeviceScalars* __restrict__ s, float eps2,
-            float theta2, int leaf_size, double G_dt, double dt, int kick) {
+            float2* __restrict__ acc32, int n, Tree t, DeviceScalars* __restrict__ s, Batch bt,
+            float eps2, float theta2, int leaf_size, double G_dt, double dt, int kick) {
     __shared__ WarpLists lists[kWarpsPerBlock];
     const int lane = threadIdx.x & 31;
     WarpLists& L = lists[threadIdx.x >> 5];
     const int ngroups = s->groups;
-    const int root = s->root;
-    const double cx = s->center[0], cy = s->center[1];
     unsigned long long cells_total = 0, pairs_total = 0;
     while (true) {
         int g = 0;
@@ -318,6 +319,10 @@ force_split(double2* __restrict__ pos, double2* __restrict__ vel, double2* __res
         if (g >= ngroups) break;
         const int2 gr = t.groups[g];
         const int g0 = gr.x, g1 = min(gr.y, n - 1);
+        // batched universes: walk the group's own universe from its root
+        const int root = bt.nuni ? bt.root[bt.uid[g0]] : s->root;
+        const double2 fc = frame_center(s, bt, g0);
+        const double cx = fc.x, cy = fc.y;
         int me[kBPL];
         bool on[kBPL];
         float px[kBPL], py[kBPL], ax[kBPL], ay[kBPL];
@@ -333,7 +338,7 @@ force_split(double2* __restrict__ pos, double2* __restrict__ vel, double2* __res
         unsigned long long ncell, npair;
         int nband = 0;
         int* band = kLearned ? t.band + (int64_t)kBandPerBody * g0 : nullptr;
-        walk_group<kQuad, kBPL, kLearned>(L, t, root, n, g0, g1, px, py, me, on, eps2, theta2,
+        walk_group<kQuad, kBPL, kLearned>(L, t, root, n, g0, g1, px, py, on, eps2, theta2,
                                           leaf_size, ax, ay, ncell, npair, &s->error, band, nband,
                                           kBandPerBody * (g1 - g0 + 1));
         if (kLearned) {
@@ -372,7 +377,7 @@ force_split(double2* __restrict__ pos, double2* __restrict__ vel, double2* __res
 
 template <bool kQuad, int kBPL, bool kLearned>
 void launch_split_kernel(nb_ctx* c, const BodyBuffers& b, bool kick, bool store_acc) {
-    int& grid = c->split_blocks[(kQuad ? 1 : 0) + (kLearned ? 2 : 0)];
+    int& grid = c->split_blocks[(kQuad ? 1 : 0) + (kLearned ? 2 : 0) + (kBPL == 1 ? 4 : 0)];
     if (grid == 0) {
         int blocks = 0;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
@@ -384,24 +389,26 @@ void launch_split_kernel(nb_ctx* c, const BodyBuffers& b, bool kick, bool store_
     const float theta2 = (float)(c->p.theta * c->p.theta);
     const int leaf = c->p.leaf_size > 0 ? c->p.leaf_size : kDefaultLeaf;
     force_split<kQuad, kBPL, kLearned><<<grid, 32 * kWarpsPerBlock, 0, c->stream>>>(
-        b.pos, b.vel, store_acc ? c->acc : nullptr, c->acc32, (int)c->n, c->tree, c->scal,
+        b.pos, b.vel, store_acc ? c->acc : nullptr, c->acc32, (int)c->n, c->tree, c->scal, c->batch,
         (float)c->p.epsilon_squared, theta2, leaf, c->p.G * c->p.timestep, c->p.timestep,
         kick ? 1 : 0);
 }
 
 }  // namespace
 
-int split_group_size(const nb_ctx* c) { return 32 * kBodiesPerLane; }
+int split_group_size(const nb_ctx* c) { return 32 * (c->bpl == 1 ? 1 : kBodiesPerLane); }
 
 void launch_force_split(nb_ctx* c, const BodyBuffers& b, bool kick, bool store_acc) {
     c->launches += 1;
     cudaMemsetAsync(&c->scal->group_ticket, 0, sizeof(unsigned), c->stream);
-    if (c->p.flags & NB_FLAG_LEARNED)
+    if (c->p.flags & NB_FLAG_LEARNED)  // the correction kernel assumes groups of 64
         launch_split_kernel<false, kBodiesPerLane, true>(c, b, kick, store_acc);
     else if (c->p.flags & NB_FLAG_QUADRUPOLE)
-        launch_split_kernel<true, kBodiesPerLane, false>(c, b, kick, store_acc);
+        c->bpl == 1 ? launch_split_kernel<true, 1, false>(c, b, kick, store_acc)
+                    : launch_split_kernel<true, kBodiesPerLane, false>(c, b, kick, store_acc);
     else
-        launch_split_kernel<false, kBodiesPerLane, false>(c, b, kick, store_acc);
+        c->bpl == 1 ? launch_split_kernel<false, 1, false>(c, b, kick, store_acc)
+                    : launch_split_kernel<false, kBodiesPerLane, false>(c, b, kick, store_acc);
 }
 
 }  // namespace nb

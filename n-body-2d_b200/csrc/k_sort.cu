@@ -142,6 +142,94 @@ __global__ void morton_kernel(const double2* __restrict__ pos, int64_t n,
 }
 
 // ---------------------------------------------------------------------------
+// Batched universes: per-universe boxes and 54-bit Morton codes under the
+// universe id.  Doubles are reduced through an order-preserving integer image
+// so plain 64-bit atomicMin/atomicMax give the exact FP64 min/max.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned long long ordered_bits(double v) {
+    const unsigned long long b = (unsigned long long)__double_as_longlong(v);
+    return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double from_ordered(unsigned long long o) {
+    const unsigned long long b = (o >> 63) ? (o & 0x7fffffffffffffffull) : ~o;
+    return __longlong_as_double((long long)b);
+}
+
+__global__ void __launch_bounds__(256)
+bbox_batch_kernel(const double2* __restrict__ pos, int64_t n, Batch b) {
+    const int lane = threadIdx.x & 31;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i - lane < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const bool valid = i < n;
+        const int u = valid ? b.uid[i] : -1;
+        const double2 p = valid ? pos[i] : make_double2(0.0, 0.0);
+        unsigned long long e[4] = {ordered_bits(p.x), ~ordered_bits(p.x), ordered_bits(p.y),
+                                   ~ordered_bits(p.y)};  // min-encoded: max via the complement
+        const int u0 = __shfl_sync(kFull, u, 0);
+        const bool uniform = __all_sync(kFull, valid && u == u0);
+        if (uniform) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const unsigned long long t = __shfl_xor_sync(kFull, e[k], o);
+                    e[k] = t < e[k] ? t : e[k];
+                }
+            if (lane == 0)
+#pragma unroll
+                for (int k = 0; k < 4; ++k) atomicMin(b.boxbits + 4 * u0 + k, e[k]);
+        } else if (valid) {
+#pragma unroll
+            for (int k = 0; k < 4; ++k) atomicMin(b.boxbits + 4 * u + k, e[k]);
+        }
+    }
+}
+
+// Squares every universe's box as the single-universe path does, and resets
+// the reduction slots for the next step.
+__global__ void bbox_batch_finish(Batch b) {
+    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= b.nuni) return;
+    unsigned long long* e = b.boxbits + 4 * u;
+    double x0 = from_ordered(e[0]), x1 = from_ordered(~e[1]);
+    double y0 = from_ordered(e[2]), y1 = from_ordered(~e[3]);
+    const double x_range = x1 - x0, y_range = y1 - y0;
+    if (x_range > y_range) {
+        const double mid = (y0 + y1) * 0.5;
+        y0 = mid - x_range * 0.5;
+        y1 = mid + x_range * 0.5;
+    } else {
+        const double mid = (x0 + x1) * 0.5;
+        x0 = mid - y_range * 0.5;
+        x1 = mid + y_range * 0.5;
+    }
+    const double w = x1 - x0;
+    b.lo[u] = make_double2(x0, y0);
+    b.center[u] = make_double2(0.5 * (x0 + x1), 0.5 * (y0 + y1));
+    b.w2[u] = w > 0.0 ? w * w : 1.0;  // a one-point universe: any width
+    e[0] = ~0ull;
+    e[1] = ~0ull;
+    e[2] = ~0ull;
+    e[3] = ~0ull;
+}
+
+__global__ void morton_batch_kernel(const double2* __restrict__ pos, int64_t n, Batch b,
+                                    uint64_t* __restrict__ key, uint32_t* __restrict__ val) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int u = b.uid[i];
+    const double2 lo = b.lo[u];
+    const double inv_w = 1.0 / sqrt(b.w2[u]);
+    const double2 p = __ldg(pos + i);
+    const double scale = (double)(1u << kBatchMortonBits);
+    const double top = scale - 1.0;
+    const uint32_t ix = __double2uint_rd(fmin(fmax((p.x - lo.x) * inv_w * scale, 0.0), top));
+    const uint32_t iy = __double2uint_rd(fmin(fmax((p.y - lo.y) * inv_w * scale, 0.0), top));
+    key[i] = ((uint64_t)u << (2 * kBatchMortonBits)) | (expand_bits_2d(ix) << 1) | expand_bits_2d(iy);
+    val[i] = (uint32_t)i;
+}
+
+// ---------------------------------------------------------------------------
 // LSD radix sort, 8-bit digits, 8 passes.  Each pass: per-tile digit counts
 // (upsweep), a per-digit scan over tiles, and a stable scatter (downsweep)
 // that ranks keys inside the tile with warp-private histograms and
@@ -497,7 +585,7 @@ onesweep_pass(const uint64_t* __restrict__ key_in, const uint32_t* __restrict__ 
 // writes the FP32 source record of each body relative to the box centre.
 __global__ void gather_kernel(const uint32_t* __restrict__ order, int64_t n, BodyBuffers src,
                               BodyBuffers dst, float4* __restrict__ body4,
-                              const DeviceScalars* __restrict__ s) {
+                              const DeviceScalars* __restrict__ s, Batch bt) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
     const uint32_t j = __ldg(order + i);
@@ -507,9 +595,11 @@ __global__ void gather_kernel(const uint32_t* __restrict__ order, int64_t n, Bod
     dst.vel[i] = __ldg(src.vel + j);
     dst.mass[i] = m;
     dst.orig[i] = __ldg(src.orig + j);
-    if (body4)
-        body4[i] = make_float4((float)(p.x - s->center[0]), (float)(p.y - s->center[1]), (float)m,
+    if (body4) {
+        const double2 c = frame_center(s, bt, (int)i);
+        body4[i] = make_float4((float)(p.x - c.x), (float)(p.y - c.y), (float)m,
                                __int_as_float((int)i));
+    }
 }
 
 inline unsigned blocks_for(int64_t n, int threads) {
@@ -519,12 +609,23 @@ inline unsigned blocks_for(int64_t n, int threads) {
 }  // namespace
 
 void launch_bbox(nb_ctx* c, const double2* pos) {
+    if (c->batch.nuni > 0) {
+        c->launches += 2;
+        bbox_batch_kernel<<<2 * c->sm_count * 8, 256, 0, c->stream>>>(pos, c->n, c->batch);
+        bbox_batch_finish<<<blocks_for(c->batch.nuni, 128), 128, 0, c->stream>>>(c->batch);
+        return;
+    }
     c->launches += 1;
     bbox_kernel<<<c->bbox_blocks, kBoxThreads, 0, c->stream>>>(pos, c->n, c->bbox_partials, c->scal);
 }
 
 void launch_morton(nb_ctx* c, const double2* pos) {
     c->launches += 1;
+    if (c->batch.nuni > 0) {
+        morton_batch_kernel<<<blocks_for(c->n, 256), 256, 0, c->stream>>>(
+            pos, c->n, c->batch, c->sort.key[0], c->sort.val[0]);
+        return;
+    }
     morton_kernel<<<blocks_for(c->n, 256), 256, 0, c->stream>>>(pos, c->n, c->scal, c->sort.key[0],
                                                                c->sort.val[0]);
 }
@@ -570,7 +671,7 @@ void launch_morton_sort_raw(const double2* pos, int64_t n, uint64_t* const key[2
 void launch_gather(nb_ctx* c, const BodyBuffers& src, const BodyBuffers& dst, float4* body4) {
     c->launches += 1;
     gather_kernel<<<blocks_for(c->n, 256), 256, 0, c->stream>>>(c->sort.val[0], c->n, src, dst,
-                                                                body4, c->scal);
+                                                                body4, c->scal, c->batch);
 }
 
 }  // namespace nb

@@ -302,7 +302,8 @@ __global__ void tree_trivial_root(const double2* __restrict__ pos, const double*
 template <bool kSplit, bool kFeat>
 __device__ __forceinline__ void cell_moments(int id, const DeviceScalars* __restrict__ s,
                                              const double2* __restrict__ pos,
-                                             const double* __restrict__ mass, const Tree& t) {
+                                             const double* __restrict__ mass, const Tree& t,
+                                             const Batch& bt) {
     const int4 ch = t.child[id];
     const int refs[4] = {ch.x, ch.y, ch.z, ch.w};
     double cm[4], cmx[4], cmy[4];
@@ -394,7 +395,7 @@ __device__ __forceinline__ void cell_moments(int id, const DeviceScalars* __rest
             __stcg(to, make_double2(txxx, txxy));
             __stcg(to + 1, make_double2(txyy, tyyy));
             // the MLP's cell features, normalised by M and the cell width
-            const double w2 = s->wsq[t.level[id]], w = sqrt(w2);
+            const double w2 = cell_width2(s, bt, t.range[id].x, t.level[id]), w = sqrt(w2);
             const double im2 = 1.0 / (M * w2), im3 = im2 / w;
             t.cellf[3 * id + 0] = make_float4((float)(mmax / M), (float)(sxx * im2),
                                               (float)(sxy * im2), (float)(syy * im2));
@@ -402,8 +403,10 @@ __device__ __forceinline__ void cell_moments(int id, const DeviceScalars* __rest
                                               (float)(txyy * im3), (float)(tyyy * im3));
             t.cellf[3 * id + 2] = make_float4(0.f, (float)w, 0.f, 0.f);
         }
-        t.cell4[id] = make_float4((float)(com.x - s->center[0]), (float)(com.y - s->center[1]),
-                                  (float)M, (float)s->wsq[t.level[id]]);
+        const int first = t.range[id].x;
+        const double2 fc = frame_center(s, bt, first);
+        t.cell4[id] = make_float4((float)(com.x - fc.x), (float)(com.y - fc.y), (float)M,
+                                  (float)cell_width2(s, bt, first, t.level[id]));
         t.cellq[id] = make_float4((float)sxx, (float)sxy, (float)syy, 0.f);
     }
 }
@@ -412,7 +415,7 @@ __device__ __forceinline__ void cell_moments(int id, const DeviceScalars* __rest
 // climb; the last child to arrive at a parent (atomic counter) computes it.
 template <bool kSplit, bool kFeat>
 __global__ void tree_moments(DeviceScalars* __restrict__ s, const double2* __restrict__ pos,
-                             const double* __restrict__ mass, Tree t) {
+                             const double* __restrict__ mass, Tree t, Batch bt) {
     int id = blockIdx.x * blockDim.x + threadIdx.x;
     const int cells = s->cells;
     if (id >= cells || t.nint[id] != 0) return;
@@ -423,7 +426,7 @@ __global__ void tree_moments(DeviceScalars* __restrict__ s, const double2* __res
             atomicOr(&s->error, kErrTree);
             return;
         }
-        cell_moments<kSplit, kFeat>(id, s, pos, mass, t);
+        cell_moments<kSplit, kFeat>(id, s, pos, mass, t, bt);
         __threadfence();
         const int par = t.parent[id];
         if (par < 0) return;
@@ -446,7 +449,8 @@ __global__ void tree_moments(DeviceScalars* __restrict__ s, const double2* __res
 // larger than a group are cut into chunks of gsize.  kWrite = false
 // counts the groups of each cell, kWrite = true writes them at gbase[cell].
 template <bool kWrite>
-__global__ void tree_groups(int n, int gsize, Tree t, const DeviceScalars* __restrict__ s) {
+__global__ void tree_groups(int n, int gsize, Tree t, const DeviceScalars* __restrict__ s,
+                            Batch bt) {
     const int id = blockIdx.x * blockDim.x + threadIdx.x;
     const int cells = s->cells;
     if (id >= n) return;
@@ -470,7 +474,10 @@ __global__ void tree_groups(int n, int gsize, Tree t, const DeviceScalars* __res
         if (kWrite) t.groups[out + emitted] = make_int2(a, b);
         ++emitted;
     };
-    if (rg.y - rg.x + 1 <= gsize) {
+    // batched universes: a forest cell above the universe roots may hold few
+    // bodies but never becomes a group; it hands its children on instead
+    const bool spans = bt.nuni && bt.uid[rg.x] != bt.uid[rg.y];
+    if (rg.y - rg.x + 1 <= gsize && !spans) {
         if (id == s->root) emit(rg.x, rg.y);  // the whole (small) tree is one group
     } else {
         const int4 ch = t.child[id];
@@ -490,14 +497,15 @@ __global__ void tree_groups(int n, int gsize, Tree t, const DeviceScalars* __res
                 b = t.leaf_last[a];
             }
             const int cnt = b - a + 1;
-            if (cnt > gsize) {
+            if (cnt > gsize || (bt.nuni && bt.uid[a] != bt.uid[b])) {  // the child emits
                 if (run_a >= 0) emit(run_a, run_b);
                 run_a = -1;
                 if (r < 0)  // oversized multi-body leaf: chunks of one group each
                     for (int k = a; k <= b; k += gsize) emit(k, min(b, k + gsize - 1));
                 continue;
             }
-            if (run_a >= 0 && b - run_a + 1 > gsize) {
+            // a group never spans two universes (a forest cell's children may)
+            if (run_a >= 0 && (b - run_a + 1 > gsize || (bt.nuni && bt.uid[a] != bt.uid[run_a]))) {
                 emit(run_a, run_b);
                 run_a = -1;
             }
@@ -509,11 +517,36 @@ __global__ void tree_groups(int n, int gsize, Tree t, const DeviceScalars* __res
     if (!kWrite) t.gcount[id] = emitted;
 }
 
+// Root reference of each universe: the cell whose body range is exactly the
+// universe's (found like a child cell in tree_link), or its single leaf.
+__global__ void batch_roots(const uint64_t* __restrict__ key, Tree t, Batch bt) {
+    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= bt.nuni) return;
+    const int a = bt.off[u], b = bt.off[u + 1] - 1;
+    if (b <= a) {
+        bt.root[u] = ~a;
+        return;
+    }
+    const int c = lcp_digits(key[a], key[b]);
+    if (c >= kMaxLevel) {  // all bodies of the universe in one level-30 leaf
+        bt.root[u] = ~a;
+        return;
+    }
+    bt.root[u] = t.cell_of[gallop_right(key, a, b, c + 1)];
+}
+
 inline unsigned blocks_for(int64_t n, int threads) {
     return (unsigned)((n + threads - 1) / threads);
 }
 
 }  // namespace
+
+void launch_batch_roots(nb_ctx* c) {
+    if (c->batch.nuni == 0) return;
+    c->launches += 1;
+    batch_roots<<<blocks_for(c->batch.nuni, 128), 128, 0, c->stream>>>(c->sort.key[0], c->tree,
+                                                                      c->batch);
+}
 
 void launch_groups(nb_ctx* c) {
     const int n = (int)c->n;
@@ -521,13 +554,13 @@ void launch_groups(nb_ctx* c) {
     c->launches += 5;
     const int gsize = split_group_size(c);
     tree_groups<false><<<blocks_for(n, kThreads), kThreads, 0, c->stream>>>(n, gsize, c->tree,
-                                                                            c->scal);
+                                                                            c->scal, c->batch);
     scan_reduce<<<sblocks, kThreads, 0, c->stream>>>(c->tree.gcount, n, c->scan.block_sums);
     scan_block_sums<<<1, kThreads, 0, c->stream>>>(c->scan.block_sums, sblocks, &c->scal->groups);
     scan_apply<<<sblocks, kThreads, 0, c->stream>>>(c->tree.gcount, n, c->scan.block_sums,
                                                      c->tree.gbase, nullptr);
     tree_groups<true><<<blocks_for(n, kThreads), kThreads, 0, c->stream>>>(n, gsize, c->tree,
-                                                                           c->scal);
+                                                                           c->scal, c->batch);
 }
 
 void launch_tree(nb_ctx* c, const BodyBuffers& b) {
@@ -553,13 +586,14 @@ void launch_moments(nb_ctx* c, const BodyBuffers& b, bool split) {
     c->launches += 1;
     const unsigned blocks = blocks_for(cap, kThreads);
     if (feat)
-        tree_moments<true, true><<<blocks, kThreads, 0, c->stream>>>(c->scal, b.pos, b.mass, c->tree);
+        tree_moments<true, true><<<blocks, kThreads, 0, c->stream>>>(c->scal, b.pos, b.mass, c->tree,
+                                                                     c->batch);
     else if (split)
         tree_moments<true, false><<<blocks, kThreads, 0, c->stream>>>(c->scal, b.pos, b.mass,
-                                                                      c->tree);
+                                                                      c->tree, c->batch);
     else
         tree_moments<false, false><<<blocks, kThreads, 0, c->stream>>>(c->scal, b.pos, b.mass,
-                                                                       c->tree);
+                                                                       c->tree, c->batch);
 }
 
 }  // namespace nb

@@ -152,6 +152,43 @@ void free_all(nb_ctx* c) {
     cudaFree(c->mlp_params);
 }
 
+int alloc_batch(nb_ctx* c, uint32_t nuni, const uint64_t* counts) {
+    nb::Batch& b = c->batch;
+    std::vector<int32_t> off(nuni + 1), uid((size_t)c->n);
+    off[0] = 0;
+    for (uint32_t u = 0; u < nuni; ++u) {
+        off[u + 1] = off[u] + (int32_t)counts[u];
+        for (int32_t i = off[u]; i < off[u + 1]; ++i) uid[i] = (int32_t)u;
+    }
+    int32_t *doff = nullptr, *duid = nullptr;
+    NB_CUDA(c, dalloc(&doff, nuni + 1));
+    NB_CUDA(c, dalloc(&duid, (size_t)c->n));
+    b.off = doff;
+    b.uid = duid;
+    NB_CUDA(c, dalloc(&b.boxbits, 4 * (size_t)nuni));
+    NB_CUDA(c, dalloc(&b.center, nuni));
+    NB_CUDA(c, dalloc(&b.w2, nuni));
+    NB_CUDA(c, dalloc(&b.lo, nuni));
+    NB_CUDA(c, dalloc(&b.root, nuni));
+    NB_CUDA(c, cudaMemcpy(doff, off.data(), sizeof(int32_t) * (nuni + 1), cudaMemcpyHostToDevice));
+    NB_CUDA(c, cudaMemcpy(duid, uid.data(), sizeof(int32_t) * c->n, cudaMemcpyHostToDevice));
+    NB_CUDA(c, cudaMemset(b.boxbits, 0xff, sizeof(unsigned long long) * 4 * nuni));
+    b.nuni = (int)nuni;
+    return NB_OK;
+}
+
+void free_batch(nb_ctx* c) {
+    nb::Batch& b = c->batch;
+    cudaFree(const_cast<int32_t*>(b.off));
+    cudaFree(const_cast<int32_t*>(b.uid));
+    cudaFree(b.boxbits);
+    cudaFree(b.center);
+    cudaFree(b.w2);
+    cudaFree(b.lo);
+    cudaFree(b.root);
+    b = nb::Batch();
+}
+
 void drop_graphs(nb_ctx* c) {
     for (auto& g : c->graph)
         if (g) {
@@ -187,6 +224,7 @@ void enqueue_step(nb_ctx* c, int parity, bool integrate, bool store_acc, bool ti
     nb::launch_gather(c, A, B, split ? c->tree.body4 : nullptr);
     mark(3);
     nb::launch_tree(c, B);
+    nb::launch_batch_roots(c);
     mark(4);
     nb::launch_moments(c, B, split);
     mark(5);
@@ -305,8 +343,13 @@ const char* nb_status_string(int s) {
 
 const char* nb_last_error(const nb_ctx* c) { return c ? c->err.c_str() : "null context"; }
 
-int nb_create(const nb_params* p, uint64_t n, const double* mass, const double* pos_xy,
-              const double* vel_xy, nb_ctx** out) {
+}  // extern "C"
+
+namespace {
+
+// nb_create and nb_batch_create: counts == nullptr for a single universe.
+int create_context(const nb_params* p, uint64_t n, const double* mass, const double* pos_xy,
+                   const double* vel_xy, uint32_t nuni, const uint64_t* counts, nb_ctx** out) {
     if (!out) return NB_ERR_INVALID;
     *out = nullptr;
     if (check_params(p) != NB_OK) return NB_ERR_INVALID;
@@ -329,6 +372,7 @@ int nb_create(const nb_params* p, uint64_t n, const double* mass, const double* 
     for (auto& e : c->phase_ev)
         if (rc == NB_OK && cudaEventCreate(&e) != cudaSuccess) rc = NB_ERR_CUDA;
     if (rc == NB_OK) rc = alloc_all(c);
+    if (rc == NB_OK && counts) rc = alloc_batch(c, nuni, counts);
     if (rc == NB_OK) rc = nb_upload(c, mass, pos_xy, vel_xy);
     if (rc != NB_OK) {
         nb_destroy(c);
@@ -338,12 +382,35 @@ int nb_create(const nb_params* p, uint64_t n, const double* mass, const double* 
     return NB_OK;
 }
 
+}  // namespace
+
+extern "C" {
+
+int nb_create(const nb_params* p, uint64_t n, const double* mass, const double* pos_xy,
+              const double* vel_xy, nb_ctx** out) {
+    return create_context(p, n, mass, pos_xy, vel_xy, 0, nullptr, out);
+}
+
+int nb_batch_create(const nb_params* p, uint32_t nuniverses, const uint64_t* counts,
+                    const double* mass, const double* pos_xy, const double* vel_xy, nb_ctx** out) {
+    if (!out || !counts || !p || nuniverses == 0 || nuniverses > (uint32_t)nb::kBatchMaxUniverses)
+        return NB_ERR_INVALID;
+    if (p->mode != NB_MODE_SPLIT || (p->flags & NB_FLAG_LEARNED)) return NB_ERR_INVALID;
+    uint64_t n = 0;
+    for (uint32_t u = 0; u < nuniverses; ++u) {
+        if (counts[u] == 0) return NB_ERR_INVALID;
+        n += counts[u];
+    }
+    return create_context(p, n, mass, pos_xy, vel_xy, nuniverses, counts, out);
+}
+
 int nb_destroy(nb_ctx* c) {
     if (!c) return NB_OK;
     DeviceGuard guard(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     drop_graphs(c);
     free_all(c);
+    free_batch(c);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     for (auto& e : c->phase_ev)
@@ -531,6 +598,68 @@ int nb_phase_times(nb_ctx* c, double* ms, int max) {
 }
 
 const char* nb_phase_name(int k) { return k >= 0 && k < nb::kPhases ? kPhaseNames[k] : ""; }
+
+int nb_autotune(nb_ctx* c, uint32_t steps, int32_t* leaf_out, int32_t* bpl_out) {
+    if (!c || steps == 0) return NB_ERR_INVALID;
+    if (c->p.mode != NB_MODE_SPLIT)
+        return fail(c, NB_ERR_INVALID, "autotuning applies to NB_MODE_SPLIT");
+    if ((c->p.flags & NB_FLAG_LEARNED) && !c->mlp_ready)
+        return fail(c, NB_ERR_INVALID, "learned mode: call nb_set_mlp_weights first");
+    DeviceGuard guard(c->device);
+    NB_CUDA(c, cudaStreamSynchronize(c->stream));
+    // the trials run on a copy of the bodies, restored afterwards
+    const size_t n = (size_t)c->n;
+    const int parity0 = c->parity;
+    const uint64_t steps0 = c->steps;
+    nb::BodyBuffers save;
+    NB_CUDA(c, dalloc(&save.pos, n));
+    NB_CUDA(c, dalloc(&save.vel, n));
+    NB_CUDA(c, dalloc(&save.mass, n));
+    NB_CUDA(c, dalloc(&save.orig, n));
+    const nb::BodyBuffers& A = c->buf[parity0];
+    cudaMemcpyAsync(save.pos, A.pos, n * 16, cudaMemcpyDeviceToDevice, c->stream);
+    cudaMemcpyAsync(save.vel, A.vel, n * 16, cudaMemcpyDeviceToDevice, c->stream);
+    cudaMemcpyAsync(save.mass, A.mass, n * 8, cudaMemcpyDeviceToDevice, c->stream);
+    cudaMemcpyAsync(save.orig, A.orig, n * 4, cudaMemcpyDeviceToDevice, c->stream);
+    const bool learned = (c->p.flags & NB_FLAG_LEARNED) != 0;
+    const int bpls[2] = {2, 1};
+    const int leaves[4] = {4, 8, 16, 32};
+    double best = 1e300;
+    int best_leaf = c->p.leaf_size, best_bpl = c->bpl;
+    int rc = NB_OK;
+    for (int bi = 0; bi < (learned ? 1 : 2) && rc == NB_OK; ++bi)
+        for (int li = 0; li < 4 && rc == NB_OK; ++li) {
+            c->bpl = bpls[bi];
+            c->p.leaf_size = leaves[li];
+            drop_graphs(c);
+            rc = nb_step(c, 1);  // warm-up (captures the graphs)
+            if (rc == NB_OK) rc = nb_step(c, steps);
+            if (rc == NB_OK) rc = nb_sync(c);
+            if (rc == NB_OK && c->ms_last < best) {
+                best = c->ms_last;
+                best_leaf = leaves[li];
+                best_bpl = bpls[bi];
+            }
+        }
+    c->bpl = best_bpl;
+    c->p.leaf_size = best_leaf;
+    drop_graphs(c);
+    c->parity = parity0;
+    c->steps = steps0;
+    const nb::BodyBuffers& R = c->buf[parity0];
+    cudaMemcpyAsync(R.pos, save.pos, n * 16, cudaMemcpyDeviceToDevice, c->stream);
+    cudaMemcpyAsync(R.vel, save.vel, n * 16, cudaMemcpyDeviceToDevice, c->stream);
+    cudaMemcpyAsync(R.mass, save.mass, n * 8, cudaMemcpyDeviceToDevice, c->stream);
+    cudaMemcpyAsync(R.orig, save.orig, n * 4, cudaMemcpyDeviceToDevice, c->stream);
+    cudaStreamSynchronize(c->stream);
+    cudaFree(save.pos);
+    cudaFree(save.vel);
+    cudaFree(save.mass);
+    cudaFree(save.orig);
+    if (leaf_out) *leaf_out = best_leaf;
+    if (bpl_out) *bpl_out = best_bpl;
+    return rc;
+}
 
 int nb_set_mlp_weights(nb_ctx* c, const float* params) {
     if (!c || !params) return NB_ERR_INVALID;

@@ -41,6 +41,27 @@ struct DeviceScalars {
     unsigned long long body_terms;
 };
 
+// Batched universes (nb_batch_create): bodies of universe u occupy the fixed
+// slot range [off[u], off[u+1]) in every step, because the sort key puts the
+// universe id above a 54-bit Morton code of the body in its own universe's
+// squared box.  The id takes the top kBatchUidDigits 2-bit digits, so a
+// universe's spatial level L is tree level L + kBatchUidDigits, and cells
+// above that level mix universes ("forest" cells, never accepted).
+constexpr int kBatchUidDigits = 5;               // 10 bits: up to 1024 universes
+constexpr int kBatchMortonBits = 27;             // per axis
+constexpr int kBatchMaxUniverses = 1 << (2 * kBatchUidDigits);
+
+struct Batch {
+    int nuni = 0;                        // 0: a single universe (the default path)
+    const int32_t* off = nullptr;        // [nuni + 1]
+    const int32_t* uid = nullptr;        // [n] universe of each body slot
+    unsigned long long* boxbits = nullptr;  // [nuni][4] order-preserving min/max of x, y
+    double2* center = nullptr;           // [nuni] squared-box centre
+    double* w2 = nullptr;                // [nuni] squared root width
+    double2* lo = nullptr;               // [nuni] squared-box lower corner
+    int32_t* root = nullptr;             // [nuni] root ref (cell, or ~first body of a leaf)
+};
+
 // Body state; two copies so the Morton gather can ping-pong.
 struct BodyBuffers {
     double2* pos = nullptr;
@@ -124,10 +145,12 @@ struct nb_ctx {
     nb::DeviceScalars* scal = nullptr;   // device
     double* bbox_partials = nullptr;     // [blocks][4]
     int bbox_blocks = 0;
-    int split_blocks[4] = {0, 0, 0, 0};  // persistent grids of the SPLIT traversal variants
+    int split_blocks[8] = {};            // persistent grids of the SPLIT traversal variants
     float* mlp_params = nullptr;         // learned mode: FP32 MLP parameters (device)
     bool mlp_ready = false;
     float2* acc32 = nullptr;             // learned mode: traversal accelerations
+    nb::Batch batch;                     // batched universes (nuni > 0)
+    int bpl = 2;                         // SPLIT: bodies per lane (group of 32 x bpl)
     double2* acc = nullptr;              // optional FP64 accelerations (sorted order)
     double2* stage_pos = nullptr;        // original-order staging for downloads
     double2* stage_vel = nullptr;
@@ -143,9 +166,23 @@ struct nb_ctx {
 
 namespace nb {
 
+// Centre of the FP32 frame of body slot i, and the squared width of a cell at
+// tree level `level` whose first body is slot i.
+__device__ __forceinline__ double2 frame_center(const DeviceScalars* s, const Batch& b, int i) {
+    if (b.nuni == 0) return make_double2(s->center[0], s->center[1]);
+    return b.center[b.uid[i]];
+}
+__device__ __forceinline__ double cell_width2(const DeviceScalars* s, const Batch& b, int i,
+                                              int level) {
+    if (b.nuni == 0) return s->wsq[level];
+    if (level < kBatchUidDigits) return __longlong_as_double(0x7ff0000000000000ll);  // +inf
+    return ldexp(b.w2[b.uid[i]], -2 * (level - kBatchUidDigits));
+}
+
 // Kernel launchers (all enqueue on ctx->stream, no host synchronisation).
 void launch_bbox(nb_ctx* c, const double2* pos);
 void launch_morton(nb_ctx* c, const double2* pos);
+void launch_batch_roots(nb_ctx* c);   // per-universe root cells after the tree build
 void launch_sort(nb_ctx* c);                                   // result in key[0]/val[0]
 void launch_gather(nb_ctx* c, const BodyBuffers& src, const BodyBuffers& dst, float4* body4);
 void launch_tree(nb_ctx* c, const BodyBuffers& b);

@@ -20,6 +20,10 @@ public:
                   uint32_t download_every = 1);
     ~BarnesHutB200() override;
 
+    // The Plummer epsilon^2 the base class derived from softening_factor
+    // (Simulation.cpp:11-15), as passed to the library.
+    double softening_squared() const { return epsilon_squared; }
+
 private:
     nb_ctx* ctx = nullptr;
     std::thread sim_thread;

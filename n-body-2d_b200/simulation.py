@@ -87,7 +87,9 @@ class SimConfig:
 class NbContext:
     """Owns one nb_ctx of libnbody_b200.so."""
 
-    def __init__(self, cfg: SimConfig, mass, pos, vel):
+    def __init__(self, cfg: SimConfig, mass, pos, vel, counts=None):
+        """counts (optional): bodies per universe for a batch of independent
+        universes concatenated in mass/pos/vel (nb_batch_create)."""
         lib = load()
         self.cfg = cfg
         self.n = int(np.asarray(mass).shape[0])
@@ -96,7 +98,14 @@ class NbContext:
         vel = _f64(vel, (self.n, 2))
         h = C.c_void_p()
         p = cfg.params()
-        check(lib.nb_create(C.byref(p), self.n, ptr(mass), ptr(pos), ptr(vel), C.byref(h)))
+        if counts is None:
+            check(lib.nb_create(C.byref(p), self.n, ptr(mass), ptr(pos), ptr(vel), C.byref(h)))
+        else:
+            cnt = np.ascontiguousarray(counts, dtype=np.uint64)
+            if int(cnt.sum()) != self.n:
+                raise ValueError("universe sizes must add up to the body count")
+            check(lib.nb_batch_create(C.byref(p), cnt.shape[0], ptr(cnt), ptr(mass), ptr(pos),
+                                      ptr(vel), C.byref(h)))
         self._h = h.value
         self._lib = lib
 
@@ -193,6 +202,13 @@ class NbContext:
         if k < 0:
             check(-k, self._h)
         return {self._lib.nb_phase_name(i).decode(): float(ms[i]) for i in range(k)}
+
+    def autotune(self, steps: int = 3) -> tuple[int, int]:
+        """Times the SPLIT leaf sizes and group sizes; returns (leaf, bodies per lane)."""
+        leaf, bpl = C.c_int32(), C.c_int32()
+        check(self._lib.nb_autotune(self.handle, steps, C.addressof(leaf), C.addressof(bpl)),
+              self._h)
+        return leaf.value, bpl.value
 
     # -- learned correction -----------------------------------------------
     def set_mlp_weights(self, params: np.ndarray) -> None:

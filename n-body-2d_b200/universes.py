@@ -98,6 +98,15 @@ def ensemble(count: int, seed: int, nmin: int = 1024, nmax: int = 262144) -> lis
             for k in range(count)]
 
 
+def ensemble_batch(count: int, seed: int, nmin: int = 1024, nmax: int = 262144):
+    """The ensemble concatenated in universe order, as nb_batch_create takes it:
+    (mass[N], pos[N, 2], vel[N, 2], counts[count] uint64)."""
+    unis = ensemble(count, seed, nmin, nmax)
+    counts = np.array([u[0].shape[0] for u in unis], dtype=np.uint64)
+    m, p, v = (np.ascontiguousarray(np.concatenate(x)) for x in zip(*unis))
+    return m, p, v, counts
+
+
 # The five workloads of the benchmark description, by name.
 WORKLOADS = {
     "disc16k": dict(n=16384, kind="disc", theta=0.5, steps=1000),

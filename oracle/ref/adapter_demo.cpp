@@ -7,7 +7,9 @@
 // Usage: adapter_demo <input> <output>; formats as ref_cpu_bh.cpp (the
 // header's "warmup" word selects the mode: 0 FP64, 1 SPLIT).  The reference
 // hard-wires G; masses are scaled by G / Constants::Simulation::G.  The
-// softening factor is 0, so epsilon^2 = 0 in this demo.
+// second parameter word is the reference's softening_factor; the base class
+// turns it into epsilon^2 (sampled mean pair distance x factor, squared),
+// which the output carries after the run time: seconds, eps2, pos, vel.
 #include <chrono>
 #include <cstdint>
 #include <cstdio>
@@ -48,11 +50,12 @@ int main(int argc, char** argv) {
     cfg.timestep = par[2];
     cfg.iterations = (uint64_t)steps;
     cfg.theta = par[0];
-    cfg.softening_factor = 0.0;
+    cfg.softening_factor = par[1];
     cfg.threads = 1;
-    double seconds = 0.0;
+    double seconds = 0.0, eps2 = 0.0;
     {
         BarnesHutB200 sim(cfg, bodies, mode ? NB_MODE_SPLIT : NB_MODE_FP64, 1);
+        eps2 = sim.softening_squared();
         const auto t0 = std::chrono::steady_clock::now();
         sim.run();
         while (!sim.is_finished()) std::this_thread::sleep_for(std::chrono::microseconds(100));
@@ -61,6 +64,7 @@ int main(int argc, char** argv) {
     std::FILE* out = std::fopen(argv[2], "wb");
     if (!out) return 6;
     std::fwrite(&seconds, 8, 1, out);
+    std::fwrite(&eps2, 8, 1, out);
     std::fwrite(bodies.pos_data(), 8, 2 * n, out);
     std::fwrite(bodies.vel_data(), 8, 2 * n, out);
     std::fclose(out);

@@ -52,3 +52,23 @@ def test_invalid_arguments_rejected_before_any_device_call(nbp):
     assert lib.nb_create(C.byref(p), 0, one, one, one, C.byref(h)) == 1
     assert lib.nb_create(None, 1, one, one, one, C.byref(h)) == 1
     assert lib.nb_destroy(None) == 0
+
+
+def test_batch_create_rejects_bad_batches_before_any_device_call(nbp):
+    lib = nbp.load()
+    h = C.c_void_p()
+    p = nbp.NbParams()
+    lib.nb_params_default(C.byref(p))
+    one = (C.c_double * 8)(*([0.0] * 8))
+    counts = (C.c_uint64 * 2)(1, 1)
+    # FP64 parity mode holds one universe
+    assert lib.nb_batch_create(C.byref(p), 2, counts, one, one, one, C.byref(h)) == 1
+    p.mode = nbp.NB_MODE_SPLIT
+    assert lib.nb_batch_create(C.byref(p), 0, counts, one, one, one, C.byref(h)) == 1
+    assert lib.nb_batch_create(C.byref(p), 1025, counts, one, one, one, C.byref(h)) == 1
+    assert lib.nb_batch_create(C.byref(p), 2, None, one, one, one, C.byref(h)) == 1
+    empty = (C.c_uint64 * 2)(1, 0)
+    assert lib.nb_batch_create(C.byref(p), 2, empty, one, one, one, C.byref(h)) == 1
+    p.flags = nbp.NB_FLAG_LEARNED
+    assert lib.nb_batch_create(C.byref(p), 2, counts, one, one, one, C.byref(h)) == 1
+    assert lib.nb_autotune(None, 1, None, None) == 1

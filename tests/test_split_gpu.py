@@ -12,8 +12,8 @@ pytestmark = pytest.mark.gpu
 EPS2 = 1e-4
 
 
-def accel(nbp, m, p, v, mode, theta, quad=False, leaf=0):
-    cfg = nbp.SimConfig(theta=theta, epsilon_squared=EPS2, mode=mode, quadrupole=quad,
+def accel(nbp, m, p, v, mode, theta, quad=False, leaf=0, eps2=EPS2):
+    cfg = nbp.SimConfig(theta=theta, epsilon_squared=eps2, mode=mode, quadrupole=quad,
                         leaf_size=leaf)
     with nbp.NbContext(cfg, m, p, v) as ctx:
         a = ctx.accelerations()
@@ -90,3 +90,21 @@ def test_split_coincident_and_ragged(nbp, orc):
     center = (0.5 * (box[0] + box[1]), 0.5 * (box[2] + box[3]))
     bound = orc.allpairs_fp32_bound(m, p, center, eps2=EPS2)
     assert (np.linalg.norm(a - exact, axis=1) <= bound).all()
+
+
+def test_split_zero_softening_coincident_bodies_add_nothing(nbp):
+    """eps^2 = 0: bodies that share FP32 coordinates (here: exactly coincident
+    pairs) add nothing to each other instead of 0 * inf; every other pair
+    follows the unsoftened law."""
+    rng = np.random.default_rng(6)
+    n = 2000
+    p = rng.random((n, 2))
+    p[1000:1010] = p[:10]
+    m = rng.random(n) + 0.5
+    a, _ = accel(nbp, m, p, np.zeros((n, 2)), nbp.NB_MODE_SPLIT, 0.0, leaf=1, eps2=0.0)
+    assert np.isfinite(a).all()
+    d = p[None, :, :] - p[:, None, :]
+    r2 = (d * d).sum(-1)
+    w = np.where(r2 > 0, m[None, :] / np.where(r2 > 0, r2, 1.0) ** 1.5, 0.0)
+    exact = (w[:, :, None] * d).sum(1)
+    assert np.percentile(rel_err(a, exact), 99) < 1e-3
