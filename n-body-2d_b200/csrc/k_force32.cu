@@ -34,12 +34,31 @@ constexpr int kList = 64;
 constexpr int kBodiesPerLane = 2;      // group of 64 bodies per warp
 constexpr int kDefaultLeaf = 8;        // cells this small are summed body by body
 
+// Interaction lists hold entries in pairs, so that one lane evaluates two
+// entries with the packed FP32x2 instructions of sm_100 (FADD2/FMUL2/FFMA2):
+// pair k is xy[k] = (x0, x1, y0, y1) and m[k] = (m0, m1), with the quadrupole
+// (xx0, xx1, xy0, xy1) in qa[k] and (yy0, yy1) in qb[k].
 struct WarpLists {
     int stack[kStkAlloc];
-    float4 cell[kList];
-    float4 quad[kList];
-    float4 body[kList];
+    float4 cxy[kList / 2];
+    float2 cm[kList / 2];
+    float4 qa[kList / 2];
+    float2 qb[kList / 2];
+    float4 bxy[kList / 2];
+    float2 bm[kList / 2];
 };
+
+// An entry that adds nothing: zero mass far away, so that d2 stays finite
+// and positive whatever eps2 is (it completes a pair at an odd count).
+constexpr float kPadCoord = 1e15f;
+
+__device__ __forceinline__ void put_entry(float4* xy, float2* m, int slot, float x, float y,
+                                          float mass) {
+    float* f = reinterpret_cast<float*>(xy + (slot >> 1));
+    f[slot & 1] = x;
+    f[2 + (slot & 1)] = y;
+    reinterpret_cast<float*>(m)[slot] = mass;
+}
 
 __device__ __forceinline__ unsigned lanemask_lt() {
     unsigned m;
@@ -70,82 +89,106 @@ __device__ __forceinline__ float warp_max(float v) {
     return v;
 }
 
-// Sum cnt cell entries into the accelerations of the lane's kBPL bodies.
-template <bool kQuad, int kBPL>
-__device__ __forceinline__ void cell_terms(const float4 e, const float4 q, const float* px,
-                                           const float* py, float eps2, float* ax, float* ay) {
+// One pair of list entries against the lane's kBPL bodies.  nx/ny hold the
+// negated body coordinates broadcast to both halves.  Each half follows the
+// scalar law d2 = dx^2 + (dy^2 + eps2), a = (m / r^2) / r of the reference's
+// pair term (CU:427-431) with the same rounding; the halves are separate
+// partial sums.  kZeroSoft: eps2 = 0, where an entry at the body's own FP32
+// coordinates (the body itself, or one that coincides with it at FP32
+// resolution) adds nothing instead of 0 * inf.  With eps2 > 0 the body's own
+// entry has dx = dy = 0 exactly and adds 0 without a test.
+template <bool kZeroSoft, int kBPL>
+__device__ __forceinline__ void mono_pair(const float4 xy, const float2 m, const float2* nx,
+                                          const float2* ny, const float2 e2, float2* ax,
+                                          float2* ay) {
+    const float2 ex = make_float2(xy.x, xy.y), ey = make_float2(xy.z, xy.w);
 #pragma unroll
     for (int b = 0; b < kBPL; ++b) {
-        const float dx = e.x - px[b], dy = e.y - py[b];
-        const float d2 = fmaf(dx, dx, fmaf(dy, dy, eps2));
-        const float inv = rsqrtf(d2);
-        const float inv2 = inv * inv;
-        const float inv3 = inv * inv2;
-        if (kQuad) {
-            const float inv5 = inv3 * inv2;
-            const float inv7 = inv5 * inv2;
-            const float sdx = fmaf(q.x, dx, q.y * dy);
-            const float sdy = fmaf(q.y, dx, q.z * dy);
-            const float dsd = fmaf(dx, sdx, dy * sdy);
-            // a = d [M r^-3 - 1.5 tr(S) r^-5 + 7.5 (d.S.d) r^-7] - 3 r^-5 S d
-            const float radial =
-                fmaf(7.5f * dsd, inv7, fmaf(-1.5f * (q.x + q.z), inv5, e.z * inv3));
-            ax[b] = fmaf(dx, radial, fmaf(-3.f * inv5, sdx, ax[b]));
-            ay[b] = fmaf(dy, radial, fmaf(-3.f * inv5, sdy, ay[b]));
-        } else {
-            const float a = e.z * inv3;
-            ax[b] = fmaf(dx, a, ax[b]);
-            ay[b] = fmaf(dy, a, ay[b]);
+        const float2 dx = __fadd2_rn(ex, nx[b]);
+        const float2 dy = __fadd2_rn(ey, ny[b]);
+        const float2 d2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, e2));
+        const float2 inv = make_float2(rsqrtf(d2.x), rsqrtf(d2.y));
+        float2 a = __fmul2_rn(__fmul2_rn(m, __fmul2_rn(inv, inv)), inv);
+        if (kZeroSoft) {
+            a.x = d2.x == 0.f ? 0.f : a.x;
+            a.y = d2.y == 0.f ? 0.f : a.y;
+        }
+        ax[b] = __ffma2_rn(dx, a, ax[b]);
+        ay[b] = __ffma2_rn(dy, a, ay[b]);
+    }
+}
+
+// Monopole plus the second-moment term of the softened potential:
+// a = d [M r^-3 - 1.5 tr(S) r^-5 + 7.5 (d.S.d) r^-7] - 3 r^-5 S d.
+template <int kBPL>
+__device__ __forceinline__ void quad_pair(const float4 xy, const float2 m, const float4 qa,
+                                          const float2 qb, const float2* nx, const float2* ny,
+                                          const float2 e2, float2* ax, float2* ay) {
+    const float2 ex = make_float2(xy.x, xy.y), ey = make_float2(xy.z, xy.w);
+    const float2 qxx = make_float2(qa.x, qa.y), qxy = make_float2(qa.z, qa.w), qyy = qb;
+    const float2 tr = __fmul2_rn(make_float2(-1.5f, -1.5f), __fadd2_rn(qxx, qyy));
+    const float2 m3 = make_float2(-3.f, -3.f), c75 = make_float2(7.5f, 7.5f);
+#pragma unroll
+    for (int b = 0; b < kBPL; ++b) {
+        const float2 dx = __fadd2_rn(ex, nx[b]);
+        const float2 dy = __fadd2_rn(ey, ny[b]);
+        const float2 d2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, e2));
+        const float2 inv = make_float2(rsqrtf(d2.x), rsqrtf(d2.y));
+        const float2 inv2 = __fmul2_rn(inv, inv);
+        const float2 inv3 = __fmul2_rn(inv, inv2);
+        const float2 inv5 = __fmul2_rn(inv3, inv2);
+        const float2 inv7 = __fmul2_rn(inv5, inv2);
+        const float2 sdx = __ffma2_rn(qxx, dx, __fmul2_rn(qxy, dy));
+        const float2 sdy = __ffma2_rn(qxy, dx, __fmul2_rn(qyy, dy));
+        const float2 dsd = __ffma2_rn(dx, sdx, __fmul2_rn(dy, sdy));
+        const float2 radial = __ffma2_rn(__fmul2_rn(c75, dsd), inv7,
+                                         __ffma2_rn(tr, inv5, __fmul2_rn(m, inv3)));
+        const float2 t5 = __fmul2_rn(m3, inv5);
+        ax[b] = __ffma2_rn(dx, radial, __ffma2_rn(t5, sdx, ax[b]));
+        ay[b] = __ffma2_rn(dy, radial, __ffma2_rn(t5, sdy, ay[b]));
+    }
+}
+
+// Sum the first npairs pairs of the cell list.
+template <bool kQuad, int kBPL>
+__device__ __forceinline__ void sum_cells(const WarpLists& L, int npairs, const float2* nx,
+                                          const float2* ny, const float2 e2, float2* ax,
+                                          float2* ay) {
+    if (npairs == 16) {
+#pragma unroll 4
+        for (int k = 0; k < 16; ++k) {
+            if (kQuad)
+                quad_pair<kBPL>(L.cxy[k], L.cm[k], L.qa[k], L.qb[k], nx, ny, e2, ax, ay);
+            else
+                mono_pair<false, kBPL>(L.cxy[k], L.cm[k], nx, ny, e2, ax, ay);
+        }
+    } else {
+        for (int k = 0; k < npairs; ++k) {
+            if (kQuad)
+                quad_pair<kBPL>(L.cxy[k], L.cm[k], L.qa[k], L.qb[k], nx, ny, e2, ax, ay);
+            else
+                mono_pair<false, kBPL>(L.cxy[k], L.cm[k], nx, ny, e2, ax, ay);
         }
     }
 }
 
-// A body's own entry has dx = dy = 0 exactly (body4 and px/py round the same
-// double difference), so with eps2 > 0 it adds 0 * finite = 0 and needs no
-// index test.  d2 == 0 (eps2 = 0 and the same FP32 coordinates: the body
-// itself, or a body that coincides with it at FP32 resolution) contributes
-// nothing instead of 0 * inf.
-template <int kBPL>
-__device__ __forceinline__ void body_terms(const float4 e, const float* px, const float* py,
-                                           float eps2, float* ax, float* ay) {
-#pragma unroll
-    for (int b = 0; b < kBPL; ++b) {
-        const float dx = e.x - px[b], dy = e.y - py[b];
-        const float d2 = fmaf(dx, dx, fmaf(dy, dy, eps2));
-        const float inv = rsqrtf(d2);
-        const float a = d2 == 0.f ? 0.f : e.z * (inv * inv) * inv;
-        ax[b] = fmaf(dx, a, ax[b]);
-        ay[b] = fmaf(dy, a, ay[b]);
-    }
-}
-
-template <bool kQuad, int kBPL>
-__device__ __forceinline__ void sum_cells(const WarpLists& L, int cnt, const float* px,
-                                          const float* py, float eps2, float* ax, float* ay) {
-    if (cnt == 32) {
+template <bool kZeroSoft, int kBPL>
+__device__ __forceinline__ void sum_bodies(const WarpLists& L, int npairs, const float2* nx,
+                                           const float2* ny, const float2 e2, float2* ax,
+                                           float2* ay) {
+    if (npairs == 16) {
 #pragma unroll 4
-        for (int j = 0; j < 32; ++j)
-            cell_terms<kQuad, kBPL>(L.cell[j], kQuad ? L.quad[j] : L.cell[j], px, py, eps2, ax, ay);
+        for (int k = 0; k < 16; ++k)
+            mono_pair<kZeroSoft, kBPL>(L.bxy[k], L.bm[k], nx, ny, e2, ax, ay);
     } else {
-        for (int j = 0; j < cnt; ++j)
-            cell_terms<kQuad, kBPL>(L.cell[j], kQuad ? L.quad[j] : L.cell[j], px, py, eps2, ax, ay);
-    }
-}
-
-template <int kBPL>
-__device__ __forceinline__ void sum_bodies(const WarpLists& L, int cnt, const float* px,
-                                           const float* py, float eps2, float* ax, float* ay) {
-    if (cnt == 32) {
-#pragma unroll 4
-        for (int j = 0; j < 32; ++j) body_terms<kBPL>(L.body[j], px, py, eps2, ax, ay);
-    } else {
-        for (int j = 0; j < cnt; ++j) body_terms<kBPL>(L.body[j], px, py, eps2, ax, ay);
+        for (int k = 0; k < npairs; ++k)
+            mono_pair<kZeroSoft, kBPL>(L.bxy[k], L.bm[k], nx, ny, e2, ax, ay);
     }
 }
 
 // Walk the tree for one group [g0, g1] of <= 32 kBPL bodies (lane l owns
 // g0 + l, g0 + 32 + l, ...) and accumulate the FP32 accelerations.
-template <bool kQuad, int kBPL, bool kLearned>
+template <bool kQuad, int kBPL, bool kLearned, bool kZeroSoft>
 __device__ __forceinline__ void walk_group(WarpLists& L, const Tree& t, int root, int n, int g0,
                                            int g1, const float* px, const float* py,
                                            const bool* act_body, float eps2, float theta2,
@@ -169,11 +212,16 @@ __device__ __forceinline__ void walk_group(WarpLists& L, const Tree& t, int root
     const float gcx = 0.5f * (bx0 + bx1), gcy = 0.5f * (by0 + by1);
     const float ghx = 0.5f * (bx1 - bx0), ghy = 0.5f * (by1 - by0);
     const unsigned below = lanemask_lt();
+    // packed operands: the body broadcast to both halves, negated
+    float2 nx[kBPL], ny[kBPL], ax2[kBPL], ay2[kBPL];
 #pragma unroll
     for (int b = 0; b < kBPL; ++b) {
-        ax[b] = 0.f;
-        ay[b] = 0.f;
+        nx[b] = make_float2(-px[b], -px[b]);
+        ny[b] = make_float2(-py[b], -py[b]);
+        ax2[b] = make_float2(0.f, 0.f);
+        ay2[b] = make_float2(0.f, 0.f);
     }
+    const float2 e2 = make_float2(eps2, eps2);
     ncell = 0;
     npair = 0;
     int ccount = 0, bcount = 0, size = 1;
@@ -221,8 +269,11 @@ __device__ __forceinline__ void walk_group(WarpLists& L, const Tree& t, int root
         const unsigned acc_mask = __ballot_sync(kFull, act == 1);
         if (act == 1) {
             const int slot = ccount + __popc(acc_mask & below);
-            L.cell[slot] = c4;
-            if (kQuad) L.quad[slot] = t.cellq[ref];
+            put_entry(L.cxy, L.cm, slot, c4.x, c4.y, c4.z);
+            if (kQuad) {
+                const float4 q = t.cellq[ref];
+                put_entry(L.qa, L.qb, slot, q.x, q.y, q.z);
+            }
         }
         if (kLearned) {
             // band: accepted here but opened by the plain theta_B walk
@@ -237,13 +288,17 @@ __device__ __forceinline__ void walk_group(WarpLists& L, const Tree& t, int root
         ccount += __popc(acc_mask);
         __syncwarp();
         if (ccount >= 32) {
-            sum_cells<kQuad, kBPL>(L, 32, px, py, eps2, ax, ay);
+            sum_cells<kQuad, kBPL>(L, 16, nx, ny, e2, ax2, ay2);
             ncell += 32;
             __syncwarp();
-            // entries 32.. move down; source and destination slots never overlap
-            if (lane < ccount - 32) {
-                L.cell[lane] = L.cell[32 + lane];
-                if (kQuad) L.quad[lane] = L.quad[32 + lane];
+            // pairs 16.. move down; source and destination never overlap
+            if (lane < (ccount - 31) / 2) {
+                L.cxy[lane] = L.cxy[16 + lane];
+                L.cm[lane] = L.cm[16 + lane];
+                if (kQuad) {
+                    L.qa[lane] = L.qa[16 + lane];
+                    L.qb[lane] = L.qb[16 + lane];
+                }
             }
             ccount -= 32;
             __syncwarp();
@@ -280,29 +335,49 @@ __device__ __forceinline__ void walk_group(WarpLists& L, const Tree& t, int root
             const int j = __shfl_sync(kFull, bfirst, owner) + item - __shfl_sync(kFull, boff, owner);
             const int added = min(32, btot - base);
             __syncwarp();
-            if (lane < added) L.body[bcount + lane] = t.body4[j];
+            if (lane < added) {
+                const float4 b4 = t.body4[j];
+                put_entry(L.bxy, L.bm, bcount + lane, b4.x, b4.y, b4.z);
+            }
             bcount += added;
             __syncwarp();
             if (bcount >= 32) {
-                sum_bodies<kBPL>(L, 32, px, py, eps2, ax, ay);
+                sum_bodies<kZeroSoft, kBPL>(L, 16, nx, ny, e2, ax2, ay2);
                 npair += 32;
                 __syncwarp();
-                if (lane < bcount - 32) L.body[lane] = L.body[32 + lane];
+                if (lane < (bcount - 31) / 2) {
+                    L.bxy[lane] = L.bxy[16 + lane];
+                    L.bm[lane] = L.bm[16 + lane];
+                }
                 bcount -= 32;
                 __syncwarp();
             }
         }
     }
-    sum_cells<kQuad, kBPL>(L, ccount, px, py, eps2, ax, ay);
-    sum_bodies<kBPL>(L, bcount, px, py, eps2, ax, ay);
+    // odd counts: a padding entry completes the last pair
+    if (lane == 0) {
+        if (ccount & 1) {
+            put_entry(L.cxy, L.cm, ccount, kPadCoord, kPadCoord, 0.f);
+            if (kQuad) put_entry(L.qa, L.qb, ccount, 0.f, 0.f, 0.f);
+        }
+        if (bcount & 1) put_entry(L.bxy, L.bm, bcount, kPadCoord, kPadCoord, 0.f);
+    }
+    __syncwarp();
+    sum_cells<kQuad, kBPL>(L, (ccount + 1) >> 1, nx, ny, e2, ax2, ay2);
+    sum_bodies<kZeroSoft, kBPL>(L, (bcount + 1) >> 1, nx, ny, e2, ax2, ay2);
     ncell += ccount;
     npair += bcount;
+#pragma unroll
+    for (int b = 0; b < kBPL; ++b) {
+        ax[b] = ax2[b].x + ax2[b].y;
+        ay[b] = ay2[b].x + ay2[b].y;
+    }
     __syncwarp();
 }
 
 // Persistent: each warp takes groups from a global ticket until none is left,
 // which balances groups of very different cost.
-template <bool kQuad, int kBPL, bool kLearned>
+template <bool kQuad, int kBPL, bool kLearned, bool kZeroSoft>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32)
 force_split(double2* __restrict__ pos, double2* __restrict__ vel, double2* __restrict__ acc_out,
             float2* __restrict__ acc32, int n, Tree t, DeviceScalars* __restrict__ s, Batch bt,
@@ -338,7 +413,7 @@ force_split(double2* __restrict__ pos, double2* __restrict__ vel, double2* __res
         unsigned long long ncell, npair;
         int nband = 0;
         int* band = kLearned ? t.band + (int64_t)kBandPerBody * g0 : nullptr;
-        walk_group<kQuad, kBPL, kLearned>(L, t, root, n, g0, g1, px, py, on, eps2, theta2,
+        walk_group<kQuad, kBPL, kLearned, kZeroSoft>(L, t, root, n, g0, g1, px, py, on, eps2, theta2,
                                           leaf_size, ax, ay, ncell, npair, &s->error, band, nband,
                                           kBandPerBody * (g1 - g0 + 1));
         if (kLearned) {
@@ -375,23 +450,34 @@ force_split(double2* __restrict__ pos, double2* __restrict__ vel, double2* __res
     }
 }
 
-template <bool kQuad, int kBPL, bool kLearned>
-void launch_split_kernel(nb_ctx* c, const BodyBuffers& b, bool kick, bool store_acc) {
-    int& grid = c->split_blocks[(kQuad ? 1 : 0) + (kLearned ? 2 : 0) + (kBPL == 1 ? 4 : 0)];
+template <bool kQuad, int kBPL, bool kLearned, bool kZeroSoft>
+void launch_split_soft(nb_ctx* c, const BodyBuffers& b, bool kick, bool store_acc, float eps2) {
+    int& grid = c->split_blocks[(kQuad ? 1 : 0) + (kLearned ? 2 : 0) + (kBPL == 1 ? 4 : 0) +
+                                (kZeroSoft ? 8 : 0)];
     if (grid == 0) {
         int blocks = 0;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                &blocks, force_split<kQuad, kBPL, kLearned>, kWarpsPerBlock * 32, 0) != cudaSuccess ||
+                &blocks, force_split<kQuad, kBPL, kLearned, kZeroSoft>, kWarpsPerBlock * 32, 0) !=
+                    cudaSuccess ||
             blocks < 1)
             blocks = 4;
         grid = c->sm_count * blocks;
     }
     const float theta2 = (float)(c->p.theta * c->p.theta);
     const int leaf = c->p.leaf_size > 0 ? c->p.leaf_size : kDefaultLeaf;
-    force_split<kQuad, kBPL, kLearned><<<grid, 32 * kWarpsPerBlock, 0, c->stream>>>(
+    force_split<kQuad, kBPL, kLearned, kZeroSoft><<<grid, 32 * kWarpsPerBlock, 0, c->stream>>>(
         b.pos, b.vel, store_acc ? c->acc : nullptr, c->acc32, (int)c->n, c->tree, c->scal, c->batch,
-        (float)c->p.epsilon_squared, theta2, leaf, c->p.G * c->p.timestep, c->p.timestep,
-        kick ? 1 : 0);
+        eps2, theta2, leaf, c->p.G * c->p.timestep, c->p.timestep, kick ? 1 : 0);
+}
+
+// eps2 = 0 takes the variant whose body terms skip coincident FP32 points
+template <bool kQuad, int kBPL, bool kLearned>
+void launch_split_kernel(nb_ctx* c, const BodyBuffers& b, bool kick, bool store_acc) {
+    const float eps2 = (float)c->p.epsilon_squared;
+    if (eps2 > 0.f)
+        launch_split_soft<kQuad, kBPL, kLearned, false>(c, b, kick, store_acc, eps2);
+    else
+        launch_split_soft<kQuad, kBPL, kLearned, true>(c, b, kick, store_acc, eps2);
 }
 
 }  // namespace

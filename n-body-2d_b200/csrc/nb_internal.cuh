@@ -145,7 +145,7 @@ struct nb_ctx {
     nb::DeviceScalars* scal = nullptr;   // device
     double* bbox_partials = nullptr;     // [blocks][4]
     int bbox_blocks = 0;
-    int split_blocks[8] = {};            // persistent grids of the SPLIT traversal variants
+    int split_blocks[16] = {};            // persistent grids of the SPLIT traversal variants
     float* mlp_params = nullptr;         // learned mode: FP32 MLP parameters (device)
     bool mlp_ready = false;
     float2* acc32 = nullptr;             // learned mode: traversal accelerations
