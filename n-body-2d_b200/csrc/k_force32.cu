@@ -17,6 +17,7 @@
 // monopole (the reference's pair law, CU:427-431) and, with quadrupoles on,
 // the second-moment term of the softened potential.  Accelerations
 // accumulate in FP32; velocities and positions are updated in FP64.
+#include <cfloat>
 #include <climits>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -51,6 +52,17 @@ struct WarpLists {
 // An entry that adds nothing: zero mass far away, so that d2 stays finite
 // and positive whatever eps2 is (it completes a pair at an odd count).
 constexpr float kPadCoord = 1e15f;
+
+// 1/sqrt(x) on the special-function unit.  kExact keeps subnormal x (the
+// eps2 = 0 variant, where d2 can be that small); otherwise x >= eps2 is a
+// normal float and the flush-to-zero form saves the subnormal handling.
+template <bool kExact>
+__device__ __forceinline__ float rsq(float x) {
+    if (kExact) return rsqrtf(x);
+    float r;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
 
 __device__ __forceinline__ void put_entry(float4* xy, float2* m, int slot, float x, float y,
                                           float mass) {
@@ -95,8 +107,9 @@ __device__ __forceinline__ float warp_max(float v) {
 // pair term (CU:427-431) with the same rounding; the halves are separate
 // partial sums.  kZeroSoft: eps2 = 0, where an entry at the body's own FP32
 // coordinates (the body itself, or one that coincides with it at FP32
-// resolution) adds nothing instead of 0 * inf.  With eps2 > 0 the body's own
-// entry has dx = dy = 0 exactly and adds 0 without a test.
+// resolution) adds nothing instead of 0 * inf, and 1/sqrt keeps subnormal
+// arguments.  With eps2 > 0 the body's own entry has dx = dy = 0 exactly and
+// adds 0 without a test.
 template <bool kZeroSoft, int kBPL>
 __device__ __forceinline__ void mono_pair(const float4 xy, const float2 m, const float2* nx,
                                           const float2* ny, const float2 e2, float2* ax,
@@ -107,7 +120,7 @@ __device__ __forceinline__ void mono_pair(const float4 xy, const float2 m, const
         const float2 dx = __fadd2_rn(ex, nx[b]);
         const float2 dy = __fadd2_rn(ey, ny[b]);
         const float2 d2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, e2));
-        const float2 inv = make_float2(rsqrtf(d2.x), rsqrtf(d2.y));
+        const float2 inv = make_float2(rsq<kZeroSoft>(d2.x), rsq<kZeroSoft>(d2.y));
         float2 a = __fmul2_rn(__fmul2_rn(m, __fmul2_rn(inv, inv)), inv);
         if (kZeroSoft) {
             a.x = d2.x == 0.f ? 0.f : a.x;
@@ -120,7 +133,7 @@ __device__ __forceinline__ void mono_pair(const float4 xy, const float2 m, const
 
 // Monopole plus the second-moment term of the softened potential:
 // a = d [M r^-3 - 1.5 tr(S) r^-5 + 7.5 (d.S.d) r^-7] - 3 r^-5 S d.
-template <int kBPL>
+template <bool kZeroSoft, int kBPL>
 __device__ __forceinline__ void quad_pair(const float4 xy, const float2 m, const float4 qa,
                                           const float2 qb, const float2* nx, const float2* ny,
                                           const float2 e2, float2* ax, float2* ay) {
@@ -133,7 +146,7 @@ __device__ __forceinline__ void quad_pair(const float4 xy, const float2 m, const
         const float2 dx = __fadd2_rn(ex, nx[b]);
         const float2 dy = __fadd2_rn(ey, ny[b]);
         const float2 d2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, e2));
-        const float2 inv = make_float2(rsqrtf(d2.x), rsqrtf(d2.y));
+        const float2 inv = make_float2(rsq<kZeroSoft>(d2.x), rsq<kZeroSoft>(d2.y));
         const float2 inv2 = __fmul2_rn(inv, inv);
         const float2 inv3 = __fmul2_rn(inv, inv2);
         const float2 inv5 = __fmul2_rn(inv3, inv2);
@@ -150,7 +163,7 @@ __device__ __forceinline__ void quad_pair(const float4 xy, const float2 m, const
 }
 
 // Sum the first npairs pairs of the cell list.
-template <bool kQuad, int kBPL>
+template <bool kQuad, bool kZeroSoft, int kBPL>
 __device__ __forceinline__ void sum_cells(const WarpLists& L, int npairs, const float2* nx,
                                           const float2* ny, const float2 e2, float2* ax,
                                           float2* ay) {
@@ -158,16 +171,18 @@ __device__ __forceinline__ void sum_cells(const WarpLists& L, int npairs, const 
 #pragma unroll 4
         for (int k = 0; k < 16; ++k) {
             if (kQuad)
-                quad_pair<kBPL>(L.cxy[k], L.cm[k], L.qa[k], L.qb[k], nx, ny, e2, ax, ay);
+                quad_pair<kZeroSoft, kBPL>(L.cxy[k], L.cm[k], L.qa[k], L.qb[k], nx, ny, e2, ax,
+                                           ay);
             else
-                mono_pair<false, kBPL>(L.cxy[k], L.cm[k], nx, ny, e2, ax, ay);
+                mono_pair<kZeroSoft, kBPL>(L.cxy[k], L.cm[k], nx, ny, e2, ax, ay);
         }
     } else {
         for (int k = 0; k < npairs; ++k) {
             if (kQuad)
-                quad_pair<kBPL>(L.cxy[k], L.cm[k], L.qa[k], L.qb[k], nx, ny, e2, ax, ay);
+                quad_pair<kZeroSoft, kBPL>(L.cxy[k], L.cm[k], L.qa[k], L.qb[k], nx, ny, e2, ax,
+                                           ay);
             else
-                mono_pair<false, kBPL>(L.cxy[k], L.cm[k], nx, ny, e2, ax, ay);
+                mono_pair<kZeroSoft, kBPL>(L.cxy[k], L.cm[k], nx, ny, e2, ax, ay);
         }
     }
 }
@@ -288,7 +303,7 @@ __device__ __forceinline__ void walk_group(WarpLists& L, const Tree& t, int root
         ccount += __popc(acc_mask);
         __syncwarp();
         if (ccount >= 32) {
-            sum_cells<kQuad, kBPL>(L, 16, nx, ny, e2, ax2, ay2);
+            sum_cells<kQuad, kZeroSoft, kBPL>(L, 16, nx, ny, e2, ax2, ay2);
             ncell += 32;
             __syncwarp();
             // pairs 16.. move down; source and destination never overlap
@@ -363,7 +378,7 @@ __device__ __forceinline__ void walk_group(WarpLists& L, const Tree& t, int root
         if (bcount & 1) put_entry(L.bxy, L.bm, bcount, kPadCoord, kPadCoord, 0.f);
     }
     __syncwarp();
-    sum_cells<kQuad, kBPL>(L, (ccount + 1) >> 1, nx, ny, e2, ax2, ay2);
+    sum_cells<kQuad, kZeroSoft, kBPL>(L, (ccount + 1) >> 1, nx, ny, e2, ax2, ay2);
     sum_bodies<kZeroSoft, kBPL>(L, (bcount + 1) >> 1, nx, ny, e2, ax2, ay2);
     ncell += ccount;
     npair += bcount;
@@ -470,11 +485,12 @@ void launch_split_soft(nb_ctx* c, const BodyBuffers& b, bool kick, bool store_ac
         eps2, theta2, leaf, c->p.G * c->p.timestep, c->p.timestep, kick ? 1 : 0);
 }
 
-// eps2 = 0 takes the variant whose body terms skip coincident FP32 points
+// eps2 = 0 takes the variant whose terms skip coincident FP32 points
 template <bool kQuad, int kBPL, bool kLearned>
 void launch_split_kernel(nb_ctx* c, const BodyBuffers& b, bool kick, bool store_acc) {
+    // eps2 below the smallest normal float is treated like eps2 = 0
     const float eps2 = (float)c->p.epsilon_squared;
-    if (eps2 > 0.f)
+    if (eps2 >= FLT_MIN)
         launch_split_soft<kQuad, kBPL, kLearned, false>(c, b, kick, store_acc, eps2);
     else
         launch_split_soft<kQuad, kBPL, kLearned, true>(c, b, kick, store_acc, eps2);

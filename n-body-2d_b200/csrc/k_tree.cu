@@ -293,13 +293,14 @@ __global__ void tree_trivial_root(const double2* __restrict__ pos, const double*
 
 // Moments of one cell from its children, in quadrant order, with the
 // reference's arithmetic (CU:329-343): M += m; R = fma(m, com, R); com = R / M.
-// kSplit also accumulates second moments about the COM by the parallel-axis
-// rule, S = sum_c [S_c + m_c d_c d_c^T] with d_c = com_c - com, in FP64, and
-// packs the FP32 records the group traversal reads.  Leaves have S = 0 (a
-// multi-body leaf spans less than width / 2^30, so its own S is negligible).
-// Children are read with L2-coherent loads: they were written by other
-// threads of this launch (climb) or of an earlier launch (per level).
-template <bool kSplit, bool kFeat>
+// kSplit packs the FP32 records the group traversal reads.  kSecond (the
+// quadrupole walk and the learned features) also accumulates second moments
+// about the COM by the parallel-axis rule, S = sum_c [S_c + m_c d_c d_c^T]
+// with d_c = com_c - com, in FP64.  Leaves have S = 0 (a multi-body leaf
+// spans less than width / 2^30, so its own S is negligible).
+// Children are read with L2-coherent loads: other threads of this launch
+// wrote them, published by the arrival counter's release/acquire.
+template <bool kSplit, bool kSecond, bool kFeat>
 __device__ __forceinline__ void cell_moments(int id, const DeviceScalars* __restrict__ s,
                                              const double2* __restrict__ pos,
                                              const double* __restrict__ mass, const Tree& t,
@@ -338,7 +339,13 @@ __device__ __forceinline__ void cell_moments(int id, const DeviceScalars* __rest
     const double2 com = make_double2(Rx / M, Ry / M);
     __stcg(t.mass + id, M);
     __stcg(t.com + id, com);
-    if (kSplit) {
+    if (kSplit && !kSecond) {
+        const int first = t.range[id].x;
+        const double2 fc = frame_center(s, bt, first);
+        t.cell4[id] = make_float4((float)(com.x - fc.x), (float)(com.y - fc.y), (float)M,
+                                  (float)cell_width2(s, bt, first, t.level[id]));
+    }
+    if (kSplit && kSecond) {
         double sxx = 0.0, sxy = 0.0, syy = 0.0;
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
@@ -411,9 +418,20 @@ __device__ __forceinline__ void cell_moments(int id, const DeviceScalars* __rest
     }
 }
 
+// Arrival at a parent: release publishes this cell's moments, acquire makes
+// the siblings' moments visible to the thread that goes on to the parent.
+__device__ __forceinline__ int arrive_acq_rel(int* counter) {
+    int old;
+    asm volatile("atom.acq_rel.gpu.global.add.s32 %0, [%1], 1;"
+                 : "=r"(old)
+                 : "l"(counter)
+                 : "memory");
+    return old;
+}
+
 // Bottom-up pass: threads start at cells without internal children and
 // climb; the last child to arrive at a parent (atomic counter) computes it.
-template <bool kSplit, bool kFeat>
+template <bool kSplit, bool kSecond, bool kFeat>
 __global__ void tree_moments(DeviceScalars* __restrict__ s, const double2* __restrict__ pos,
                              const double* __restrict__ mass, Tree t, Batch bt) {
     int id = blockIdx.x * blockDim.x + threadIdx.x;
@@ -426,17 +444,15 @@ __global__ void tree_moments(DeviceScalars* __restrict__ s, const double2* __res
             atomicOr(&s->error, kErrTree);
             return;
         }
-        cell_moments<kSplit, kFeat>(id, s, pos, mass, t, bt);
-        __threadfence();
+        cell_moments<kSplit, kSecond, kFeat>(id, s, pos, mass, t, bt);
         const int par = t.parent[id];
         if (par < 0) return;
         if (par >= cells) {
             atomicOr(&s->error, kErrTree);
             return;
         }
-        const int arrived = atomicAdd(t.ready + par, 1);
+        const int arrived = arrive_acq_rel(t.ready + par);
         if (arrived != t.nint[par] - 1) return;
-        __threadfence();
         id = par;
     }
 }
@@ -583,17 +599,22 @@ void launch_moments(nb_ctx* c, const BodyBuffers& b, bool split) {
     // Cells never exceed n - 1; threads beyond the live count exit at once.
     const int cap = (int)(c->n > 1 ? c->n - 1 : 1);
     const bool feat = split && c->tree.cellf != nullptr;
+    const bool second = split && (c->p.flags & NB_FLAG_QUADRUPOLE);
     c->launches += 1;
     const unsigned blocks = blocks_for(cap, kThreads);
     if (feat)
-        tree_moments<true, true><<<blocks, kThreads, 0, c->stream>>>(c->scal, b.pos, b.mass, c->tree,
-                                                                     c->batch);
+        tree_moments<true, true, true><<<blocks, kThreads, 0, c->stream>>>(c->scal, b.pos, b.mass,
+                                                                           c->tree, c->batch);
+    else if (second)
+        tree_moments<true, true, false><<<blocks, kThreads, 0, c->stream>>>(c->scal, b.pos, b.mass,
+                                                                            c->tree, c->batch);
     else if (split)
-        tree_moments<true, false><<<blocks, kThreads, 0, c->stream>>>(c->scal, b.pos, b.mass,
-                                                                      c->tree, c->batch);
+        tree_moments<true, false, false><<<blocks, kThreads, 0, c->stream>>>(c->scal, b.pos, b.mass,
+                                                                             c->tree, c->batch);
     else
-        tree_moments<false, false><<<blocks, kThreads, 0, c->stream>>>(c->scal, b.pos, b.mass,
-                                                                       c->tree, c->batch);
+        tree_moments<false, false, false><<<blocks, kThreads, 0, c->stream>>>(c->scal, b.pos,
+                                                                              b.mass, c->tree,
+                                                                              c->batch);
 }
 
 }  // namespace nb
