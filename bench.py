@@ -590,12 +590,18 @@ def run_variants(args, nb, m, p, v, device, plain_value, plain_accuracy) -> dict
     from nbody_b200 import accuracy as acc_mod
 
     weights = PKG / "weights" / "correction_theta1.npy"
+    record = weights.with_suffix(".json")
     out = {}
     specs = [("mono_theta1.0", dict(theta=1.0)),
+             ("mono_theta1.0_bmax0.75", dict(theta=1.0, bmax_ratio=0.75)),
              ("quad_theta0.7", dict(theta=0.7, quadrupole=True)),
-             ("quad_theta1.0", dict(theta=1.0, quadrupole=True))]
+             ("quad_theta0.8_bmax0.75", dict(theta=0.8, quadrupole=True, bmax_ratio=0.75)),
+             ("quad_theta1.0", dict(theta=1.0, quadrupole=True)),
+             ("quad_theta1.0_bmax0.75", dict(theta=1.0, quadrupole=True, bmax_ratio=0.75))]
     if weights.exists():
-        specs.insert(0, ("learned_theta1.0", dict(theta=1.0, learned=True)))
+        # the walk the network was trained on (the b_max ratio of its record)
+        bmax = json.loads(record.read_text()).get("bmax_ratio", 0.0) if record.exists() else 0.0
+        specs.insert(0, ("learned_theta1.0", dict(theta=1.0, learned=True, bmax_ratio=bmax)))
     for name, kw in specs:
         cfg = nb.SimConfig(timestep=1e-4, epsilon_squared=1e-4, G=1.0, mode=nb.NB_MODE_SPLIT,
                            device=device, **kw)

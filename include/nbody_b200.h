@@ -73,6 +73,9 @@ typedef struct nb_params {
                                body by body instead of opened (0 = default)         */
     int32_t device;         /* CUDA device ordinal                                  */
     int32_t flags;          /* NB_FLAG_* bits; others must be 0                     */
+    double bmax_ratio;      /* SPLIT: a cell is accepted only if also b_max < bmax_ratio * d,
+                               b_max = distance from its COM to its farthest corner
+                               (Barnes' b_max test); 0 = off.  FP64 mode ignores it */
 } nb_params;
 
 typedef struct nb_stats {

@@ -49,6 +49,7 @@ class NbParams(C.Structure):
         ("leaf_size", C.c_int32),
         ("device", C.c_int32),
         ("flags", C.c_int32),
+        ("bmax_ratio", C.c_double),
     ]
 
 

@@ -300,11 +300,62 @@ __global__ void tree_trivial_root(const double2* __restrict__ pos, const double*
 // spans less than width / 2^30, so its own S is negligible).
 // Children are read with L2-coherent loads: other threads of this launch
 // wrote them, published by the arrival counter's release/acquire.
+// b_max^2 of a cell: squared distance from its COM to the farthest corner of
+// its square.  The square is the cell's Morton prefix decoded in the box the
+// codes were made in (the single box, or the cell's universe); forest cells
+// above the universe roots are never accepted and get 0.
+__device__ __forceinline__ double cell_bmax2(const DeviceScalars* s, const Batch& bt,
+                                             const double2* __restrict__ pos, int first, int level,
+                                             double2 com) {
+    double2 lo;
+    double w, scale;
+    int bits, lvl = level;
+    if (bt.nuni == 0) {
+        lo = make_double2(s->box[0], s->box[2]);
+        w = s->box[1] - s->box[0];
+        scale = 4294967296.0;
+        bits = 32;
+    } else {
+        if (level < kBatchUidDigits) return 0.0;
+        const int u = bt.uid[first];
+        lo = bt.lo[u];
+        w = sqrt(bt.w2[u]);
+        scale = (double)(1u << kBatchMortonBits);
+        bits = kBatchMortonBits;
+        lvl = level - kBatchUidDigits;
+    }
+    if (!(w > 0.0)) return 0.0;
+    // the cell's column and row: the first body's grid coordinate, as the
+    // Morton kernels compute it, cut to the cell's level
+    const double inv_w = 1.0 / w, top = scale - 1.0;
+    const double2 p = pos[first];
+    const unsigned ix = __double2uint_rd(fmin(fmax((p.x - lo.x) * inv_w * scale, 0.0), top));
+    const unsigned iy = __double2uint_rd(fmin(fmax((p.y - lo.y) * inv_w * scale, 0.0), top));
+    const double wc = ldexp(w, -lvl);
+    const double kx = lvl == 0 ? 0.0 : (double)(ix >> (bits - lvl));
+    const double ky = lvl == 0 ? 0.0 : (double)(iy >> (bits - lvl));
+    const double ax = fma(kx, wc, lo.x), ay = fma(ky, wc, lo.y);
+    const double dx = fmax(fabs(ax - com.x), fabs(ax + wc - com.x));
+    const double dy = fmax(fabs(ay - com.y), fabs(ay + wc - com.y));
+    return dx * dx + dy * dy;
+}
+
+// The acceptance size the walk compares with theta^2 d^2: w^2, or with the
+// b_max test max(w^2, b_max^2 theta^2 / ratio^2) (accept_scale =
+// theta^2 / ratio^2), so that one comparison applies both tests.
+__device__ __forceinline__ float accept_size2(const DeviceScalars* s, const Batch& bt,
+                                              const double2* __restrict__ pos, int first,
+                                              int level, double2 com, float accept_scale) {
+    const double w2 = cell_width2(s, bt, first, level);
+    if (accept_scale <= 0.f) return (float)w2;
+    return (float)fmax(w2, cell_bmax2(s, bt, pos, first, level, com) * (double)accept_scale);
+}
+
 template <bool kSplit, bool kSecond, bool kFeat>
 __device__ __forceinline__ void cell_moments(int id, const DeviceScalars* __restrict__ s,
                                              const double2* __restrict__ pos,
                                              const double* __restrict__ mass, const Tree& t,
-                                             const Batch& bt) {
+                                             const Batch& bt, float accept_scale) {
     const int4 ch = t.child[id];
     const int refs[4] = {ch.x, ch.y, ch.z, ch.w};
     double cm[4], cmx[4], cmy[4];
@@ -343,7 +394,7 @@ __device__ __forceinline__ void cell_moments(int id, const DeviceScalars* __rest
         const int first = t.range[id].x;
         const double2 fc = frame_center(s, bt, first);
         t.cell4[id] = make_float4((float)(com.x - fc.x), (float)(com.y - fc.y), (float)M,
-                                  (float)cell_width2(s, bt, first, t.level[id]));
+                                  accept_size2(s, bt, pos, first, t.level[id], com, accept_scale));
     }
     if (kSplit && kSecond) {
         double sxx = 0.0, sxy = 0.0, syy = 0.0;
@@ -413,7 +464,7 @@ __device__ __forceinline__ void cell_moments(int id, const DeviceScalars* __rest
         const int first = t.range[id].x;
         const double2 fc = frame_center(s, bt, first);
         t.cell4[id] = make_float4((float)(com.x - fc.x), (float)(com.y - fc.y), (float)M,
-                                  (float)cell_width2(s, bt, first, t.level[id]));
+                                  accept_size2(s, bt, pos, first, t.level[id], com, accept_scale));
         t.cellq[id] = make_float4((float)sxx, (float)sxy, (float)syy, 0.f);
     }
 }
@@ -433,7 +484,8 @@ __device__ __forceinline__ int arrive_acq_rel(int* counter) {
 // climb; the last child to arrive at a parent (atomic counter) computes it.
 template <bool kSplit, bool kSecond, bool kFeat>
 __global__ void tree_moments(DeviceScalars* __restrict__ s, const double2* __restrict__ pos,
-                             const double* __restrict__ mass, Tree t, Batch bt) {
+                             const double* __restrict__ mass, Tree t, Batch bt,
+                             float accept_scale) {
     int id = blockIdx.x * blockDim.x + threadIdx.x;
     const int cells = s->cells;
     if (id >= cells || t.nint[id] != 0) return;
@@ -444,7 +496,7 @@ __global__ void tree_moments(DeviceScalars* __restrict__ s, const double2* __res
             atomicOr(&s->error, kErrTree);
             return;
         }
-        cell_moments<kSplit, kSecond, kFeat>(id, s, pos, mass, t, bt);
+        cell_moments<kSplit, kSecond, kFeat>(id, s, pos, mass, t, bt, accept_scale);
         const int par = t.parent[id];
         if (par < 0) return;
         if (par >= cells) {
@@ -600,21 +652,23 @@ void launch_moments(nb_ctx* c, const BodyBuffers& b, bool split) {
     const int cap = (int)(c->n > 1 ? c->n - 1 : 1);
     const bool feat = split && c->tree.cellf != nullptr;
     const bool second = split && (c->p.flags & NB_FLAG_QUADRUPOLE);
+    const double ratio = c->p.bmax_ratio;
+    const float accept_scale =
+        split && ratio > 0.0 ? (float)(c->p.theta * c->p.theta / (ratio * ratio)) : 0.f;
     c->launches += 1;
     const unsigned blocks = blocks_for(cap, kThreads);
     if (feat)
-        tree_moments<true, true, true><<<blocks, kThreads, 0, c->stream>>>(c->scal, b.pos, b.mass,
-                                                                           c->tree, c->batch);
+        tree_moments<true, true, true><<<blocks, kThreads, 0, c->stream>>>(
+            c->scal, b.pos, b.mass, c->tree, c->batch, accept_scale);
     else if (second)
-        tree_moments<true, true, false><<<blocks, kThreads, 0, c->stream>>>(c->scal, b.pos, b.mass,
-                                                                            c->tree, c->batch);
+        tree_moments<true, true, false><<<blocks, kThreads, 0, c->stream>>>(
+            c->scal, b.pos, b.mass, c->tree, c->batch, accept_scale);
     else if (split)
-        tree_moments<true, false, false><<<blocks, kThreads, 0, c->stream>>>(c->scal, b.pos, b.mass,
-                                                                             c->tree, c->batch);
+        tree_moments<true, false, false><<<blocks, kThreads, 0, c->stream>>>(
+            c->scal, b.pos, b.mass, c->tree, c->batch, accept_scale);
     else
-        tree_moments<false, false, false><<<blocks, kThreads, 0, c->stream>>>(c->scal, b.pos,
-                                                                              b.mass, c->tree,
-                                                                              c->batch);
+        tree_moments<false, false, false><<<blocks, kThreads, 0, c->stream>>>(
+            c->scal, b.pos, b.mass, c->tree, c->batch, 0.f);
 }
 
 }  // namespace nb

@@ -46,9 +46,9 @@ bool finite_array(const double* a, size_t count) {
 int check_params(const nb_params* p) {
     if (!p) return NB_ERR_INVALID;
     if (!std::isfinite(p->G) || !std::isfinite(p->timestep) || !std::isfinite(p->theta) ||
-        !std::isfinite(p->epsilon_squared))
+        !std::isfinite(p->epsilon_squared) || !std::isfinite(p->bmax_ratio))
         return NB_ERR_INVALID;
-    if (p->theta < 0.0 || p->epsilon_squared < 0.0) return NB_ERR_INVALID;
+    if (p->theta < 0.0 || p->epsilon_squared < 0.0 || p->bmax_ratio < 0.0) return NB_ERR_INVALID;
     if (p->mode != NB_MODE_FP64 && p->mode != NB_MODE_SPLIT) return NB_ERR_INVALID;
     if (p->leaf_size < 0 || (p->flags & ~(int32_t)(NB_FLAG_QUADRUPOLE | NB_FLAG_LEARNED)) != 0)
         return NB_ERR_INVALID;

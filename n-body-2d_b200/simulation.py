@@ -68,6 +68,7 @@ class SimConfig:
     device: int = 0
     quadrupole: bool = False
     learned: bool = False
+    bmax_ratio: float = 0.0
 
     def params(self) -> NbParams:
         p = NbParams()
@@ -79,6 +80,7 @@ class SimConfig:
         p.mode = self.mode
         p.leaf_size = self.leaf_size
         p.device = self.device
+        p.bmax_ratio = self.bmax_ratio
         p.flags = ((_lib.NB_FLAG_QUADRUPOLE if self.quadrupole else 0)
                    | (_lib.NB_FLAG_LEARNED if self.learned else 0))
         return p

@@ -7,8 +7,12 @@ network is trained by the library's own BF16 tensor-core kernels
 (nb_mlp_train).  The weights land in weights/correction_theta<theta>.npy with a
 JSON record of the run beside them.
 
-    python n-body-2d_b200/train_correction.py [--theta 1.0] [--samples 16777216]
-        [--collision-n 4194304] [--epochs 6] [--out DIR]
+    python n-body-2d_b200/train_correction.py [--theta 1.0] [--bmax 0.75]
+        [--samples 16777216] [--collision-n 4194304] [--epochs 6] [--out DIR]
+
+--bmax is the b_max acceptance ratio of the walk the network corrects
+(nb_params.bmax_ratio); inference must use the same value, which the JSON
+record carries.
 """
 from __future__ import annotations
 
@@ -35,7 +39,7 @@ def _package():
     return mod
 
 
-def collect(nb, theta, total, collision_n, eps2=1e-4, seeds=range(1, 9)):
+def collect(nb, theta, bmax, total, collision_n, eps2=1e-4, seeds=range(1, 9)):
     """About total/16 samples from each of the 16 snapshots."""
     per = total // (2 * len(seeds))
     Xs, Ys, info = [], [], []
@@ -43,7 +47,7 @@ def collect(nb, theta, total, collision_n, eps2=1e-4, seeds=range(1, 9)):
         for kind, n in (("disc", 16384), ("collision", collision_n)):
             m, p, v = nb.universes.make(kind, n, seed)
             cfg = nb.SimConfig(theta=theta, epsilon_squared=eps2, mode=nb.NB_MODE_SPLIT,
-                               learned=True)
+                               learned=True, bmax_ratio=bmax)
             with nb.NbContext(cfg, m, p, v) as ctx:
                 # a few hundred band cells per target group
                 X, Y = ctx.mlp_samples(max(64, per // 150), seed=seed, capacity=per)
@@ -56,6 +60,7 @@ def collect(nb, theta, total, collision_n, eps2=1e-4, seeds=range(1, 9)):
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--theta", type=float, default=1.0)
+    ap.add_argument("--bmax", type=float, default=0.75)
     ap.add_argument("--samples", type=int, default=1 << 24)
     ap.add_argument("--collision-n", type=int, default=4194304)
     ap.add_argument("--epochs", type=int, default=6)
@@ -65,7 +70,7 @@ def main(argv=None):
     args = ap.parse_args(argv)
     nb = _package()
     t0 = time.time()
-    X, Y, info = collect(nb, args.theta, args.samples, args.collision_n)
+    X, Y, info = collect(nb, args.theta, args.bmax, args.samples, args.collision_n)
     t_samples = time.time() - t0
     t0 = time.time()
     params, losses = nb.mlp_train(X, Y, epochs=args.epochs, batch=args.batch, lr=args.lr, seed=0)
@@ -76,7 +81,8 @@ def main(argv=None):
     out.mkdir(parents=True, exist_ok=True)
     stem = f"correction_theta{args.theta:g}"
     np.save(out / f"{stem}.npy", params.astype(np.float32))
-    rec = {"theta": args.theta, "samples": int(X.shape[0]), "snapshots": info,
+    rec = {"theta": args.theta, "bmax_ratio": args.bmax, "samples": int(X.shape[0]),
+           "snapshots": info,
            "epochs": args.epochs, "batch": args.batch, "lr": args.lr,
            "loss_per_epoch": [float(x) for x in losses], "relative_rms_fit": fit,
            "seconds_sampling": round(t_samples, 2), "seconds_training": round(t_train, 2)}

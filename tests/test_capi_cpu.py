@@ -72,3 +72,15 @@ def test_batch_create_rejects_bad_batches_before_any_device_call(nbp):
     p.flags = nbp.NB_FLAG_LEARNED
     assert lib.nb_batch_create(C.byref(p), 2, counts, one, one, one, C.byref(h)) == 1
     assert lib.nb_autotune(None, 1, None, None) == 1
+
+
+def test_bmax_ratio_validated(nbp):
+    lib = nbp.load()
+    h = C.c_void_p()
+    p = nbp.NbParams()
+    lib.nb_params_default(C.byref(p))
+    assert p.bmax_ratio == 0.0
+    one = (C.c_double * 2)(0.0, 0.0)
+    for bad in (-0.5, float("nan"), float("inf")):
+        p.bmax_ratio = bad
+        assert lib.nb_create(C.byref(p), 1, one, one, one, C.byref(h)) == 1

@@ -108,3 +108,23 @@ def test_split_zero_softening_coincident_bodies_add_nothing(nbp):
     w = np.where(r2 > 0, m[None, :] / np.where(r2 > 0, r2, 1.0) ** 1.5, 0.0)
     exact = (w[:, :, None] * d).sum(1)
     assert np.percentile(rel_err(a, exact), 99) < 1e-3
+
+
+@pytest.mark.parametrize("quad", [False, True])
+def test_bmax_guard_tightens_the_walk(nbp, quad):
+    """Barnes' b_max test on top of the width test: a cell whose centre of
+    mass sits near a corner is opened unless d > b_max / ratio.  At theta = 1
+    that removes the slowly converging cells that set the p99 error."""
+    m, p, v = nbp.universes.colliding_discs(65536, 4)
+    tgt = np.arange(0, 65536, 5)
+    exact = nbp.allpairs_accelerations(m, p, tgt, EPS2)
+    out = {}
+    for ratio in (0.0, 0.75):
+        cfg = nbp.SimConfig(theta=1.0, epsilon_squared=EPS2, mode=nbp.NB_MODE_SPLIT,
+                            quadrupole=quad, bmax_ratio=ratio)
+        with nbp.NbContext(cfg, m, p, v) as ctx:
+            a = ctx.accelerations()
+            st = ctx.stats()
+        out[ratio] = (np.percentile(rel_err(a[tgt], exact), 99), st.cell_interactions)
+    assert out[0.75][1] >= out[0.0][1]  # only ever opens more cells
+    assert out[0.75][0] < 0.7 * out[0.0][0]
