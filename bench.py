@@ -312,6 +312,7 @@ def run_reference_ensemble(args, refcpu, cores: int, world: int) -> None:
 def _config(args) -> dict:
     return {"workload": args.workload, "n": args.n, "theta": args.theta, "mode": args.mode,
             "quadrupole": bool(getattr(args, "quad", False)), "leaf_size": getattr(args, "leaf", 0),
+            "learned": bool(getattr(args, "learned", False)), "bmax_ratio": getattr(args, "bmax", 0.0),
             "softening": 0.01, "dt": 1e-4, "G": 1.0, "state": "f64",
             "l2": "inputs larger than L2 (state + tree > 126 MB at this N)"}
 
@@ -330,9 +331,15 @@ def run_ours(args) -> None:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     m, p, v = _workload(args.kind, args.n, seed=rank)
     mode = nb.NB_MODE_SPLIT if args.mode == "split" else nb.NB_MODE_FP64
+    weights = None
+    if args.learned:
+        weights, args.bmax = _learned_weights()
     cfg = nb.SimConfig(timestep=1e-4, theta=args.theta, epsilon_squared=1e-4, G=1.0, mode=mode,
-                       device=local, quadrupole=args.quad, leaf_size=args.leaf)
+                       device=local, quadrupole=args.quad, leaf_size=args.leaf,
+                       learned=args.learned, bmax_ratio=args.bmax)
     ctx = nb.NbContext(cfg, m, p, v)
+    if weights is not None:
+        ctx.set_mlp_weights(weights)
     ctx.step(args.warmup)
 
     def barrier():
@@ -581,6 +588,14 @@ def run_ensemble(args) -> None:
         print(json.dumps(line), flush=True)
 
 
+def _learned_weights():
+    """The trained correction and the b_max ratio of the walk it was trained on."""
+    weights = PKG / "weights" / "correction_theta1.npy"
+    record = weights.with_suffix(".json")
+    bmax = json.loads(record.read_text()).get("bmax_ratio", 0.0) if record.exists() else 0.0
+    return np.load(weights), bmax
+
+
 def run_variants(args, nb, m, p, v, device, plain_value, plain_accuracy) -> dict:
     """The learned theta = 1.0 step next to the plain theta = 0.5 one (same
     workload, same timing method), plus the analytic-quadrupole and plain
@@ -654,10 +669,17 @@ def main(argv=None):
     ap.add_argument("--variants", action="store_true",
                     help="also time the learned, quadrupole and plain theta=1.0 walks")
     ap.add_argument("--universes", type=int, default=512, help="ensemble512: universe count")
+    ap.add_argument("--bmax", type=float, default=0.0,
+                    help="SPLIT: b_max acceptance ratio (nb_params.bmax_ratio; 0 = off)")
+    ap.add_argument("--learned", action="store_true",
+                    help="SPLIT with the learned far-field correction (weights/correction_theta1; "
+                         "its b_max ratio)")
     args = ap.parse_args(argv)
     kind, n, theta = WORKLOADS[args.workload]
     args.kind = kind
     args.n = args.n or n
+    if args.learned and args.theta is None:
+        theta = 1.0  # the learned correction's walk
     args.theta = theta if args.theta is None else args.theta
     if args.warmup < 3:
         args.warmup = 3

@@ -457,24 +457,29 @@ int mlp_smem_bytes() { return (int)sizeof(TrainSmem); }
 namespace {
 
 // ---- features shared by sampling and inference -------------------------
-// (p - c), d and the cell record -> the 12 features (see the file header).
-__device__ __forceinline__ void mlp_features(float ux, float uy, float d, float eps2,
-                                             const float4 f0, const float4 f1, const float4 f2,
-                                             float* x) {
-    const float inv = 1.f / d;
-    x[0] = ux * inv;
-    x[1] = uy * inv;
-    x[2] = f2.y * inv;  // w / d
-    x[3] = f0.x;        // heaviest child's mass fraction
-    x[4] = f0.y;        // S / (M w^2)
-    x[5] = f0.z;
-    x[6] = f0.w;
-    x[7] = f1.x;        // T / (M w^3)
-    x[8] = f1.y;
-    x[9] = f1.z;
-    x[10] = f1.w;
-    x[11] = eps2 / (d * d + eps2);
+// The (point, cell) features: u = (p - c) / d (2), w / d and
+// eps^2 / (d^2 + eps^2), plus the output scale M / d^2; the cell's eight
+// moment features come from cellh.  Sampling and inference both call this,
+// so training data and inference agree bit for bit.
+struct PointFeatures {
+    float x0, x1, x2, x11, scale;
+};
+
+__device__ __forceinline__ PointFeatures point_features(float ux, float uy, float w, float mass,
+                                                        float eps2) {
+    const float d2 = fmaxf(fmaf(ux, ux, uy * uy), 1e-30f);
+    const float inv = rsqrtf(d2);
+    PointFeatures f;
+    f.x0 = ux * inv;
+    f.x1 = uy * inv;
+    f.x2 = w * inv;
+    f.x11 = eps2 / (d2 + eps2);
+    f.scale = mass * (inv * inv);
+    return f;
 }
+
+__device__ __forceinline__ float bf16_lo(uint32_t w) { return __uint_as_float(w << 16); }
+__device__ __forceinline__ float bf16_hi(uint32_t w) { return __uint_as_float(w & 0xffff0000u); }
 
 // ---- residual samples (training data) ----------------------------------
 // Samples are drawn exactly as inference uses the network: one warp per target
@@ -587,9 +592,12 @@ mlp_samples_kernel(Tree t, const DeviceScalars* __restrict__ s, const double2* _
                 const double scale = (double)dc2 / (M * nb);
                 const unsigned slot = atomicAdd(count, 1u);
                 if (slot < cap) {
-                    float x[kNin];
-                    mlp_features(ux, uy, sqrtf(dc2), (float)eps2, t.cellf[3 * ref],
-                                 t.cellf[3 * ref + 1], t.cellf[3 * ref + 2], x);
+                    const PointFeatures pf = point_features(ux, uy, t.cellw[ref], c4.z,
+                                                            (float)eps2);
+                    const uint4 h = t.cellh[ref];
+                    const float x[kNin] = {pf.x0,       pf.x1,       pf.x2,       bf16_lo(h.x),
+                                           bf16_hi(h.x), bf16_lo(h.y), bf16_hi(h.y), bf16_lo(h.z),
+                                           bf16_hi(h.z), bf16_lo(h.w), bf16_hi(h.w), pf.x11};
 #pragma unroll
                     for (int k = 0; k < kNin; ++k) X[(int64_t)slot * kNin + k] = x[k];
                     Y[2 * (int64_t)slot] = (float)(rx * scale);
@@ -606,26 +614,160 @@ mlp_samples_kernel(Tree t, const DeviceScalars* __restrict__ s, const double2* _
 // accepted cell and the direct sums); band[] lists, per group, the cells
 // accepted at theta but not at theta_B (capacity kBandPerBody per body of the
 // group, starting at kBandPerBody * first body).
-struct CorrSmem {
-    MlpWeights W;
-    __nv_bfloat16 x[kWarps][16][16];
-    float scale[kWarps][16][2];  // per tile row: M / d^2 and the row's validity
+//
+// The weights sit in shared memory as per-lane B fragments, prepared once per
+// nb_set_mlp_weights (mlp_prepare_infer), so each fragment (or pair of
+// k-tiles) is one 64/128-bit shared load.  The input tile's columns are the
+// features in the order 3..10 (the cell's BF16 record, copied as is), 0, 1,
+// 2, 11, then zeros; the layer-1 image permutes W1's columns to match.  The
+// hidden activations are tanh on packed BF16 pairs (one SFU op per two
+// values), which is also the rounding the next layer's A fragment needs.
+struct InferW {
+    uint2 w1[8][32];      // layer 1, n-tile nt: {b0, b1}
+    uint4 w2[8][2][32];   // layer 2, n-tile nt, k-tiles 2j and 2j + 1: {b0, b1, b0', b1'}
+    uint4 w3[2][32];      // layer 3 (outputs padded to 8), k-tiles 2j and 2j + 1
+    float2 b1[8][4];      // bias of columns 8 nt + 2q and 8 nt + 2q + 1
+    float2 b2[8][4];
+    float2 b3[4];
+    float yscale;
 };
 
-__global__ void __launch_bounds__(kWarps * 32)
-mlp_correct_kick(const float* __restrict__ params, Tree t, const DeviceScalars* __restrict__ s,
+constexpr int kCorrWarps = 4;
+
+struct CorrSmem {
+    InferW W;
+    uint4 x[kCorrWarps][2][16][2];  // per warp: two 16-row input tiles, 32 bytes a row
+    float scale[kCorrWarps][2][16];  // per row: M / d^2 (0 for padding rows)
+};
+
+// Input column of the inference tile -> feature index (-1: zero padding).
+__device__ __forceinline__ int infer_feature(int col) {
+    return col < 8 ? col + 3 : col < 11 ? col - 8 : col == 11 ? 11 : -1;
+}
+
+__global__ void mlp_prepare_infer(const float* __restrict__ p, InferW* __restrict__ W) {
+    const int lane = threadIdx.x & 31, nt = threadIdx.x >> 5, g = lane >> 2, q = lane & 3;
+    const int n = 8 * nt + g;
+    auto w1 = [&](int col) {
+        const int f = infer_feature(col);
+        return f < 0 ? 0.f : p[kW1 + n * kNin + f];
+    };
+    W->w1[nt][lane] = make_uint2(pack_bf16(w1(2 * q), w1(2 * q + 1)),
+                                 pack_bf16(w1(2 * q + 8), w1(2 * q + 9)));
+    auto w2 = [&](int k) { return p[kW2 + n * kH + k]; };
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+        const int k0 = 32 * j + 2 * q, k1 = k0 + 16;
+        W->w2[nt][j][lane] = make_uint4(pack_bf16(w2(k0), w2(k0 + 1)), pack_bf16(w2(k0 + 8), w2(k0 + 9)),
+                                        pack_bf16(w2(k1), w2(k1 + 1)), pack_bf16(w2(k1 + 8), w2(k1 + 9)));
+    }
+    if (nt == 0) {
+        auto w3 = [&](int k) { return g < 2 ? p[kW3 + g * kH + k] : 0.f; };
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            const int k0 = 32 * j + 2 * q, k1 = k0 + 16;
+            W->w3[j][lane] = make_uint4(pack_bf16(w3(k0), w3(k0 + 1)), pack_bf16(w3(k0 + 8), w3(k0 + 9)),
+                                        pack_bf16(w3(k1), w3(k1 + 1)), pack_bf16(w3(k1 + 8), w3(k1 + 9)));
+        }
+        if (lane < 4)
+            W->b3[lane] = lane == 0 ? make_float2(p[kB3], p[kB3 + 1]) : make_float2(0.f, 0.f);
+        if (lane == 0) W->yscale = p[kYS];
+    }
+    if (lane < 4) {
+        W->b1[nt][lane] = make_float2(p[kB1 + 8 * nt + 2 * lane], p[kB1 + 8 * nt + 2 * lane + 1]);
+        W->b2[nt][lane] = make_float2(p[kB2 + 8 * nt + 2 * lane], p[kB2 + 8 * nt + 2 * lane + 1]);
+    }
+}
+
+__device__ __forceinline__ uint32_t tanh_bf16x2(uint32_t x) {
+    uint32_t y;
+    asm("tanh.approx.bf16x2 %0, %1;" : "=r"(y) : "r"(x));
+    return y;
+}
+
+// kT independent 16-row tiles through the network (their mma chains
+// interleave); y[t] = output fragment of tile t (columns 2q, 2q+1 of rows g,
+// g + 8; only q = 0 holds the two outputs).
+template <int kT>
+__device__ __forceinline__ void infer_tiles(const InferW& W, const uint32_t (*a)[4], float (*y)[4]) {
+    const int lane = threadIdx.x & 31, q = lane & 3;
+    uint32_t h1[kT][4][4], h2[kT][4][4];
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt) {
+        const float2 b = W.b1[nt][q];
+        const uint2 f = W.w1[nt][lane];
+#pragma unroll
+        for (int t = 0; t < kT; ++t) {
+            float c[4] = {b.x, b.y, b.x, b.y};
+            mma16816(c, a[t], f.x, f.y);
+            h1[t][nt >> 1][(nt & 1) * 2] = tanh_bf16x2(pack_bf16(c[0], c[1]));
+            h1[t][nt >> 1][(nt & 1) * 2 + 1] = tanh_bf16x2(pack_bf16(c[2], c[3]));
+        }
+    }
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt) {
+        const float2 b = W.b2[nt][q];
+        float c[kT][4];
+#pragma unroll
+        for (int t = 0; t < kT; ++t) {
+            c[t][0] = b.x;
+            c[t][1] = b.y;
+            c[t][2] = b.x;
+            c[t][3] = b.y;
+        }
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            const uint4 f = W.w2[nt][j][lane];
+#pragma unroll
+            for (int t = 0; t < kT; ++t) {
+                mma16816(c[t], h1[t][2 * j], f.x, f.y);
+                mma16816(c[t], h1[t][2 * j + 1], f.z, f.w);
+            }
+        }
+#pragma unroll
+        for (int t = 0; t < kT; ++t) {
+            h2[t][nt >> 1][(nt & 1) * 2] = tanh_bf16x2(pack_bf16(c[t][0], c[t][1]));
+            h2[t][nt >> 1][(nt & 1) * 2 + 1] = tanh_bf16x2(pack_bf16(c[t][2], c[t][3]));
+        }
+    }
+    const float2 b = W.b3[q];
+#pragma unroll
+    for (int t = 0; t < kT; ++t) {
+        y[t][0] = b.x;
+        y[t][1] = b.y;
+        y[t][2] = b.x;
+        y[t][3] = b.y;
+    }
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+        const uint4 f = W.w3[j][lane];
+#pragma unroll
+        for (int t = 0; t < kT; ++t) {
+            mma16816(y[t], h2[t][2 * j], f.x, f.y);
+            mma16816(y[t], h2[t][2 * j + 1], f.z, f.w);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kCorrWarps * 32)
+mlp_correct_kick(const InferW* __restrict__ Wg, Tree t, const DeviceScalars* __restrict__ s,
                  double2* __restrict__ pos, double2* __restrict__ vel,
                  const float2* __restrict__ acc32, double2* __restrict__ acc_out, int n,
                  float eps2, double G_dt, double dt, int kick) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     CorrSmem& S = *reinterpret_cast<CorrSmem*>(smem_raw);
-    fill_weights(params, S.W);
+    {
+        const uint4* src = reinterpret_cast<const uint4*>(Wg);
+        uint4* dst = reinterpret_cast<uint4*>(&S.W);
+        for (int k = threadIdx.x; k < (int)(sizeof(InferW) / 16); k += blockDim.x) dst[k] = src[k];
+    }
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, q = lane & 3;
+    const int row = lane & 15, half = lane >> 4;
     const double cx = s->center[0], cy = s->center[1];
     const int ngroups = s->groups;
     const float ys = S.W.yscale;
-    for (int gi = blockIdx.x * kWarps + warp; gi < ngroups; gi += gridDim.x * kWarps) {
+    for (int gi = blockIdx.x * kCorrWarps + warp; gi < ngroups; gi += gridDim.x * kCorrWarps) {
         const int2 gr = t.groups[gi];
         const int g0 = gr.x, g1 = min(gr.y, n - 1);
         double2 P[2];
@@ -654,39 +796,41 @@ mlp_correct_kick(const float* __restrict__ params, Tree t, const DeviceScalars* 
         const int nband = min(t.band_count[gi], kBandPerBody * (g1 - g0 + 1));
         const int* band = t.band + (int64_t)kBandPerBody * g0;
         float cxs = 0.f, cys = 0.f;
-        for (int base = 0; base < nband; base += 16) {
-            // lanes 0..15 build the features of one band cell each
-            if (lane < 16) {
-                const int r = base + lane;
-                float x[kNin];
-                float sc = 0.f;
-                if (r < nband) {
-                    const int ref = band[r];
-                    const float4 c4 = t.cell4[ref];
-                    const float ux = gx - c4.x, uy = gy - c4.y;
-                    const float d2 = fmaxf(ux * ux + uy * uy, 1e-30f);
-                    mlp_features(ux, uy, sqrtf(d2), eps2, t.cellf[3 * ref], t.cellf[3 * ref + 1],
-                                 t.cellf[3 * ref + 2], x);
-                    sc = c4.z / d2;
-                } else {
-#pragma unroll
-                    for (int k = 0; k < kNin; ++k) x[k] = 0.f;
-                }
-                uint32_t* row = reinterpret_cast<uint32_t*>(&S.x[warp][lane][0]);
-#pragma unroll
-                for (int k = 0; k < kNin; k += 2) row[k / 2] = pack_bf16(x[k], x[k + 1]);
-                row[6] = 0u;
-                row[7] = 0u;
-                S.scale[warp][lane][0] = sc;
+        for (int base = 0; base < nband; base += 32) {
+            // lane l builds row l % 16 of tile l / 16
+            const int r = base + lane;
+            uint4 lo = make_uint4(0u, 0u, 0u, 0u), hi = lo;
+            float sc = 0.f;
+            if (r < nband) {
+                const int ref = band[r];
+                const float4 c4 = t.cell4[ref];
+                const PointFeatures pf = point_features(gx - c4.x, gy - c4.y, t.cellw[ref], c4.z,
+                                                        eps2);
+                lo = t.cellh[ref];
+                hi = make_uint4(pack_bf16(pf.x0, pf.x1), pack_bf16(pf.x2, pf.x11), 0u, 0u);
+                sc = pf.scale;
             }
+            S.x[warp][half][row][0] = lo;
+            S.x[warp][half][row][1] = hi;
+            S.scale[warp][half][row] = sc;
             __syncwarp();
-            uint32_t a[4];
-            load_a(&S.x[warp][0][0], 16, 0, a);
-            Fwd f;
-            mlp_forward<false>(S.W, a, f);
+            uint32_t a[2][4];
+            float y[2][4];
+            load_a(reinterpret_cast<const __nv_bfloat16*>(&S.x[warp][0][0][0]), 16, 0, a[0]);
+            if (nband - base > 16) {
+                load_a(reinterpret_cast<const __nv_bfloat16*>(&S.x[warp][1][0][0]), 16, 0, a[1]);
+                infer_tiles<2>(S.W, a, y);
+            } else {
+                infer_tiles<1>(S.W, a, y);
+                y[1][0] = y[1][1] = y[1][2] = y[1][3] = 0.f;
+            }
             if (q == 0) {
-                cxs += ys * (f.y[0] * S.scale[warp][g][0] + f.y[2] * S.scale[warp][g + 8][0]);
-                cys += ys * (f.y[1] * S.scale[warp][g][0] + f.y[3] * S.scale[warp][g + 8][0]);
+#pragma unroll
+                for (int tt = 0; tt < 2; ++tt) {
+                    const float s0 = S.scale[warp][tt][g], s1 = S.scale[warp][tt][g + 8];
+                    cxs = fmaf(y[tt][0], s0, fmaf(y[tt][2], s1, cxs));
+                    cys = fmaf(y[tt][1], s0, fmaf(y[tt][3], s1, cys));
+                }
             }
             __syncwarp();
         }
@@ -694,6 +838,8 @@ mlp_correct_kick(const float* __restrict__ params, Tree t, const DeviceScalars* 
             cxs += __shfl_xor_sync(kFull, cxs, o);
             cys += __shfl_xor_sync(kFull, cys, o);
         }
+        cxs *= ys;
+        cys *= ys;
 #pragma unroll
         for (int b = 0; b < 2; ++b) {
             if (!on[b]) continue;
@@ -719,17 +865,29 @@ inline unsigned blocks_for(int64_t n, int per) { return (unsigned)((n + per - 1)
 
 }  // namespace
 
+size_t mlp_infer_bytes() { return sizeof(InferW); }
+
+void mlp_prepare_inference(nb_ctx* c) {
+    mlp_prepare_infer<<<1, 256, 0, c->stream>>>(c->mlp_params, static_cast<InferW*>(c->mlp_infer));
+}
+
 void launch_mlp_correct(nb_ctx* c, const BodyBuffers& b, bool kick, bool store_acc) {
     c->launches += 1;
     const int smem = (int)sizeof(CorrSmem);
-    static bool attr_set = false;
-    if (!attr_set) {
+    static int grid_per_sm = 0;
+    if (grid_per_sm == 0) {
         cudaFuncSetAttribute(mlp_correct_kick, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        attr_set = true;
+        int blocks = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, mlp_correct_kick,
+                                                          kCorrWarps * 32, smem) != cudaSuccess ||
+            blocks < 1)
+            blocks = 2;
+        grid_per_sm = blocks;
     }
-    mlp_correct_kick<<<c->sm_count * 8, kWarps * 32, smem, c->stream>>>(
-        c->mlp_params, c->tree, c->scal, b.pos, b.vel, c->acc32, store_acc ? c->acc : nullptr,
-        (int)c->n, (float)c->p.epsilon_squared, c->p.G * c->p.timestep, c->p.timestep, kick ? 1 : 0);
+    mlp_correct_kick<<<c->sm_count * grid_per_sm, kCorrWarps * 32, smem, c->stream>>>(
+        static_cast<const InferW*>(c->mlp_infer), c->tree, c->scal, b.pos, b.vel, c->acc32,
+        store_acc ? c->acc : nullptr, (int)c->n, (float)c->p.epsilon_squared,
+        c->p.G * c->p.timestep, c->p.timestep, kick ? 1 : 0);
 }
 
 void launch_mlp_samples(nb_ctx* c, const BodyBuffers& b, const int* pick, int npick, float* X,

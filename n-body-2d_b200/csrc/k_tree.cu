@@ -24,6 +24,7 @@
 // level, so opening decisions and force terms equal the reference's
 // (cell widths come from the level, never from the body range).
 #include <climits>
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -351,6 +352,12 @@ __device__ __forceinline__ float accept_size2(const DeviceScalars* s, const Batc
     return (float)fmax(w2, cell_bmax2(s, bt, pos, first, level, com) * (double)accept_scale);
 }
 
+// Two floats rounded to BF16 (round to nearest even), lo in the low half.
+__device__ __forceinline__ uint32_t bf16_pair(float lo, float hi) {
+    const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<const uint32_t*>(&v);
+}
+
 template <bool kSplit, bool kSecond, bool kFeat>
 __device__ __forceinline__ void cell_moments(int id, const DeviceScalars* __restrict__ s,
                                              const double2* __restrict__ pos,
@@ -452,14 +459,15 @@ __device__ __forceinline__ void cell_moments(int id, const DeviceScalars* __rest
             double2* to = reinterpret_cast<double2*>(t.t64 + id);
             __stcg(to, make_double2(txxx, txxy));
             __stcg(to + 1, make_double2(txyy, tyyy));
-            // the MLP's cell features, normalised by M and the cell width
+            // the MLP's cell features, normalised by M and the cell width; the
+            // network reads them as BF16, so they are stored rounded
             const double w2 = cell_width2(s, bt, t.range[id].x, t.level[id]), w = sqrt(w2);
             const double im2 = 1.0 / (M * w2), im3 = im2 / w;
-            t.cellf[3 * id + 0] = make_float4((float)(mmax / M), (float)(sxx * im2),
-                                              (float)(sxy * im2), (float)(syy * im2));
-            t.cellf[3 * id + 1] = make_float4((float)(txxx * im3), (float)(txxy * im3),
-                                              (float)(txyy * im3), (float)(tyyy * im3));
-            t.cellf[3 * id + 2] = make_float4(0.f, (float)w, 0.f, 0.f);
+            t.cellh[id] = make_uint4(bf16_pair((float)(mmax / M), (float)(sxx * im2)),
+                                     bf16_pair((float)(sxy * im2), (float)(syy * im2)),
+                                     bf16_pair((float)(txxx * im3), (float)(txxy * im3)),
+                                     bf16_pair((float)(txyy * im3), (float)(tyyy * im3)));
+            t.cellw[id] = (float)w;
         }
         const int first = t.range[id].x;
         const double2 fc = frame_center(s, bt, first);
@@ -650,7 +658,7 @@ void launch_tree(nb_ctx* c, const BodyBuffers& b) {
 void launch_moments(nb_ctx* c, const BodyBuffers& b, bool split) {
     // Cells never exceed n - 1; threads beyond the live count exit at once.
     const int cap = (int)(c->n > 1 ? c->n - 1 : 1);
-    const bool feat = split && c->tree.cellf != nullptr;
+    const bool feat = split && c->tree.cellh != nullptr;
     const bool second = split && (c->p.flags & NB_FLAG_QUADRUPOLE);
     const double ratio = c->p.bmax_ratio;
     const float accept_scale =

@@ -96,11 +96,13 @@ int alloc_all(nb_ctx* c) {
     }
     if (c->p.flags & NB_FLAG_LEARNED) {
         NB_CUDA(c, dalloc(&t.t64, n));
-        NB_CUDA(c, dalloc(&t.cellf, 3 * n));
+        NB_CUDA(c, dalloc(&t.cellh, n));
+        NB_CUDA(c, dalloc(&t.cellw, n));
         NB_CUDA(c, dalloc(&t.band, (size_t)nb::kBandPerBody * n));
         NB_CUDA(c, dalloc(&t.band_count, n));
         NB_CUDA(c, dalloc(&c->acc32, n));
         NB_CUDA(c, dalloc(&c->mlp_params, NB_MLP_PARAMS));
+        NB_CUDA(c, cudaMalloc(&c->mlp_infer, nb::mlp_infer_bytes()));
     }
     NB_CUDA(c, dalloc(&t.leaf_last, n));
     NB_CUDA(c, dalloc(&t.leaf_plevel, n));
@@ -141,7 +143,7 @@ void free_all(nb_ctx* c) {
                          t.leaf_plevel, t.bucket_mass, t.bucket_com, t.flag,      t.cell_of,
                          t.start_of,  t.range,       t.s64,         t.cell4,      t.cellq,
                          t.body4,     t.gcount,      t.gbase,       t.groups,     t.rep_of,
-                         t.t64,       t.cellf,       t.band,        t.band_count};
+                         t.t64,       t.cellh,       t.cellw,       t.band,       t.band_count};
     for (void* q : tree_ptrs) cudaFree(q);
     cudaFree(c->scal);
     cudaFree(c->bbox_partials);
@@ -670,6 +672,8 @@ int nb_set_mlp_weights(nb_ctx* c, const float* params) {
     DeviceGuard guard(c->device);
     NB_CUDA(c, cudaMemcpyAsync(c->mlp_params, params, sizeof(float) * NB_MLP_PARAMS,
                                cudaMemcpyHostToDevice, c->stream));
+    nb::mlp_prepare_inference(c);
+    NB_CUDA(c, cudaGetLastError());
     NB_CUDA(c, cudaStreamSynchronize(c->stream));
     c->mlp_ready = true;
     return NB_OK;

@@ -88,10 +88,12 @@ struct Tree {
     float4* cell4 = nullptr;     // {com_x - cx, com_y - cy, mass, width^2}
     float4* cellq = nullptr;     // {Sxx, Sxy, Syy, 0}
     float4* body4 = nullptr;     // per body {x - cx, y - cy, mass, index bits}
-    // learned correction: third moments (FP64, bottom-up) and the
-    // packed per-cell MLP features (3 float4 per cell, see k_mlp.cu)
+    // learned correction: third moments (FP64, bottom-up) and the per-cell
+    // MLP features (see k_mlp.cu): the eight moment features as BF16 and the
+    // cell width
     double4* t64 = nullptr;      // {Txxx, Txxy, Txyy, Tyyy}
-    float4* cellf = nullptr;
+    uint4* cellh = nullptr;      // BF16 pairs {f3 f4, f5 f6, f7 f8, f9 f10}
+    float* cellw = nullptr;
     int32_t* band = nullptr;       // per group: band cells, kBandPerBody x first body onwards
     int32_t* band_count = nullptr; // per group: band cells found
     // SPLIT target groups: <= split_group_size() Morton-consecutive bodies in one
@@ -147,6 +149,7 @@ struct nb_ctx {
     int bbox_blocks = 0;
     int split_blocks[16] = {};            // persistent grids of the SPLIT traversal variants
     float* mlp_params = nullptr;         // learned mode: FP32 MLP parameters (device)
+    void* mlp_infer = nullptr;           // learned mode: BF16 fragment images for inference
     bool mlp_ready = false;
     float2* acc32 = nullptr;             // learned mode: traversal accelerations
     nb::Batch batch;                     // batched universes (nuni > 0)
@@ -189,6 +192,8 @@ void launch_tree(nb_ctx* c, const BodyBuffers& b);
 void launch_moments(nb_ctx* c, const BodyBuffers& b, bool split);
 int split_group_size(const nb_ctx* c);   // bodies per SPLIT traversal group
 void launch_mlp_correct(nb_ctx* c, const BodyBuffers& b, bool kick, bool store_acc);
+size_t mlp_infer_bytes();
+void mlp_prepare_inference(nb_ctx* c);
 void launch_mlp_samples(nb_ctx* c, const BodyBuffers& b, const int* slots, int nslots, float* X,
                         float* Y, unsigned* count, unsigned cap);
 int mlp_forward_device(const float* params, const float* X, int64_t n, float* Y, cudaStream_t st);
