@@ -276,6 +276,18 @@ __global__ void tree_link(const uint64_t* __restrict__ key, int n,
     t.child[id] = make_int4(ref[0], ref[1], ref[2], ref[3]);
     t.nint[id] = nint;
     t.ready[id] = 0;
+    // cells whose children are all leaves start the bottom-up climb: listed
+    // with one atomic per warp
+    const unsigned active = __activemask();
+    const unsigned starts = __ballot_sync(active, nint == 0);
+    if (nint == 0) {
+        const int leader = __ffs(starts) - 1;
+        const int lane = threadIdx.x & 31;
+        int base = 0;
+        if (lane == leader) base = atomicAdd(&s->nstart, __popc(starts));
+        base = __shfl_sync(starts, base, leader);
+        t.start_list[base + __popc(starts & ((1u << lane) - 1u))] = id;
+    }
     if (first == 0 && last == n - 1) {
         s->root = id;
         t.parent[id] = -1;
@@ -494,9 +506,10 @@ template <bool kSplit, bool kSecond, bool kFeat>
 __global__ void tree_moments(DeviceScalars* __restrict__ s, const double2* __restrict__ pos,
                              const double* __restrict__ mass, Tree t, Batch bt,
                              float accept_scale) {
-    int id = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int cells = s->cells;
-    if (id >= cells || t.nint[id] != 0) return;
+    if (k >= s->nstart) return;
+    int id = t.start_list[k];
     // A path to the root crosses at most 30 cells; the bound only guards
     // against a malformed tree.
     for (int hop = 0;; ++hop) {
@@ -650,6 +663,7 @@ void launch_tree(nb_ctx* c, const BodyBuffers& b) {
     scan_block_sums<<<1, kThreads, 0, c->stream>>>(c->scan.block_sums, sblocks, &c->scal->cells);
     scan_apply<<<sblocks, kThreads, 0, c->stream>>>(c->tree.flag, n, c->scan.block_sums,
                                                      c->tree.cell_of, c->tree.rep_of);
+    cudaMemsetAsync(&c->scal->nstart, 0, sizeof(int32_t), c->stream);
     tree_link<<<blocks_for(n, kThreads), kThreads, 0, c->stream>>>(key, n, b.pos, b.mass, c->tree,
                                                                     c->scal);
     tree_trivial_root<<<1, 1, 0, c->stream>>>(b.pos, b.mass, n, c->tree, c->scal);

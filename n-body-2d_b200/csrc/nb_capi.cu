@@ -85,6 +85,7 @@ int alloc_all(nb_ctx* c) {
     NB_CUDA(c, dalloc(&t.mass, n));
     NB_CUDA(c, dalloc(&t.com, n));
     NB_CUDA(c, dalloc(&t.range, n));
+    NB_CUDA(c, dalloc(&t.start_list, n));
     if (c->p.mode == NB_MODE_SPLIT) {
         NB_CUDA(c, dalloc(&t.s64, n));
         NB_CUDA(c, dalloc(&t.cell4, n));
@@ -143,7 +144,8 @@ void free_all(nb_ctx* c) {
                          t.leaf_plevel, t.bucket_mass, t.bucket_com, t.flag,      t.cell_of,
                          t.start_of,  t.range,       t.s64,         t.cell4,      t.cellq,
                          t.body4,     t.gcount,      t.gbase,       t.groups,     t.rep_of,
-                         t.t64,       t.cellh,       t.cellw,       t.band,       t.band_count};
+                         t.t64,       t.cellh,       t.cellw,       t.band,       t.band_count,
+                         t.start_list};
     for (void* q : tree_ptrs) cudaFree(q);
     cudaFree(c->scal);
     cudaFree(c->bbox_partials);

@@ -39,6 +39,7 @@ struct DeviceScalars {
     unsigned bbox_ticket;     // last-block-done counter of the bbox reduction
     unsigned long long cell_terms;
     unsigned long long body_terms;
+    int32_t nstart;           // cells whose children are all leaves (climb starts)
 };
 
 // Batched universes (nb_batch_create): bodies of universe u occupy the fixed
@@ -96,6 +97,7 @@ struct Tree {
     float* cellw = nullptr;
     int32_t* band = nullptr;       // per group: band cells, kBandPerBody x first body onwards
     int32_t* band_count = nullptr; // per group: band cells found
+    int32_t* start_list = nullptr; // cells without internal children, in any order
     // SPLIT target groups: <= split_group_size() Morton-consecutive bodies in one
     // parent cell (merged sibling cells/leaves), stored as body ranges
     int32_t* gcount = nullptr;   // groups each cell emits
