@@ -40,8 +40,12 @@ FLOPS_PER_INTERACTION = 14  # dx,dy,d2,+eps,r^-3 (3 mul),m*,2 fma: FP64/FP32 flo
 FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
 # Algorithmic HBM bytes per body for each memory-bound phase (FP64 state,
 # u64 codes, u32 payload): bbox 16 + Morton 16 in / 12 out; 8 radix passes of
-# 12 in + 12 out; gather 44 in + 44 out; drift 32 in + 16 out.
-PHASE_BYTES_PER_BODY = {"bbox+morton": 16 + 28, "sort": 8 * 24, "gather": 88, "drift": 48}
+# 12 in + 12 out; gather 44 in + 44 out; tree build about 8 x 3 reads + 32
+# writes per cell at 1.72 cells per body (96); moments 24 per body + 24 per
+# cell (65); drift 32 in + 16 out (FP64 mode only: SPLIT fuses it into the
+# force kernel, and the learned step's last phase is the correction kernel).
+PHASE_BYTES_PER_BODY = {"bbox+morton": 16 + 28, "sort": 8 * 24, "gather": 88, "tree": 96,
+                        "moments": 65, "drift": 48}
 
 
 def _package():
@@ -399,6 +403,8 @@ def run_ours(args) -> None:
     hbm = peaks.get("hbm_gbs", FALLBACK_PEAKS["hbm_gbs"])
     rooflines = {}
     for name, bpb in PHASE_BYTES_PER_BODY.items():
+        if name == "drift" and args.mode != "fp64":
+            continue
         if phases.get(name, 0) > 0:
             gbs = bpb * args.n / (phases[name] * 1e-3) / 1e9
             rooflines[name] = {"bound": "hbm", "achieved": round(gbs, 1), "peak": hbm,
