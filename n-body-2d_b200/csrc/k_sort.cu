@@ -479,7 +479,9 @@ __device__ __forceinline__ void st_status(uint32_t* p, uint32_t v) {
     asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-__global__ void __launch_bounds__(kSortThreads)
+// Four blocks per SM (at most 64 registers): tiles of 3072 keys keep enough
+// loads in flight per block, and the occupancy hides the look-back.
+__global__ void __launch_bounds__(kSortThreads, 4)
 onesweep_pass(const uint64_t* __restrict__ key_in, const uint32_t* __restrict__ val_in,
               uint64_t* __restrict__ key_out, uint32_t* __restrict__ val_out, int64_t n, int shift,
               const uint32_t* __restrict__ bins, uint32_t* __restrict__ status,

@@ -14,9 +14,9 @@ namespace nb {
 
 constexpr int kMaxLevel = 30;     // level-30 cells are leaves (BarnesHutCuda.cu:182)
 constexpr int kStackDepth = 96;   // >= 1 + 3 * 30 pending cells of a DFS
-constexpr int kSortTileItems = 8; // keys per thread in a radix tile
+constexpr int kSortTileItems = 12; // keys per thread in a radix tile
 constexpr int kSortThreads = 256;
-constexpr int kSortTile = kSortTileItems * kSortThreads;  // 2048 keys
+constexpr int kSortTile = kSortTileItems * kSortThreads;  // 3072 keys
 constexpr int kPhases = 8;        // morton, sort, gather, tree, moments, groups, force, drift
 constexpr float kThetaBand = 0.5f; // learned mode: cells the plain 0.5 walk would open get the MLP
 constexpr int kBandPerBody = 16;   // learned mode: band-list capacity per body of a group
