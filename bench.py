@@ -334,7 +334,8 @@ def run_ours(args) -> None:
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     m, p, v = _workload(args.kind, args.n, seed=rank)
-    mode = nb.NB_MODE_SPLIT if args.mode == "split" else nb.NB_MODE_FP64
+    mode = {"split": nb.NB_MODE_SPLIT, "fp64": nb.NB_MODE_FP64,
+            "allpairs": nb.NB_MODE_ALLPAIRS}[args.mode]
     weights = None
     if args.learned:
         weights, args.bmax = _learned_weights()
@@ -397,7 +398,7 @@ def run_ours(args) -> None:
     interactions = st.cell_interactions + st.body_interactions
     force_ms = phases.get("force", ms)
     # FP64: 64 FMA lanes per SM per clock on B200 (37 TF at 1.965 GHz); FP32: 128.
-    lanes = 64 if args.mode == "fp64" else 128
+    lanes = 128 if args.mode == "split" else 64
     fp_peak = 148 * lanes * 2 * sm_mhz * 1e6 / 1e12
     achieved = FLOPS_PER_INTERACTION * interactions / (force_ms * 1e-3) / 1e12
     hbm = peaks.get("hbm_gbs", FALLBACK_PEAKS["hbm_gbs"])
@@ -405,6 +406,8 @@ def run_ours(args) -> None:
     for name, bpb in PHASE_BYTES_PER_BODY.items():
         if name == "drift" and args.mode != "fp64":
             continue
+        if args.mode == "allpairs" and name != "force":
+            continue  # the all-pairs step has no sort, tree or drift phase
         if phases.get(name, 0) > 0:
             gbs = bpb * args.n / (phases[name] * 1e-3) / 1e9
             rooflines[name] = {"bound": "hbm", "achieved": round(gbs, 1), "peak": hbm,
@@ -414,9 +417,9 @@ def run_ours(args) -> None:
         "metric": "body-steps/s", "value": value, "unit": "body-steps/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64" if args.mode == "fp64" else "f32+f64", "data": "synthetic",
+        "dtype": "f32+f64" if args.mode == "split" else "f64", "data": "synthetic",
         "config": _config(args),
-        "roofline": {"kernel": "force", "bound": "fp64" if args.mode == "fp64" else "fp32",
+        "roofline": {"kernel": "force", "bound": "fp32" if args.mode == "split" else "fp64",
                      "achieved": round(achieved, 3), "peak": round(fp_peak, 2),
                      "unit": "TFLOP/s", "frac": round(achieved / fp_peak, 4),
                      "traffic": _force_traffic(args.n) if args.mode == "split" else None,
@@ -663,7 +666,8 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--mode", choices=["fp64", "split"], default="split")
+    ap.add_argument("--mode", choices=["fp64", "split", "allpairs"], default="split",
+                    help="allpairs: the reference's AllPairsSim on the GPU (FP64, no tree)")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="collision4m")
     ap.add_argument("--n", type=int, default=None, help="override the body count")
     ap.add_argument("--theta", type=float, default=None)

@@ -53,10 +53,18 @@ extern "C" {
  * and the integrator's position/velocity accumulation. */
 #define NB_MODE_FP64 0
 #define NB_MODE_SPLIT 1
+/* NB_MODE_ALLPAIRS: the reference's AllPairsSim backend
+ * (src/Simulation/src/AllPairs.cpp:24-49): drift x += v dt, then the kick
+ * with the exact FP64 sum over all other bodies; no tree, no sort.  The pair
+ * law is Plummer's (CU:427-431), or with NB_FLAG_CPU_LAW the law of
+ * Simulation::force (src/Simulation/src/Simulation.cpp:74-80),
+ * |a| = G m / (d^2 + eps^2) along the unit vector, which AllPairsSim uses. */
+#define NB_MODE_ALLPAIRS 2
 
 /* nb_params.flags bits */
 #define NB_FLAG_QUADRUPOLE 1u  /* SPLIT: add the cells' second-moment term */
 #define NB_FLAG_LEARNED 2u     /* SPLIT: learned far-field correction (set weights first) */
+#define NB_FLAG_CPU_LAW 4u     /* ALLPAIRS: the reference CPU backends' pair law        */
 
 /* Learned correction: parameters of the 12 -> 64 -> 64 -> 2 MLP as one FP32
  * vector: W1[64][12], b1[64], W2[64][64], b2[64], W3[2][64], b3[2], then the
@@ -99,6 +107,27 @@ NB_API int nb_params_default(nb_params* p);
  * allocates every device buffer once and uploads the bodies. */
 NB_API int nb_create(const nb_params* p, uint64_t n, const double* mass, const double* pos_xy,
               const double* vel_xy, nb_ctx** out);
+
+/* Headless rendering of the current bodies into an RGBA8 image: the frame
+ * the reference draws (src/Graphics/src/Graphics.cpp:122-128) through
+ * SFML/OpenGL, without a graphics stack.  The view is the reference's
+ * ViewPort rectangle (src/Graphics/lib/ViewPort/src/ViewPort.cpp): world
+ * coordinates (x, y) of the top-left corner, world extent width x height
+ * (resolution x pixel_scale), and the window resolution.  Bodies are points
+ * of point_diameter pixels (1..50, Constants.hpp:40-41) clipped to circles as
+ * the body shader does (Graphics.cpp:20-26), white with alpha 120/255 over
+ * black (Constants.hpp:39); the exact coverage and blending rules are in
+ * csrc/k_render.cu.  rgba_out receives res_y rows of res_x pixels, row 0 at
+ * the top.  The first call at a resolution allocates the image buffers. */
+typedef struct nb_view {
+    double x, y;
+    double width, height;
+    uint32_t res_x, res_y;
+    float point_diameter;
+    uint32_t reserved;  /* must be 0 */
+} nb_view;
+
+NB_API int nb_render(nb_ctx* ctx, const nb_view* view, uint8_t* rgba_out);
 
 /* Batched universes (no counterpart in the reference, which holds one
  * universe per process): nuniverses independent universes of counts[u]

@@ -23,8 +23,10 @@ NB_ERR_NOTFOUND = 6
 
 NB_MODE_FP64 = 0
 NB_MODE_SPLIT = 1
+NB_MODE_ALLPAIRS = 2
 NB_FLAG_QUADRUPOLE = 1
 NB_FLAG_LEARNED = 2
+NB_FLAG_CPU_LAW = 4
 NB_MLP_PARAMS = 5123  # include/nbody_b200.h
 NB_STATIC_SORT_MAX_BODIES = 262144  # include/nbody_b200.h
 
@@ -35,8 +37,21 @@ EXPORTS = (
     "nb_debug_tree", "nb_get_stats", "nb_last_error", "nb_status_string",
     "nb_allpairs_accelerations", "nb_phase_times", "nb_phase_name", "nb_morton_sort_static",
     "nb_set_mlp_weights", "nb_mlp_samples", "nb_mlp_forward", "nb_mlp_loss_grad", "nb_mlp_train",
-    "nb_batch_create", "nb_autotune",
+    "nb_batch_create", "nb_autotune", "nb_render",
 )
+
+
+class NbView(C.Structure):
+    _fields_ = [
+        ("x", C.c_double),
+        ("y", C.c_double),
+        ("width", C.c_double),
+        ("height", C.c_double),
+        ("res_x", C.c_uint32),
+        ("res_y", C.c_uint32),
+        ("point_diameter", C.c_float),
+        ("reserved", C.c_uint32),
+    ]
 
 
 class NbParams(C.Structure):
@@ -116,6 +131,7 @@ def load() -> C.CDLL:
     lib.nb_batch_create.argtypes = [C.POINTER(NbParams), C.c_uint32, _P, _P, _P, _P,
                                     C.POINTER(_P)]
     lib.nb_autotune.argtypes = [_P, C.c_uint32, _P, _P]
+    lib.nb_render.argtypes = [_P, C.POINTER(NbView), _P]
     lib.nb_set_mlp_weights.argtypes = [_P, _P]
     lib.nb_mlp_samples.argtypes = [_P, C.c_uint64, C.c_uint64, C.c_uint64, _P, _P, _P]
     lib.nb_mlp_forward.argtypes = [C.c_int32, _P, C.c_uint64, _P, _P]

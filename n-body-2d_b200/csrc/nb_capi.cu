@@ -49,10 +49,14 @@ int check_params(const nb_params* p) {
         !std::isfinite(p->epsilon_squared) || !std::isfinite(p->bmax_ratio))
         return NB_ERR_INVALID;
     if (p->theta < 0.0 || p->epsilon_squared < 0.0 || p->bmax_ratio < 0.0) return NB_ERR_INVALID;
-    if (p->mode != NB_MODE_FP64 && p->mode != NB_MODE_SPLIT) return NB_ERR_INVALID;
-    if (p->leaf_size < 0 || (p->flags & ~(int32_t)(NB_FLAG_QUADRUPOLE | NB_FLAG_LEARNED)) != 0)
+    if (p->mode != NB_MODE_FP64 && p->mode != NB_MODE_SPLIT && p->mode != NB_MODE_ALLPAIRS)
         return NB_ERR_INVALID;
-    if ((p->flags & NB_FLAG_LEARNED) && p->mode != NB_MODE_SPLIT) return NB_ERR_INVALID;
+    if (p->leaf_size < 0 ||
+        (p->flags & ~(int32_t)(NB_FLAG_QUADRUPOLE | NB_FLAG_LEARNED | NB_FLAG_CPU_LAW)) != 0)
+        return NB_ERR_INVALID;
+    if ((p->flags & (NB_FLAG_LEARNED | NB_FLAG_QUADRUPOLE)) && p->mode != NB_MODE_SPLIT)
+        return NB_ERR_INVALID;
+    if ((p->flags & NB_FLAG_CPU_LAW) && p->mode != NB_MODE_ALLPAIRS) return NB_ERR_INVALID;
     return NB_OK;
 }
 
@@ -152,6 +156,9 @@ void free_all(nb_ctx* c) {
     cudaFree(c->acc);
     cudaFree(c->stage_pos);
     cudaFree(c->stage_vel);
+    cudaFree(c->render_count);
+    cudaFree(c->render_rgba);
+    cudaFree(c->render_table);
     cudaFree(c->acc32);
     cudaFree(c->mlp_params);
 }
@@ -219,6 +226,14 @@ void enqueue_step(nb_ctx* c, int parity, bool integrate, bool store_acc, bool ti
     };
     mark(0);
     cudaMemsetAsync(&c->scal->cell_terms, 0, 2 * sizeof(unsigned long long), c->stream);
+    if (c->p.mode == NB_MODE_ALLPAIRS) {
+        // AllPairsSim: drift into the other buffer, then the all-pairs kick there
+        for (int k = 1; k < 7; ++k) mark(k);
+        nb::launch_allpairs_step(c, A, B, integrate, store_acc);
+        mark(7);
+        mark(8);
+        return;
+    }
     nb::launch_bbox(c, A.pos);
     nb::launch_morton(c, A.pos);
     mark(1);
@@ -602,6 +617,48 @@ int nb_phase_times(nb_ctx* c, double* ms, int max) {
 }
 
 const char* nb_phase_name(int k) { return k >= 0 && k < nb::kPhases ? kPhaseNames[k] : ""; }
+
+int nb_render(nb_ctx* c, const nb_view* v, uint8_t* rgba_out) {
+    if (!c || !v || !rgba_out) return NB_ERR_INVALID;
+    if (v->res_x == 0 || v->res_y == 0 || v->res_x > 16384 || v->res_y > 16384 || v->reserved)
+        return fail(c, NB_ERR_INVALID, "resolution must be 1..16384 pixels per side");
+    if (!std::isfinite(v->x) || !std::isfinite(v->y) || !(v->width > 0.0) || !(v->height > 0.0) ||
+        !std::isfinite(v->width) || !std::isfinite(v->height))
+        return fail(c, NB_ERR_INVALID, "view rectangle must be finite with positive size");
+    if (!(v->point_diameter >= 1.f && v->point_diameter <= 50.f))
+        return fail(c, NB_ERR_INVALID, "point diameter must be 1..50 pixels");
+    DeviceGuard guard(c->device);
+    const int64_t pixels = (int64_t)v->res_x * v->res_y;
+    if (!c->render_table) {
+        // k successive blends of white at alpha 120/255 over black, 8 bits each
+        uint8_t table[256];
+        double cv = 0.0;
+        for (int k = 0; k < 256; ++k) {
+            table[k] = (uint8_t)cv;
+            cv = std::floor(120.0 + cv * 135.0 / 255.0 + 0.5);
+        }
+        NB_CUDA(c, dalloc(&c->render_table, 256));
+        NB_CUDA(c, cudaMemcpy(c->render_table, table, 256, cudaMemcpyHostToDevice));
+    }
+    if (c->render_pixels < pixels) {
+        NB_CUDA(c, cudaStreamSynchronize(c->stream));
+        cudaFree(c->render_count);
+        cudaFree(c->render_rgba);
+        c->render_count = nullptr;
+        c->render_rgba = nullptr;
+        c->render_pixels = 0;
+        NB_CUDA(c, dalloc(&c->render_count, pixels));
+        NB_CUDA(c, dalloc(&c->render_rgba, pixels));
+        c->render_pixels = pixels;
+    }
+    nb::launch_render(c, c->buf[c->parity].pos, *v, c->render_count, c->render_table,
+                      c->render_rgba);
+    NB_CUDA(c, cudaGetLastError());
+    NB_CUDA(c, cudaMemcpyAsync(rgba_out, c->render_rgba, (size_t)pixels * 4, cudaMemcpyDeviceToHost,
+                               c->stream));
+    NB_CUDA(c, cudaStreamSynchronize(c->stream));
+    return read_device_error(c);
+}
 
 int nb_autotune(nb_ctx* c, uint32_t steps, int32_t* leaf_out, int32_t* bpl_out) {
     if (!c || steps == 0) return NB_ERR_INVALID;

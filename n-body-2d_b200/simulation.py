@@ -69,6 +69,7 @@ class SimConfig:
     quadrupole: bool = False
     learned: bool = False
     bmax_ratio: float = 0.0
+    cpu_law: bool = False   # NB_MODE_ALLPAIRS: the reference CPU backends' pair law
 
     def params(self) -> NbParams:
         p = NbParams()
@@ -82,7 +83,8 @@ class SimConfig:
         p.device = self.device
         p.bmax_ratio = self.bmax_ratio
         p.flags = ((_lib.NB_FLAG_QUADRUPOLE if self.quadrupole else 0)
-                   | (_lib.NB_FLAG_LEARNED if self.learned else 0))
+                   | (_lib.NB_FLAG_LEARNED if self.learned else 0)
+                   | (_lib.NB_FLAG_CPU_LAW if self.cpu_law else 0))
         return p
 
 
@@ -204,6 +206,15 @@ class NbContext:
         if k < 0:
             check(-k, self._h)
         return {self._lib.nb_phase_name(i).decode(): float(ms[i]) for i in range(k)}
+
+    def render(self, view, point_diameter: float = 1.0) -> np.ndarray:
+        """The current bodies drawn as the reference's window would show them
+        (nb_render): view is a render.ViewPort or an NbView; returns
+        [res_y, res_x, 4] uint8, row 0 at the top."""
+        v = view.as_view(point_diameter) if hasattr(view, "as_view") else view
+        out = np.empty((v.res_y, v.res_x, 4), dtype=np.uint8)
+        check(self._lib.nb_render(self.handle, C.byref(v), out.ctypes.data), self._h)
+        return out
 
     def autotune(self, steps: int = 3) -> tuple[int, int]:
         """Times the SPLIT leaf sizes and group sizes; returns (leaf, bodies per lane)."""

@@ -52,3 +52,10 @@ def rel_err(a, b, floor=0.0):
     num = np.linalg.norm(np.asarray(a) - np.asarray(b), axis=-1)
     den = np.maximum(np.linalg.norm(np.asarray(b), axis=-1), floor)
     return num / den
+
+
+@pytest.fixture(scope="session")
+def orc_render():
+    from oracle import render_oracle
+
+    return render_oracle
