@@ -28,25 +28,16 @@ __device__ __forceinline__ double warp_max(double v) {
 
 // Exact FP64 min/max of all positions, reduced per block, then folded and
 // squared by the last block to finish (CU:78-114 + the host squaring at
-// CU:665-677, done here on the device in the same FP64 operations).
-__global__ void __launch_bounds__(kBoxThreads)
-bbox_kernel(const double2* __restrict__ pos, int64_t n, double* __restrict__ partials,
-            DeviceScalars* __restrict__ s) {
-    double xmin = INFINITY, xmax = -INFINITY, ymin = INFINITY, ymax = -INFINITY;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        const double2 p = __ldg(pos + i);
-        xmin = fmin(xmin, p.x);
-        xmax = fmax(xmax, p.x);
-        ymin = fmin(ymin, p.y);
-        ymax = fmax(ymax, p.y);
-    }
+// CU:665-677, done here on the device in the same FP64 operations).  Min and
+// max are exact in any order, so the reduction tree is free: each thread
+// keeps four loads in flight, and the last block folds the partials with all
+// its threads.
+__device__ __forceinline__ void box_fold(double& xmin, double& xmax, double& ymin, double& ymax,
+                                         double (*red)[kBoxThreads / 32]) {
     xmin = warp_min(xmin);
     xmax = warp_max(xmax);
     ymin = warp_min(ymin);
     ymax = warp_max(ymax);
-    __shared__ double red[4][kBoxThreads / 32];
-    __shared__ bool last_block;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (lane == 0) {
         red[0][warp] = xmin;
@@ -62,6 +53,38 @@ bbox_kernel(const double2* __restrict__ pos, int64_t n, double* __restrict__ par
             ymin = fmin(ymin, red[2][w]);
             ymax = fmax(ymax, red[3][w]);
         }
+    }
+}
+
+__global__ void __launch_bounds__(kBoxThreads)
+bbox_kernel(const double2* __restrict__ pos, int64_t n, double* __restrict__ partials,
+            DeviceScalars* __restrict__ s) {
+    double xmin = INFINITY, xmax = -INFINITY, ymin = INFINITY, ymax = -INFINITY;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    for (; i + 3 * stride < n; i += 4 * stride) {
+        double2 p[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) p[u] = __ldg(pos + i + u * stride);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            xmin = fmin(xmin, p[u].x);
+            xmax = fmax(xmax, p[u].x);
+            ymin = fmin(ymin, p[u].y);
+            ymax = fmax(ymax, p[u].y);
+        }
+    }
+    for (; i < n; i += stride) {
+        const double2 p = __ldg(pos + i);
+        xmin = fmin(xmin, p.x);
+        xmax = fmax(xmax, p.x);
+        ymin = fmin(ymin, p.y);
+        ymax = fmax(ymax, p.y);
+    }
+    __shared__ double red[4][kBoxThreads / 32];
+    __shared__ bool last_block;
+    box_fold(xmin, xmax, ymin, ymax, red);
+    if (threadIdx.x == 0) {
         double* out = partials + 4 * blockIdx.x;
         out[0] = xmin;
         out[1] = xmax;
@@ -72,18 +95,20 @@ bbox_kernel(const double2* __restrict__ pos, int64_t n, double* __restrict__ par
     }
     __syncthreads();
     if (!last_block) return;
+    __threadfence();
+    // CU:649-654 seeds with +-DBL_MAX; folding from there is identical.
+    double bx0 = 1.7976931348623157e308, bx1 = -1.7976931348623157e308;
+    double by0 = 1.7976931348623157e308, by1 = -1.7976931348623157e308;
+    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+        const double* in = partials + 4 * b;
+        bx0 = fmin(bx0, __ldcg(in + 0));
+        bx1 = fmax(bx1, __ldcg(in + 1));
+        by0 = fmin(by0, __ldcg(in + 2));
+        by1 = fmax(by1, __ldcg(in + 3));
+    }
+    __syncthreads();  // red[] is reused
+    box_fold(bx0, bx1, by0, by1, red);
     if (threadIdx.x == 0) {
-        __threadfence();
-        // CU:649-654 seeds with +-DBL_MAX; folding from there is identical.
-        double bx0 = 1.7976931348623157e308, bx1 = -1.7976931348623157e308;
-        double by0 = 1.7976931348623157e308, by1 = -1.7976931348623157e308;
-        for (unsigned b = 0; b < gridDim.x; ++b) {
-            const double* in = partials + 4 * b;
-            bx0 = fmin(bx0, __ldcg(in + 0));
-            bx1 = fmax(bx1, __ldcg(in + 1));
-            by0 = fmin(by0, __ldcg(in + 2));
-            by1 = fmax(by1, __ldcg(in + 3));
-        }
         const double x_range = bx1 - bx0;
         const double y_range = by1 - by0;
         if (x_range > y_range) {
