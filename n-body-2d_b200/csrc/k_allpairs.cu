@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
 #include <cmath>
 #include <string>
 
@@ -62,28 +63,30 @@ __global__ void allpairs_drift(nb::BodyBuffers a, nb::BodyBuffers b, int64_t n, 
     b.orig[i] = a.orig[i];
 }
 
-// Stage 2 (AllPairs.cpp:38-49): every body sums all others (the sum runs over
-// j in order, each pair evaluated from both sides: twice the reference's pair
-// evaluations, no atomics), then v += a G dt.  kCpuLaw: the law of
-// Simulation::force, a = m (p_j - p_i) / (d (d^2 + eps2)) (Simulation.cpp:
-// 74-80, G applied with the kick); otherwise Plummer's
-// a = m (p_j - p_i) (d^2 + eps2)^-3/2.
+// Stage 2 (AllPairs.cpp:38-49): every body sums all others (each pair is
+// evaluated from both sides: twice the reference's pair evaluations, no
+// atomics).  kCpuLaw: the law of Simulation::force,
+// a = m (p_j - p_i) / (d (d^2 + eps2)) (Simulation.cpp:74-80, G applied with
+// the kick); otherwise Plummer's a = m (p_j - p_i) (d^2 + eps2)^-3/2.  Block
+// (x, y) sums targets x*256.. over source chunk y; small systems split the
+// sources into chunks so that the grid fills the GPU, and the partial sums
+// are added in chunk order by the kick (deterministic).
 template <bool kCpuLaw>
 __global__ void __launch_bounds__(kThreads)
-allpairs_kick(double2* __restrict__ pos, const double* __restrict__ mass, double2* __restrict__ vel,
-              double2* __restrict__ acc_out, int64_t n, double eps2, double G_dt, int kick,
-              unsigned long long* __restrict__ body_terms) {
+allpairs_partial(const double2* __restrict__ pos, const double* __restrict__ mass, int64_t n,
+                 int64_t chunk, double eps2, double2* __restrict__ partial) {
     __shared__ double2 sp[kThreads];
     __shared__ double sm[kThreads];
     const int64_t i = blockIdx.x * (int64_t)kThreads + threadIdx.x;
     const double2 p = i < n ? pos[i] : make_double2(0.0, 0.0);
+    const int64_t s0 = blockIdx.y * chunk, s1 = min(n, s0 + chunk);
     double ax = 0.0, ay = 0.0;
-    for (int64_t base = 0; base < n; base += kThreads) {
+    for (int64_t base = s0; base < s1; base += kThreads) {
         const int64_t j = base + threadIdx.x;
-        sp[threadIdx.x] = j < n ? pos[j] : make_double2(0.0, 0.0);
-        sm[threadIdx.x] = j < n ? mass[j] : 0.0;
+        sp[threadIdx.x] = j < s1 ? pos[j] : make_double2(0.0, 0.0);
+        sm[threadIdx.x] = j < s1 ? mass[j] : 0.0;
         __syncthreads();
-        const int lim = (int)min((int64_t)kThreads, n - base);
+        const int lim = (int)min((int64_t)kThreads, s1 - base);
         for (int q = 0; q < lim; ++q) {
             if (base + q == i) continue;
             const double dx = sp[q].x - p.x;
@@ -101,7 +104,20 @@ allpairs_kick(double2* __restrict__ pos, const double* __restrict__ mass, double
         }
         __syncthreads();
     }
+    if (i < n) partial[blockIdx.y * n + i] = make_double2(ax, ay);
+}
+
+__global__ void allpairs_kick(const double2* __restrict__ partial, int chunks, int64_t n,
+                              double2* __restrict__ vel, double2* __restrict__ acc_out,
+                              double G_dt, int kick, unsigned long long* __restrict__ body_terms) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
+    double ax = 0.0, ay = 0.0;
+    for (int c = 0; c < chunks; ++c) {
+        const double2 a = partial[c * n + i];
+        ax += a.x;
+        ay += a.y;
+    }
     if (acc_out) acc_out[i] = make_double2(ax, ay);
     if (kick) {
         double2 v = vel[i];
@@ -109,28 +125,38 @@ allpairs_kick(double2* __restrict__ pos, const double* __restrict__ mass, double
         v.y += ay * G_dt;
         vel[i] = v;
     }
-    if (threadIdx.x == 0) atomicAdd(body_terms, (unsigned long long)min((int64_t)kThreads, n - i) * (n - 1));
+    if (threadIdx.x == 0)
+        atomicAdd(body_terms, (unsigned long long)min((int64_t)blockDim.x, n - i) * (n - 1));
 }
 
 }  // namespace
 
+int nb::allpairs_chunks(int64_t n, int sm_count) {
+    const int64_t xblocks = (n + kThreads - 1) / kThreads;
+    const int64_t want = (int64_t)sm_count * 8;  // blocks to fill the GPU a few times over
+    int64_t chunks = (want + xblocks - 1) / xblocks;
+    chunks = std::min<int64_t>(chunks, std::max<int64_t>(1, n / kThreads));
+    return (int)std::max<int64_t>(1, std::min<int64_t>(chunks, 64));
+}
+
 void nb::launch_allpairs_step(nb_ctx* c, const BodyBuffers& a, const BodyBuffers& b, bool integrate,
                               bool store_acc) {
     const unsigned blocks = (unsigned)((c->n + kThreads - 1) / kThreads);
-    c->launches += 2;
+    const int chunks = allpairs_chunks(c->n, c->sm_count);
+    const int64_t chunk = (c->n + chunks - 1) / chunks;
+    c->launches += 3;
     allpairs_drift<<<blocks, kThreads, 0, c->stream>>>(a, b, c->n, integrate ? c->p.timestep : 0.0);
-    const double G_dt = c->p.G * c->p.timestep;
-    double2* acc = store_acc ? c->acc : nullptr;
+    const dim3 grid(blocks, (unsigned)chunks);
     if (c->p.flags & NB_FLAG_CPU_LAW)
-        allpairs_kick<true><<<blocks, kThreads, 0, c->stream>>>(b.pos, b.mass, b.vel, acc, c->n,
-                                                                c->p.epsilon_squared, G_dt,
-                                                                integrate ? 1 : 0,
-                                                                &c->scal->body_terms);
+        allpairs_partial<true><<<grid, kThreads, 0, c->stream>>>(b.pos, b.mass, c->n, chunk,
+                                                                c->p.epsilon_squared, c->ap_partial);
     else
-        allpairs_kick<false><<<blocks, kThreads, 0, c->stream>>>(b.pos, b.mass, b.vel, acc, c->n,
-                                                                 c->p.epsilon_squared, G_dt,
-                                                                 integrate ? 1 : 0,
-                                                                 &c->scal->body_terms);
+        allpairs_partial<false><<<grid, kThreads, 0, c->stream>>>(b.pos, b.mass, c->n, chunk,
+                                                                 c->p.epsilon_squared, c->ap_partial);
+    allpairs_kick<<<blocks, kThreads, 0, c->stream>>>(c->ap_partial, chunks, c->n, b.vel,
+                                                       store_acc ? c->acc : nullptr,
+                                                       c->p.G * c->p.timestep, integrate ? 1 : 0,
+                                                       &c->scal->body_terms);
 }
 
 extern "C" int nb_allpairs_accelerations(int32_t device, uint64_t n, const double* mass,

@@ -90,6 +90,8 @@ int alloc_all(nb_ctx* c) {
     NB_CUDA(c, dalloc(&t.com, n));
     NB_CUDA(c, dalloc(&t.range, n));
     NB_CUDA(c, dalloc(&t.start_list, n));
+    if (c->p.mode == NB_MODE_ALLPAIRS)
+        NB_CUDA(c, dalloc(&c->ap_partial, n * (size_t)nb::allpairs_chunks((int64_t)n, c->sm_count)));
     if (c->p.mode == NB_MODE_SPLIT) {
         NB_CUDA(c, dalloc(&t.s64, n));
         NB_CUDA(c, dalloc(&t.cell4, n));
@@ -156,6 +158,7 @@ void free_all(nb_ctx* c) {
     cudaFree(c->acc);
     cudaFree(c->stage_pos);
     cudaFree(c->stage_vel);
+    cudaFree(c->ap_partial);
     cudaFree(c->render_count);
     cudaFree(c->render_rgba);
     cudaFree(c->render_table);

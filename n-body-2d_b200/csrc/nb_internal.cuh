@@ -152,6 +152,7 @@ struct nb_ctx {
     int split_blocks[16] = {};            // persistent grids of the SPLIT traversal variants
     float* mlp_params = nullptr;         // learned mode: FP32 MLP parameters (device)
     void* mlp_infer = nullptr;           // learned mode: BF16 fragment images for inference
+    double2* ap_partial = nullptr;       // NB_MODE_ALLPAIRS: per-source-chunk partial sums
     uint32_t* render_count = nullptr;    // nb_render: coverings per pixel
     uchar4* render_rgba = nullptr;       // nb_render: the image
     uint8_t* render_table = nullptr;     // nb_render: covering count -> 8-bit value
@@ -215,6 +216,7 @@ void launch_render(nb_ctx* c, const double2* pos, const nb_view& v, uint32_t* co
                    const uint8_t* table, uchar4* rgba);
 void launch_allpairs_step(nb_ctx* c, const BodyBuffers& a, const BodyBuffers& b, bool integrate,
                           bool store_acc);
+int allpairs_chunks(int64_t n, int sm_count);
 void launch_scatter(nb_ctx* c, const BodyBuffers& b, double2* out_pos, double2* out_vel,
                     const double2* acc, double2* out_acc);
 void launch_identity(nb_ctx* c, int32_t* orig);
