@@ -415,7 +415,7 @@ __device__ __forceinline__ void cell_moments(int id, const DeviceScalars* __rest
         t.cell4[id] = make_float4((float)(com.x - fc.x), (float)(com.y - fc.y), (float)M,
                                   accept_size2(s, bt, pos, first, t.level[id], com, accept_scale));
     }
-    if (kSplit && kSecond) {
+    if (kSplit && kSecond && !kFeat) {
         double sxx = 0.0, sxy = 0.0, syy = 0.0;
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
@@ -436,56 +436,55 @@ __device__ __forceinline__ void cell_moments(int id, const DeviceScalars* __rest
         double2* so = reinterpret_cast<double2*>(t.s64 + id);
         __stcg(so, make_double2(sxx, sxy));
         __stcg(so + 1, make_double2(syy, 0.0));
-        if (kFeat) {
-            // Third moments T_ijk about the COM, by the same shift rule
-            // (u = u_child + d):
-            //   T += T_c + (d_i S_c,jk + d_j S_c,ik + d_k S_c,ij) + m d_i d_j d_k
-            double txxx = 0.0, txxy = 0.0, txyy = 0.0, tyyy = 0.0, mmax = 0.0;
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const int r = refs[q];
-                if (r == INT_MIN) continue;
-                const double m = cm[q];
-                mmax = fmax(mmax, m);
-                const double dx = cmx[q] - com.x, dy = cmy[q] - com.y;
-                double cxx = 0.0, cxy = 0.0, cyy = 0.0;
-                double c3[4] = {0.0, 0.0, 0.0, 0.0};
-                if (r >= 0) {
-                    const double2* sc = reinterpret_cast<const double2*>(t.s64 + r);
-                    const double2 s01 = __ldcg(sc), s2 = __ldcg(sc + 1);
-                    cxx = s01.x;
-                    cxy = s01.y;
-                    cyy = s2.x;
-                    const double2* tc = reinterpret_cast<const double2*>(t.t64 + r);
-                    const double2 t01 = __ldcg(tc), t23 = __ldcg(tc + 1);
-                    c3[0] = t01.x;
-                    c3[1] = t01.y;
-                    c3[2] = t23.x;
-                    c3[3] = t23.y;
-                }
-                txxx += c3[0] + 3.0 * dx * cxx + m * dx * dx * dx;
-                txxy += c3[1] + 2.0 * dx * cxy + dy * cxx + m * dx * dx * dy;
-                txyy += c3[2] + dx * cyy + 2.0 * dy * cxy + m * dx * dy * dy;
-                tyyy += c3[3] + 3.0 * dy * cyy + m * dy * dy * dy;
-            }
-            double2* to = reinterpret_cast<double2*>(t.t64 + id);
-            __stcg(to, make_double2(txxx, txxy));
-            __stcg(to + 1, make_double2(txyy, tyyy));
-            // the MLP's cell features, normalised by M and the cell width; the
-            // network reads them as BF16, so they are stored rounded
-            const double w2 = cell_width2(s, bt, t.range[id].x, t.level[id]), w = sqrt(w2);
-            const double im2 = 1.0 / (M * w2), im3 = im2 / w;
-            t.cellh[id] = make_uint4(bf16_pair((float)(mmax / M), (float)(sxx * im2)),
-                                     bf16_pair((float)(sxy * im2), (float)(syy * im2)),
-                                     bf16_pair((float)(txxx * im3), (float)(txxy * im3)),
-                                     bf16_pair((float)(txyy * im3), (float)(tyyy * im3)));
-            t.cellw[id] = (float)w;
-        }
         const int first = t.range[id].x;
         const double2 fc = frame_center(s, bt, first);
         t.cell4[id] = make_float4((float)(com.x - fc.x), (float)(com.y - fc.y), (float)M,
                                   accept_size2(s, bt, pos, first, t.level[id], com, accept_scale));
         t.cellq[id] = make_float4((float)sxx, (float)sxy, (float)syy, 0.f);
+    }
+    if (kSplit && kFeat) {
+        // The learned features: second and third moments about the COM by the
+        // parallel-axis shift, in FP32 (they only feed BF16 features):
+        //   S += S_c + m d d^T
+        //   T += T_c + (d_i S_c,jk + d_j S_c,ik + d_k S_c,ij) + m d_i d_j d_k
+        float sxx = 0.f, sxy = 0.f, syy = 0.f;
+        float txxx = 0.f, txxy = 0.f, txyy = 0.f, tyyy = 0.f;
+        double mmax = 0.0;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int r = refs[q];
+            if (r == INT_MIN) continue;
+            const float m = (float)cm[q];
+            mmax = fmax(mmax, cm[q]);
+            const float dx = (float)(cmx[q] - com.x), dy = (float)(cmy[q] - com.y);
+            float4 cs = make_float4(0.f, 0.f, 0.f, 0.f), ct = cs;
+            if (r >= 0) {
+                cs = __ldcg(t.cellq + r);
+                ct = __ldcg(t.t32 + r);
+            }
+            txxx += ct.x + 3.f * dx * cs.x + m * dx * dx * dx;
+            txxy += ct.y + 2.f * dx * cs.y + dy * cs.x + m * dx * dx * dy;
+            txyy += ct.z + dx * cs.z + 2.f * dy * cs.y + m * dx * dy * dy;
+            tyyy += ct.w + 3.f * dy * cs.z + m * dy * dy * dy;
+            sxx += cs.x + m * dx * dx;
+            sxy += cs.y + m * dx * dy;
+            syy += cs.z + m * dy * dy;
+        }
+        __stcg(t.cellq + id, make_float4(sxx, sxy, syy, 0.f));
+        __stcg(t.t32 + id, make_float4(txxx, txxy, txyy, tyyy));
+        // the MLP's cell features, normalised by M and the cell width; the
+        // network reads them as BF16, so they are stored rounded
+        const int first = t.range[id].x;
+        const double w2 = cell_width2(s, bt, first, t.level[id]), w = sqrt(w2);
+        const float im2 = (float)(1.0 / (M * w2)), im3 = (float)(1.0 / (M * w2 * w));
+        t.cellh[id] = make_uint4(bf16_pair((float)(mmax / M), sxx * im2),
+                                 bf16_pair(sxy * im2, syy * im2),
+                                 bf16_pair(txxx * im3, txxy * im3),
+                                 bf16_pair(txyy * im3, tyyy * im3));
+        t.cellw[id] = (float)w;
+        const double2 fc = frame_center(s, bt, first);
+        t.cell4[id] = make_float4((float)(com.x - fc.x), (float)(com.y - fc.y), (float)M,
+                                  accept_size2(s, bt, pos, first, t.level[id], com, accept_scale));
     }
 }
 

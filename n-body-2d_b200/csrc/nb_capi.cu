@@ -102,7 +102,7 @@ int alloc_all(nb_ctx* c) {
         NB_CUDA(c, dalloc(&t.groups, n));
     }
     if (c->p.flags & NB_FLAG_LEARNED) {
-        NB_CUDA(c, dalloc(&t.t64, n));
+        NB_CUDA(c, dalloc(&t.t32, n));
         NB_CUDA(c, dalloc(&t.cellh, n));
         NB_CUDA(c, dalloc(&t.cellw, n));
         NB_CUDA(c, dalloc(&t.band, (size_t)nb::kBandPerBody * n));
@@ -150,7 +150,7 @@ void free_all(nb_ctx* c) {
                          t.leaf_plevel, t.bucket_mass, t.bucket_com, t.flag,      t.cell_of,
                          t.start_of,  t.range,       t.s64,         t.cell4,      t.cellq,
                          t.body4,     t.gcount,      t.gbase,       t.groups,     t.rep_of,
-                         t.t64,       t.cellh,       t.cellw,       t.band,       t.band_count,
+                         t.t32,       t.cellh,       t.cellw,       t.band,       t.band_count,
                          t.start_list};
     for (void* q : tree_ptrs) cudaFree(q);
     cudaFree(c->scal);

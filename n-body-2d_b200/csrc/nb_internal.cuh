@@ -92,7 +92,7 @@ struct Tree {
     // learned correction: third moments (FP64, bottom-up) and the per-cell
     // MLP features (see k_mlp.cu): the eight moment features as BF16 and the
     // cell width
-    double4* t64 = nullptr;      // {Txxx, Txxy, Txyy, Tyyy}
+    float4* t32 = nullptr;       // {Txxx, Txxy, Txyy, Tyyy} (FP32: they only feed BF16 features)
     uint4* cellh = nullptr;      // BF16 pairs {f3 f4, f5 f6, f7 f8, f9 f10}
     float* cellw = nullptr;
     int32_t* band = nullptr;       // per group: band cells, kBandPerBody x first body onwards
