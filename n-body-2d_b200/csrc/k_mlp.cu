@@ -592,9 +592,9 @@ mlp_samples_kernel(Tree t, const DeviceScalars* __restrict__ s, const double2* _
                 const double scale = (double)dc2 / (M * nb);
                 const unsigned slot = atomicAdd(count, 1u);
                 if (slot < cap) {
-                    const PointFeatures pf = point_features(ux, uy, t.cellw[ref], c4.z,
-                                                            (float)eps2);
-                    const uint4 h = t.cellh[ref];
+                    const float w = __uint_as_float(t.cellh[2 * ref + 1].w);
+                    const PointFeatures pf = point_features(ux, uy, w, c4.z, (float)eps2);
+                    const uint4 h = t.cellh[2 * ref];
                     const float x[kNin] = {pf.x0,       pf.x1,       pf.x2,       bf16_lo(h.x),
                                            bf16_hi(h.x), bf16_lo(h.y), bf16_hi(h.y), bf16_lo(h.z),
                                            bf16_hi(h.z), bf16_lo(h.w), bf16_hi(h.w), pf.x11};
@@ -805,10 +805,12 @@ mlp_correct_kick(const InferW* __restrict__ Wg, Tree t, const DeviceScalars* __r
             float sc = 0.f;
             if (r < nband) {
                 const int ref = band[r];
-                const float4 c4 = t.cell4[ref];
-                const PointFeatures pf = point_features(gx - c4.x, gy - c4.y, t.cellw[ref], c4.z,
-                                                        eps2);
-                lo = t.cellh[ref];
+                // one 32-byte record: the BF16 features, then COM, mass, width
+                lo = t.cellh[2 * ref];
+                const uint4 gb = t.cellh[2 * ref + 1];
+                const PointFeatures pf =
+                    point_features(gx - __uint_as_float(gb.x), gy - __uint_as_float(gb.y),
+                                   __uint_as_float(gb.w), __uint_as_float(gb.z), eps2);
                 hi = make_uint4(pack_bf16(pf.x0, pf.x1), pack_bf16(pf.x2, pf.x11), 0u, 0u);
                 sc = pf.scale;
             }

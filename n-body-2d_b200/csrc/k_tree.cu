@@ -477,14 +477,17 @@ __device__ __forceinline__ void cell_moments(int id, const DeviceScalars* __rest
         const int first = t.range[id].x;
         const double w2 = cell_width2(s, bt, first, t.level[id]), w = sqrt(w2);
         const float im2 = (float)(1.0 / (M * w2)), im3 = (float)(1.0 / (M * w2 * w));
-        t.cellh[id] = make_uint4(bf16_pair((float)(mmax / M), sxx * im2),
-                                 bf16_pair(sxy * im2, syy * im2),
-                                 bf16_pair(txxx * im3, txxy * im3),
-                                 bf16_pair(txyy * im3, tyyy * im3));
-        t.cellw[id] = (float)w;
         const double2 fc = frame_center(s, bt, first);
-        t.cell4[id] = make_float4((float)(com.x - fc.x), (float)(com.y - fc.y), (float)M,
-                                  accept_size2(s, bt, pos, first, t.level[id], com, accept_scale));
+        const float4 c4 = make_float4((float)(com.x - fc.x), (float)(com.y - fc.y), (float)M,
+                                      accept_size2(s, bt, pos, first, t.level[id], com,
+                                                   accept_scale));
+        t.cell4[id] = c4;
+        t.cellh[2 * id] = make_uint4(bf16_pair((float)(mmax / M), sxx * im2),
+                                     bf16_pair(sxy * im2, syy * im2),
+                                     bf16_pair(txxx * im3, txxy * im3),
+                                     bf16_pair(txyy * im3, tyyy * im3));
+        t.cellh[2 * id + 1] = make_uint4(__float_as_uint(c4.x), __float_as_uint(c4.y),
+                                         __float_as_uint(c4.z), __float_as_uint((float)w));
     }
 }
 

@@ -103,8 +103,7 @@ int alloc_all(nb_ctx* c) {
     }
     if (c->p.flags & NB_FLAG_LEARNED) {
         NB_CUDA(c, dalloc(&t.t32, n));
-        NB_CUDA(c, dalloc(&t.cellh, n));
-        NB_CUDA(c, dalloc(&t.cellw, n));
+        NB_CUDA(c, dalloc(&t.cellh, 2 * n));
         NB_CUDA(c, dalloc(&t.band, (size_t)nb::kBandPerBody * n));
         NB_CUDA(c, dalloc(&t.band_count, n));
         NB_CUDA(c, dalloc(&c->acc32, n));
@@ -150,7 +149,7 @@ void free_all(nb_ctx* c) {
                          t.leaf_plevel, t.bucket_mass, t.bucket_com, t.flag,      t.cell_of,
                          t.start_of,  t.range,       t.s64,         t.cell4,      t.cellq,
                          t.body4,     t.gcount,      t.gbase,       t.groups,     t.rep_of,
-                         t.t32,       t.cellh,       t.cellw,       t.band,       t.band_count,
+                         t.t32,       t.cellh,       t.band,        t.band_count,
                          t.start_list};
     for (void* q : tree_ptrs) cudaFree(q);
     cudaFree(c->scal);

@@ -93,8 +93,10 @@ struct Tree {
     // MLP features (see k_mlp.cu): the eight moment features as BF16 and the
     // cell width
     float4* t32 = nullptr;       // {Txxx, Txxy, Txyy, Tyyy} (FP32: they only feed BF16 features)
-    uint4* cellh = nullptr;      // BF16 pairs {f3 f4, f5 f6, f7 f8, f9 f10}
-    float* cellw = nullptr;
+    // two uint4 per cell (one 32-byte sector for the correction's gathers):
+    // BF16 pairs {f3 f4, f5 f6, f7 f8, f9 f10}, then the float bits of
+    // {com_x - cx, com_y - cy, mass, width}
+    uint4* cellh = nullptr;
     int32_t* band = nullptr;       // per group: band cells, kBandPerBody x first body onwards
     int32_t* band_count = nullptr; // per group: band cells found
     int32_t* start_list = nullptr; // cells without internal children, in any order
