@@ -749,9 +749,9 @@ __device__ __forceinline__ void infer_tiles(const InferW& W, const uint32_t (*a)
     }
 }
 
-// at most 128 registers: four blocks of four warps per SM (measured faster
-// than three blocks without the cap, despite a few spilled bytes)
-__global__ void __launch_bounds__(kCorrWarps * 32, 4)
+// at most 102 registers: five blocks of four warps per SM (measured faster
+// than four or six, despite a few spilled bytes)
+__global__ void __launch_bounds__(kCorrWarps * 32, 5)
 mlp_correct_kick(const InferW* __restrict__ Wg, Tree t, const DeviceScalars* __restrict__ s,
                  double2* __restrict__ pos, double2* __restrict__ vel,
                  const float2* __restrict__ acc32, double2* __restrict__ acc_out, int n,
