@@ -250,6 +250,19 @@ def run_reference(args) -> None:
         sample = (f"{args.steps} timed steps of the full N={args.n} workload, CPU restatement "
                   f"of the reference GPU step, {cores} OpenMP threads")
     value = args.n / t
+    ref_gpu = None
+    if args.workload == "disc16k":
+        # config 0 is small enough for the reference's own GPU kernels, on the
+        # same inputs (the stack bound is checked by the oracle first)
+        from oracle import refgpu
+
+        r = refgpu.time_steps(m, p, v, theta=args.theta, steps=args.steps)
+        ref_gpu = ({"value": args.n / r["seconds_per_step"], "unit": "body-steps/s",
+                    "ms_per_step": r["seconds_per_step"] * 1e3, "max_stack": r["max_stack"],
+                    "how": "the reference's CUDA kernels (BarnesHutCuda.cu, unmodified) under the "
+                           "harness driver, host clock over K steps after one untimed step, "
+                           "without the per-step download of the bodies"}
+                   if "seconds_per_step" in r else r)
     line = {
         "impl": "reference", "metric": "body-steps/s", "value": value, "unit": "body-steps/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
@@ -260,6 +273,8 @@ def run_reference(args) -> None:
         "e2e": {"value": value, "unit": "body-steps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
+    if ref_gpu is not None:
+        line["reference_gpu"] = ref_gpu
     print(json.dumps(line), flush=True)
 
 

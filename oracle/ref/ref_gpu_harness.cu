@@ -18,13 +18,15 @@
 // Usage: ref_gpu_harness <input> <output>
 // input : int64 n, steps, pad, pad; double theta, epsilon_squared, dt, G;
 //         mass[n]; pos[2n]; vel[2n]
-// output: int64 n, nodes_allocated, levels, pad; double box[4] (squared, first
+// output: int64 n, nodes_allocated, levels, ns per step (steps 1.. on the host
+//         clock, 0 for one step); double box[4] (squared, first
 //         step); uint64 sorted codes[n]; int32 permutation[n]; int32 orig[n];
 //         double acc[2n] (first step, sorted order, without G);
 //         double pos[2n], vel[2n] (after all steps, original order)
 #include "BarnesHutCuda.cu"
 
 #include <cfloat>
+#include <chrono>
 #include <cstdio>
 #include <vector>
 
@@ -200,7 +202,11 @@ int main(int argc, char** argv) {
     std::vector<double> acc(2 * n);
     BarnesHutCuda::Box box0{};
     int32_t nodes0 = 0, levels0 = 0;
+    // steps after the first are timed on the host clock: the reference's step
+    // is host-driven (a D2H count per tree level), so its cost is wall time
+    std::chrono::steady_clock::time_point t1;
     for (int64_t step = 0; step < steps; ++step) {
+        if (step == 1) t1 = std::chrono::steady_clock::now();
         squared_box(s);
         sort_and_reorder(s);
         build_tree(s);
@@ -220,6 +226,9 @@ int main(int argc, char** argv) {
         Kernel::update_positions<<<(n + BLOCK_SIZE - 1) / BLOCK_SIZE, BLOCK_SIZE>>>(s.pos, s.vel, n, dt);
         CUDA_CHECK(cudaDeviceSynchronize());
     }
+    const double timed = steps > 1 ? std::chrono::duration<double>(
+                                         std::chrono::steady_clock::now() - t1).count()
+                                   : 0.0;
     Kernel::scatter_to_original_order<<<(n + BLOCK_SIZE - 1) / BLOCK_SIZE, BLOCK_SIZE>>>(
         s.pos, s.vel, s.idx, s.pos_alt, s.vel_alt, n);
     CUDA_CHECK(cudaDeviceSynchronize());
@@ -228,7 +237,9 @@ int main(int argc, char** argv) {
 
     std::FILE* out = std::fopen(argv[2], "wb");
     if (!out) return 6;
-    const int64_t oh[4] = {n, nodes0, levels0, 0};
+    // header word 3: nanoseconds per step over steps 1.. (0 for a single step)
+    const int64_t ns_per_step = steps > 1 ? (int64_t)(timed * 1e9 / (double)(steps - 1)) : 0;
+    const int64_t oh[4] = {n, nodes0, levels0, ns_per_step};
     std::fwrite(oh, 8, 4, out);
     std::fwrite(&box0, 8, 4, out);
     std::fwrite(codes.data(), 8, n, out);
