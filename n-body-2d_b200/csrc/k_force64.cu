@@ -159,6 +159,23 @@ __global__ void scatter_kernel(const double2* __restrict__ pos, const double2* _
     if (out_acc) out_acc[o] = acc[i];
 }
 
+// Uploaded bodies: orig = identity, and the checks nb_upload promises
+// (finite positions and velocities, positive finite masses) done on the
+// device: bit 0 of *bad for a non-finite value, bit 1 for a mass <= 0.
+__global__ void upload_kernel(int32_t* __restrict__ orig, const double* __restrict__ mass,
+                              const double2* __restrict__ pos, const double2* __restrict__ vel,
+                              int64_t n, unsigned* __restrict__ bad) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    orig[i] = (int32_t)i;
+    const double m = mass[i];
+    const double2 p = pos[i], v = vel[i];
+    unsigned f = 0;
+    if (!(isfinite(m) && isfinite(p.x) && isfinite(p.y) && isfinite(v.x) && isfinite(v.y))) f |= 1u;
+    if (!(m > 0.0)) f |= 2u;
+    if (__any_sync(__activemask(), f != 0) && f) atomicOr(bad, f);
+}
+
 __global__ void identity_kernel(int32_t* orig, int64_t n) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i < n) orig[i] = (int32_t)i;
@@ -194,6 +211,12 @@ void launch_scatter(nb_ctx* c, const BodyBuffers& b, double2* out_pos, double2* 
 void launch_identity(nb_ctx* c, int32_t* orig) {
     c->launches += 1;
     identity_kernel<<<blocks_for(c->n, 256), 256, 0, c->stream>>>(orig, c->n);
+}
+
+void launch_upload_check(nb_ctx* c, const BodyBuffers& b, unsigned* bad) {
+    c->launches += 1;
+    upload_kernel<<<blocks_for(c->n, 256), 256, 0, c->stream>>>(b.orig, b.mass, b.pos, b.vel, c->n,
+                                                                 bad);
 }
 
 }  // namespace nb

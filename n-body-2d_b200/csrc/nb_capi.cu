@@ -37,11 +37,6 @@ cudaError_t dalloc(T** p, size_t count) {
     return cudaMalloc(reinterpret_cast<void**>(p), sizeof(T) * (count ? count : 1));
 }
 
-bool finite_array(const double* a, size_t count) {
-    for (size_t i = 0; i < count; ++i)
-        if (!std::isfinite(a[i])) return false;
-    return true;
-}
 
 int check_params(const nb_params* p) {
     if (!p) return NB_ERR_INVALID;
@@ -441,21 +436,27 @@ int nb_destroy(nb_ctx* c) {
     return NB_OK;
 }
 
+// The bodies are checked on the device after the copy (a host loop over 5n
+// doubles costs more than the copy itself).  A rejected upload has already
+// replaced the state: upload valid bodies before stepping again.
 int nb_upload(nb_ctx* c, const double* mass, const double* pos_xy, const double* vel_xy) {
     if (!c || !mass || !pos_xy || !vel_xy) return NB_ERR_INVALID;
     const size_t n = (size_t)c->n;
-    if (!finite_array(mass, n) || !finite_array(pos_xy, 2 * n) || !finite_array(vel_xy, 2 * n))
-        return fail(c, NB_ERR_INVALID, "non-finite mass, position or velocity");
-    for (size_t i = 0; i < n; ++i)
-        if (!(mass[i] > 0.0)) return fail(c, NB_ERR_INVALID, "masses must be positive");
     DeviceGuard guard(c->device);
     c->parity = 0;
     const nb::BodyBuffers& A = c->buf[0];
+    NB_CUDA(c, cudaMemsetAsync(&c->scal->upload_bad, 0, sizeof(unsigned), c->stream));
     NB_CUDA(c, cudaMemcpyAsync(A.mass, mass, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     NB_CUDA(c, cudaMemcpyAsync(A.pos, pos_xy, n * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
     NB_CUDA(c, cudaMemcpyAsync(A.vel, vel_xy, n * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
-    nb::launch_identity(c, A.orig);
+    nb::launch_upload_check(c, A, &c->scal->upload_bad);
     NB_CUDA(c, cudaGetLastError());
+    unsigned bad = 0;
+    NB_CUDA(c, cudaMemcpyAsync(&bad, &c->scal->upload_bad, sizeof(unsigned), cudaMemcpyDeviceToHost,
+                               c->stream));
+    NB_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (bad & 1u) return fail(c, NB_ERR_INVALID, "non-finite mass, position or velocity");
+    if (bad & 2u) return fail(c, NB_ERR_INVALID, "masses must be positive");
     return NB_OK;
 }
 

@@ -40,6 +40,7 @@ struct DeviceScalars {
     unsigned long long cell_terms;
     unsigned long long body_terms;
     int32_t nstart;           // cells whose children are all leaves (climb starts)
+    unsigned upload_bad;      // nb_upload's checks: bit 0 non-finite, bit 1 mass <= 0
 };
 
 // Batched universes (nb_batch_create): bodies of universe u occupy the fixed
@@ -214,6 +215,7 @@ void launch_groups(nb_ctx* c);
 void launch_force_split(nb_ctx* c, const BodyBuffers& b, bool kick, bool store_acc);
 void launch_force_fp64(nb_ctx* c, const BodyBuffers& b, bool kick, bool store_acc);
 void launch_drift(nb_ctx* c, const BodyBuffers& b);
+void launch_upload_check(nb_ctx* c, const BodyBuffers& b, unsigned* bad);
 void launch_render(nb_ctx* c, const double2* pos, const nb_view& v, uint32_t* count,
                    const uint8_t* table, uchar4* rgba);
 void launch_allpairs_step(nb_ctx* c, const BodyBuffers& a, const BodyBuffers& b, bool integrate,

@@ -189,3 +189,26 @@ def test_allpairs_kernel_matches_oracle(nbp, orc):
     acc = nbp.allpairs_accelerations(m, p, tgt, EPS2)
     acc_o = orc.allpairs_plummer(m, p, tgt, eps2=EPS2)
     assert rel_err(acc, acc_o).max() < 1e-12
+
+
+def test_upload_rejects_non_finite_and_non_positive_masses(nbp):
+    m, p, v = nbp.universes.exponential_disc(5000, 1)
+    with nbp.NbContext(nbp.SimConfig(mode=nbp.NB_MODE_SPLIT), m, p, v) as ctx:
+        bad = p.copy()
+        bad[1234, 1] = np.nan
+        with pytest.raises(nbp.NbError, match="non-finite"):
+            ctx.upload(m, bad, v)
+        badv = v.copy()
+        badv[17, 0] = np.inf
+        with pytest.raises(nbp.NbError, match="non-finite"):
+            ctx.upload(m, p, badv)
+        badm = m.copy()
+        badm[4999] = 0.0
+        with pytest.raises(nbp.NbError, match="positive"):
+            ctx.upload(badm, p, v)
+        ctx.upload(m, p, v)
+        ctx.step(1)
+        p1, _ = ctx.download()
+        assert np.isfinite(p1).all()
+    with pytest.raises(nbp.NbError):
+        nbp.NbContext(nbp.SimConfig(), -m, p, v)
