@@ -108,6 +108,16 @@ NB_API int nb_params_default(nb_params* p);
 NB_API int nb_create(const nb_params* p, uint64_t n, const double* mass, const double* pos_xy,
               const double* vel_xy, nb_ctx** out);
 
+/* Asynchronous form of nb_download: enqueues the same copy after the steps
+ * enqueued so far and returns at once.  The device-to-host copy runs on the
+ * context's copy stream, so it overlaps whatever is enqueued next (an
+ * nb_upload's host-to-device copy, the next nb_step).  pos_xy / vel_xy must
+ * stay valid, and be pinned for the copy to be asynchronous, until
+ * nb_download_wait (or nb_sync) returns.  No counterpart in the reference,
+ * which copies the bodies back synchronously every step (CU:632-646). */
+NB_API int nb_download_async(nb_ctx* ctx, double* pos_xy, double* vel_xy);
+NB_API int nb_download_wait(nb_ctx* ctx);
+
 /* Headless rendering of the current bodies into an RGBA8 image: the frame
  * the reference draws (src/Graphics/src/Graphics.cpp:122-128) through
  * SFML/OpenGL, without a graphics stack.  The view is the reference's

@@ -37,7 +37,7 @@ EXPORTS = (
     "nb_debug_tree", "nb_get_stats", "nb_last_error", "nb_status_string",
     "nb_allpairs_accelerations", "nb_phase_times", "nb_phase_name", "nb_morton_sort_static",
     "nb_set_mlp_weights", "nb_mlp_samples", "nb_mlp_forward", "nb_mlp_loss_grad", "nb_mlp_train",
-    "nb_batch_create", "nb_autotune", "nb_render",
+    "nb_batch_create", "nb_autotune", "nb_render", "nb_download_async", "nb_download_wait",
 )
 
 
@@ -132,6 +132,8 @@ def load() -> C.CDLL:
                                     C.POINTER(_P)]
     lib.nb_autotune.argtypes = [_P, C.c_uint32, _P, _P]
     lib.nb_render.argtypes = [_P, C.POINTER(NbView), _P]
+    lib.nb_download_async.argtypes = [_P, _P, _P]
+    lib.nb_download_wait.argtypes = [_P]
     lib.nb_set_mlp_weights.argtypes = [_P, _P]
     lib.nb_mlp_samples.argtypes = [_P, C.c_uint64, C.c_uint64, C.c_uint64, _P, _P, _P]
     lib.nb_mlp_forward.argtypes = [C.c_int32, _P, C.c_uint64, _P, _P]

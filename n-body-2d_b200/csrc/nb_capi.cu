@@ -382,7 +382,10 @@ int create_context(const nb_params* p, uint64_t n, const double* mass, const dou
     int rc = NB_OK;
     if (cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess ||
         cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) {
+        cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->staged, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->copied, cudaEventDisableTiming) != cudaSuccess) {
         rc = NB_ERR_CUDA;
     }
     for (auto& e : c->phase_ev)
@@ -424,11 +427,15 @@ int nb_destroy(nb_ctx* c) {
     if (!c) return NB_OK;
     DeviceGuard guard(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
     drop_graphs(c);
     free_all(c);
     free_batch(c);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->staged) cudaEventDestroy(c->staged);
+    if (c->copied) cudaEventDestroy(c->copied);
+    if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     for (auto& e : c->phase_ev)
         if (e) cudaEventDestroy(e);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -497,10 +504,41 @@ int nb_sync(nb_ctx* c) {
     if (!c) return NB_ERR_INVALID;
     DeviceGuard guard(c->device);
     NB_CUDA(c, cudaStreamSynchronize(c->stream));
+    NB_CUDA(c, cudaStreamSynchronize(c->copy_stream));
     float ms = 0.f;
     if (c->batch_steps && cudaEventElapsedTime(&ms, c->ev0, c->ev1) == cudaSuccess)
         c->ms_last = ms / c->batch_steps;
     c->batch_steps = 0;
+    return read_device_error(c);
+}
+
+int nb_download_async(nb_ctx* c, double* pos_xy, double* vel_xy) {
+    if (!c) return NB_ERR_INVALID;
+    if (!pos_xy && !vel_xy) return NB_OK;
+    DeviceGuard guard(c->device);
+    const nb::BodyBuffers& A = c->buf[c->parity];
+    const size_t bytes = (size_t)c->n * sizeof(double2);
+    // the staging buffers are reused: the previous copy-out must be done
+    NB_CUDA(c, cudaStreamWaitEvent(c->stream, c->copied, 0));
+    nb::launch_scatter(c, A, pos_xy ? c->stage_pos : nullptr, vel_xy ? c->stage_vel : nullptr,
+                       nullptr, nullptr);
+    NB_CUDA(c, cudaGetLastError());
+    NB_CUDA(c, cudaEventRecord(c->staged, c->stream));
+    NB_CUDA(c, cudaStreamWaitEvent(c->copy_stream, c->staged, 0));
+    if (pos_xy)
+        NB_CUDA(c, cudaMemcpyAsync(pos_xy, c->stage_pos, bytes, cudaMemcpyDeviceToHost,
+                                   c->copy_stream));
+    if (vel_xy)
+        NB_CUDA(c, cudaMemcpyAsync(vel_xy, c->stage_vel, bytes, cudaMemcpyDeviceToHost,
+                                   c->copy_stream));
+    NB_CUDA(c, cudaEventRecord(c->copied, c->copy_stream));
+    return NB_OK;
+}
+
+int nb_download_wait(nb_ctx* c) {
+    if (!c) return NB_ERR_INVALID;
+    DeviceGuard guard(c->device);
+    NB_CUDA(c, cudaStreamSynchronize(c->copy_stream));
     return read_device_error(c);
 }
 
@@ -510,6 +548,7 @@ int nb_download(nb_ctx* c, double* pos_xy, double* vel_xy) {
     DeviceGuard guard(c->device);
     const nb::BodyBuffers& A = c->buf[c->parity];
     const size_t bytes = (size_t)c->n * sizeof(double2);
+    NB_CUDA(c, cudaStreamWaitEvent(c->stream, c->copied, 0));
     nb::launch_scatter(c, A, pos_xy ? c->stage_pos : nullptr, vel_xy ? c->stage_vel : nullptr,
                        nullptr, nullptr);
     NB_CUDA(c, cudaGetLastError());

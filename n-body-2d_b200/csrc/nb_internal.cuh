@@ -143,6 +143,9 @@ struct nb_ctx {
     int sm_count = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaStream_t copy_stream = nullptr;  // nb_download_async: device-to-host copies
+    cudaEvent_t staged = nullptr;        // the download's scatter into the staging buffers is done
+    cudaEvent_t copied = nullptr;        // the staging buffers have been copied out (free again)
     cudaEvent_t phase_ev[nb::kPhases + 1] = {};
     int parity = 0;                 // which BodyBuffers holds the state
     nb::BodyBuffers buf[2];

@@ -164,6 +164,17 @@ class NbContext:
         check(self._lib.nb_download(self.handle, ptr(pos), ptr(vel)), self._h)
         return pos, vel
 
+    def download_async(self, pos: np.ndarray, vel: np.ndarray) -> None:
+        """nb_download_async: the copy overlaps what is enqueued next; pos and
+        vel (pinned, [n, 2] float64) are valid after download_wait()."""
+        for a in (pos, vel):
+            if a.shape != (self.n, 2) or a.dtype != np.float64 or not a.flags.c_contiguous:
+                raise ValueError("download_async needs C-contiguous float64 [n, 2] arrays")
+        check(self._lib.nb_download_async(self.handle, ptr(pos), ptr(vel)), self._h)
+
+    def download_wait(self) -> None:
+        check(self._lib.nb_download_wait(self.handle), self._h)
+
     def accelerations(self) -> np.ndarray:
         acc = np.empty((self.n, 2))
         check(self._lib.nb_accelerations(self.handle, ptr(acc)), self._h)

@@ -212,3 +212,26 @@ def test_upload_rejects_non_finite_and_non_positive_masses(nbp):
         assert np.isfinite(p1).all()
     with pytest.raises(nbp.NbError):
         nbp.NbContext(nbp.SimConfig(), -m, p, v)
+
+
+def test_download_async_matches_download(nbp):
+    torch = pytest.importorskip("torch")
+    m, p, v = nbp.universes.colliding_discs(20000, 3)
+    pin = lambda: torch.empty((20000, 2), dtype=torch.float64, pin_memory=True).numpy()
+    with nbp.NbContext(nbp.SimConfig(mode=nbp.NB_MODE_SPLIT), m, p, v) as ctx:
+        outs = []
+        for k in range(3):
+            ctx.upload(m, p, v)
+            ctx.step(k + 1, sync=False)
+            po, vo = pin(), pin()
+            ctx.download_async(po, vo)
+            outs.append((po, vo))
+        ctx.download_wait()
+        ps, vs = ctx.download()
+    with nbp.NbContext(nbp.SimConfig(mode=nbp.NB_MODE_SPLIT), m, p, v) as ref:
+        for k in range(3):
+            ref.upload(m, p, v)
+            ref.step(k + 1)
+            pr, vr = ref.download()
+            assert np.array_equal(outs[k][0], pr) and np.array_equal(outs[k][1], vr)
+    assert np.array_equal(ps, outs[2][0]) and np.array_equal(vs, outs[2][1])
