@@ -108,6 +108,14 @@ NB_API int nb_params_default(nb_params* p);
 NB_API int nb_create(const nb_params* p, uint64_t n, const double* mass, const double* pos_xy,
               const double* vel_xy, nb_ctx** out);
 
+/* Failure-detection check (no counterpart in the reference, which has no
+ * device-side waits): runs one radix-sort pass whose look-back waits on a
+ * tile that never publishes.  The wait is bounded (about a second), so the
+ * kernel gives up, raises its timeout flag and returns; the call then
+ * returns NB_ERR_TIMEOUT, and the device stays usable.  NB_OK would mean the
+ * bound did not trigger.  For tests. */
+NB_API int nb_debug_wait_timeout(int32_t device);
+
 /* Asynchronous form of nb_download: enqueues the same copy after the steps
  * enqueued so far and returns at once.  The device-to-host copy runs on the
  * context's copy stream, so it overlaps whatever is enqueued next (an

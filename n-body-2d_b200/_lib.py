@@ -38,6 +38,7 @@ EXPORTS = (
     "nb_allpairs_accelerations", "nb_phase_times", "nb_phase_name", "nb_morton_sort_static",
     "nb_set_mlp_weights", "nb_mlp_samples", "nb_mlp_forward", "nb_mlp_loss_grad", "nb_mlp_train",
     "nb_batch_create", "nb_autotune", "nb_render", "nb_download_async", "nb_download_wait",
+    "nb_debug_wait_timeout",
 )
 
 
@@ -134,6 +135,7 @@ def load() -> C.CDLL:
     lib.nb_render.argtypes = [_P, C.POINTER(NbView), _P]
     lib.nb_download_async.argtypes = [_P, _P, _P]
     lib.nb_download_wait.argtypes = [_P]
+    lib.nb_debug_wait_timeout.argtypes = [C.c_int32]
     lib.nb_set_mlp_weights.argtypes = [_P, _P]
     lib.nb_mlp_samples.argtypes = [_P, C.c_uint64, C.c_uint64, C.c_uint64, _P, _P, _P]
     lib.nb_mlp_forward.argtypes = [C.c_int32, _P, C.c_uint64, _P, _P]

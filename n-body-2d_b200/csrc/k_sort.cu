@@ -657,6 +657,47 @@ void launch_morton(nb_ctx* c, const double2* pos) {
                                                                c->sort.val[0]);
 }
 
+// One radix pass over two tiles of keys in which only the second tile runs:
+// its look-back waits on a predecessor that never publishes, so the bounded
+// wait must give up and raise kErrTimeout.  Returns the error bits.
+unsigned sort_timeout_probe(cudaStream_t st) {
+    constexpr int n = 2 * kSortTile;
+    uint64_t *key_in = nullptr, *key_out = nullptr;
+    uint32_t *val_in = nullptr, *val_out = nullptr, *hist = nullptr, *status = nullptr;
+    unsigned *counter = nullptr, *err = nullptr;
+    unsigned flags = ~0u;
+    if (cudaMalloc(&key_in, n * sizeof(uint64_t)) == cudaSuccess &&
+        cudaMalloc(&key_out, n * sizeof(uint64_t)) == cudaSuccess &&
+        cudaMalloc(&val_in, n * sizeof(uint32_t)) == cudaSuccess &&
+        cudaMalloc(&val_out, n * sizeof(uint32_t)) == cudaSuccess &&
+        cudaMalloc(&hist, 256 * sizeof(uint32_t)) == cudaSuccess &&
+        cudaMalloc(&status, 2 * 256 * sizeof(uint32_t)) == cudaSuccess &&
+        cudaMalloc(&counter, sizeof(unsigned)) == cudaSuccess &&
+        cudaMalloc(&err, sizeof(unsigned)) == cudaSuccess) {
+        // all keys zero: digit 0 holds every key, bins are all 0
+        cudaMemsetAsync(key_in, 0, n * sizeof(uint64_t), st);
+        cudaMemsetAsync(val_in, 0, n * sizeof(uint32_t), st);
+        cudaMemsetAsync(hist, 0, 256 * sizeof(uint32_t), st);
+        cudaMemsetAsync(status, 0, 2 * 256 * sizeof(uint32_t), st);
+        cudaMemsetAsync(err, 0, sizeof(unsigned), st);
+        const unsigned one = 1u;  // the single block takes tile 1
+        cudaMemcpyAsync(counter, &one, sizeof(unsigned), cudaMemcpyHostToDevice, st);
+        onesweep_pass<<<1, kSortThreads, 0, st>>>(key_in, val_in, key_out, val_out, n, 0, hist, status,
+                                                  counter, err);
+        cudaMemcpyAsync(&flags, err, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
+        if (cudaStreamSynchronize(st) != cudaSuccess) flags = ~0u;
+    }
+    cudaFree(key_in);
+    cudaFree(key_out);
+    cudaFree(val_in);
+    cudaFree(val_out);
+    cudaFree(hist);
+    cudaFree(status);
+    cudaFree(counter);
+    cudaFree(err);
+    return flags;
+}
+
 void launch_sort(nb_ctx* c) {
     const int tiles = c->sort.tiles;
     c->launches += 2 + 8;

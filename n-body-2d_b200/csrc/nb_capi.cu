@@ -512,6 +512,19 @@ int nb_sync(nb_ctx* c) {
     return read_device_error(c);
 }
 
+int nb_debug_wait_timeout(int32_t device) {
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev)
+        return NB_ERR_NOTFOUND;
+    DeviceGuard guard(device);
+    cudaStream_t st = nullptr;
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return NB_ERR_CUDA;
+    const unsigned flags = nb::sort_timeout_probe(st);
+    cudaStreamDestroy(st);
+    if (flags == ~0u) return NB_ERR_CUDA;
+    return (flags & nb::kErrTimeout) ? NB_ERR_TIMEOUT : NB_OK;
+}
+
 int nb_download_async(nb_ctx* c, double* pos_xy, double* vel_xy) {
     if (!c) return NB_ERR_INVALID;
     if (!pos_xy && !vel_xy) return NB_OK;

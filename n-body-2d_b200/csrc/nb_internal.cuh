@@ -199,7 +199,8 @@ __device__ __forceinline__ double cell_width2(const DeviceScalars* s, const Batc
 void launch_bbox(nb_ctx* c, const double2* pos);
 void launch_morton(nb_ctx* c, const double2* pos);
 void launch_batch_roots(nb_ctx* c);   // per-universe root cells after the tree build
-void launch_sort(nb_ctx* c);                                   // result in key[0]/val[0]
+void launch_sort(nb_ctx* c);
+unsigned sort_timeout_probe(cudaStream_t st);                                   // result in key[0]/val[0]
 void launch_gather(nb_ctx* c, const BodyBuffers& src, const BodyBuffers& dst, float4* body4);
 void launch_tree(nb_ctx* c, const BodyBuffers& b);
 void launch_moments(nb_ctx* c, const BodyBuffers& b, bool split);

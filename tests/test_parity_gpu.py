@@ -235,3 +235,19 @@ def test_download_async_matches_download(nbp):
             pr, vr = ref.download()
             assert np.array_equal(outs[k][0], pr) and np.array_equal(outs[k][1], vr)
     assert np.array_equal(ps, outs[2][0]) and np.array_equal(vs, outs[2][1])
+
+
+def test_bounded_wait_times_out_without_hanging(nbp):
+    """The radix sort's look-back waits on a predecessor tile; with one that
+    never publishes, the wait gives up after its iteration bound, the kernel
+    raises the timeout flag and returns, and the GPU stays usable."""
+    import time
+
+    lib = nbp.load()
+    t0 = time.perf_counter()
+    assert lib.nb_debug_wait_timeout(0) == 4  # NB_ERR_TIMEOUT
+    assert time.perf_counter() - t0 < 60
+    m, p, v = nbp.universes.exponential_disc(1000, 2)
+    with nbp.NbContext(nbp.SimConfig(mode=nbp.NB_MODE_SPLIT), m, p, v) as ctx:
+        ctx.step(2)
+        assert np.isfinite(ctx.download()[0]).all()
