@@ -878,17 +878,18 @@ void mlp_prepare_inference(nb_ctx* c) {
 void launch_mlp_correct(nb_ctx* c, const BodyBuffers& b, bool kick, bool store_acc) {
     c->launches += 1;
     const int smem = (int)sizeof(CorrSmem);
-    static int grid_per_sm = 0;
-    if (grid_per_sm == 0) {
+    // per context, so per device: the shared-memory attribute is a property
+    // of the kernel on the current device
+    if (c->corr_blocks_per_sm == 0) {
         cudaFuncSetAttribute(mlp_correct_kick, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         int blocks = 0;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, mlp_correct_kick,
                                                           kCorrWarps * 32, smem) != cudaSuccess ||
             blocks < 1)
             blocks = 2;
-        grid_per_sm = blocks;
+        c->corr_blocks_per_sm = blocks;
     }
-    mlp_correct_kick<<<c->sm_count * grid_per_sm, kCorrWarps * 32, smem, c->stream>>>(
+    mlp_correct_kick<<<c->sm_count * c->corr_blocks_per_sm, kCorrWarps * 32, smem, c->stream>>>(
         static_cast<const InferW*>(c->mlp_infer), c->tree, c->scal, b.pos, b.vel, c->acc32,
         store_acc ? c->acc : nullptr, (int)c->n, (float)c->p.epsilon_squared,
         c->p.G * c->p.timestep, c->p.timestep, kick ? 1 : 0);
@@ -912,11 +913,9 @@ int mlp_forward_device(const float* params, const float* X, int64_t n, float* Y,
 int mlp_grad_device(const float* params, const float* X, const float* Yt, const int64_t* idx,
                     int64_t n, float* grad, float* loss, int blocks, cudaStream_t st) {
     const int smem = (int)sizeof(TrainSmem);
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaFuncSetAttribute(mlp_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        attr_set = true;
-    }
+    // set on every call: the attribute belongs to the current device, and the
+    // library keeps no process-wide state
+    cudaFuncSetAttribute(mlp_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     mlp_grad_kernel<<<blocks, kWarps * 32, smem, st>>>(params, X, Yt, idx, n, 1.f / (float)n, grad,
                                                        loss);
     return cudaGetLastError() == cudaSuccess ? NB_OK : NB_ERR_CUDA;

@@ -156,6 +156,7 @@ struct nb_ctx {
     double* bbox_partials = nullptr;     // [blocks][4]
     int bbox_blocks = 0;
     int split_blocks[16] = {};            // persistent grids of the SPLIT traversal variants
+    int corr_blocks_per_sm = 0;          // learned correction kernel occupancy (0 = not set up)
     float* mlp_params = nullptr;         // learned mode: FP32 MLP parameters (device)
     void* mlp_infer = nullptr;           // learned mode: BF16 fragment images for inference
     double2* ap_partial = nullptr;       // NB_MODE_ALLPAIRS: per-source-chunk partial sums
