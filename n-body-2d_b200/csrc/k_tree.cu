@@ -532,6 +532,136 @@ __global__ void tree_moments(DeviceScalars* __restrict__ s, const double2* __res
     }
 }
 
+// ---- SPLIT monopole moments from prefix sums ----------------------------
+// A cell's bodies are one contiguous range of the sorted bodies, so its mass
+// and first moment are differences of prefix sums over the bodies: one scan
+// and one independent pass over the cells replace the bottom-up climb.  The
+// sums are taken relative to each body's frame centre in FP64, so the
+// cancellation in a difference stays far below the FP32 rounding of the cell
+// records.  The FP64 parity mode (the reference's summation order) and the
+// second and third moments (whose differences would cancel) keep the climb.
+__device__ __forceinline__ double4 d4_add(double4 a, double4 b) {
+    return make_double4(a.x + b.x, a.y + b.y, a.z + b.z, 0.0);
+}
+
+__device__ __forceinline__ double4 body_term(const double2* __restrict__ pos,
+                                             const double* __restrict__ mass,
+                                             const DeviceScalars* __restrict__ s, const Batch& bt,
+                                             int i) {
+    const double m = mass[i];
+    const double2 p = pos[i], c = frame_center(s, bt, i);
+    return make_double4(m, m * (p.x - c.x), m * (p.y - c.y), 0.0);
+}
+
+__device__ double4 block_sum_d4(double4 v, double4* red) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        v.x += __shfl_down_sync(kFull, v.x, o);
+        v.y += __shfl_down_sync(kFull, v.y, o);
+        v.z += __shfl_down_sync(kFull, v.z, o);
+    }
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    double4 tot = make_double4(0.0, 0.0, 0.0, 0.0);
+    if (threadIdx.x == 0)
+        for (int w = 0; w < kThreads / 32; ++w) tot = d4_add(tot, red[w]);
+    return tot;  // valid in thread 0
+}
+
+// Phase 1: per tile of kScanTile bodies, the total.
+__global__ void __launch_bounds__(kThreads)
+prefix_reduce(const double2* __restrict__ pos, const double* __restrict__ mass, int n,
+              const DeviceScalars* __restrict__ s, Batch bt, double4* __restrict__ tiles) {
+    __shared__ double4 red[kThreads / 32];
+    const int base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+    double4 v = make_double4(0.0, 0.0, 0.0, 0.0);
+    for (int k = 0; k < kScanItems; ++k)
+        if (base + k < n) v = d4_add(v, body_term(pos, mass, s, bt, base + k));
+    const double4 tot = block_sum_d4(v, red);
+    if (threadIdx.x == 0) tiles[blockIdx.x] = tot;
+}
+
+// Exclusive scan, in thread order, of one value per thread of the block.
+__device__ double4 block_exclusive_d4(double4 v, double4* part, double4& total) {
+    part[threadIdx.x] = v;
+    __syncthreads();
+    for (int o = 1; o < kThreads; o <<= 1) {
+        const double4 t = threadIdx.x >= o ? part[threadIdx.x - o] : make_double4(0.0, 0.0, 0.0, 0.0);
+        __syncthreads();
+        part[threadIdx.x] = d4_add(part[threadIdx.x], t);
+        __syncthreads();
+    }
+    total = part[kThreads - 1];
+    const double4 ex = threadIdx.x > 0 ? part[threadIdx.x - 1] : make_double4(0.0, 0.0, 0.0, 0.0);
+    __syncthreads();  // part[] is reused by the caller's next round
+    return ex;
+}
+
+// Phase 2: exclusive scan of the tile totals (one block, chunks of
+// kThreads * kScanItems tiles in order); tiles[ntiles] = the grand total.
+__global__ void __launch_bounds__(kThreads) prefix_tiles_scan(double4* __restrict__ tiles, int ntiles) {
+    __shared__ double4 part[kThreads];
+    double4 carry = make_double4(0.0, 0.0, 0.0, 0.0);
+    for (int c0 = 0; c0 < ntiles; c0 += kScanTile) {
+        const int base = c0 + threadIdx.x * kScanItems;
+        double4 v[kScanItems];
+        double4 run = make_double4(0.0, 0.0, 0.0, 0.0);
+        for (int k = 0; k < kScanItems; ++k) {
+            v[k] = base + k < ntiles ? tiles[base + k] : make_double4(0.0, 0.0, 0.0, 0.0);
+            run = d4_add(run, v[k]);
+        }
+        double4 total;
+        double4 acc = d4_add(carry, block_exclusive_d4(run, part, total));
+        for (int k = 0; k < kScanItems; ++k) {
+            if (base + k < ntiles) tiles[base + k] = acc;
+            acc = d4_add(acc, v[k]);
+        }
+        carry = d4_add(carry, total);
+    }
+    if (threadIdx.x == 0) tiles[ntiles] = carry;
+}
+
+// Phase 3: prefix[i] = sum over bodies before i; prefix[n] = the total.
+__global__ void __launch_bounds__(kThreads)
+prefix_apply(const double2* __restrict__ pos, const double* __restrict__ mass, int n,
+             const DeviceScalars* __restrict__ s, Batch bt, const double4* __restrict__ tiles,
+             int ntiles, double4* __restrict__ prefix) {
+    __shared__ double4 part[kThreads];
+    const int base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+    double4 v[kScanItems];
+    double4 run = make_double4(0.0, 0.0, 0.0, 0.0);
+    for (int k = 0; k < kScanItems; ++k) {
+        v[k] = base + k < n ? body_term(pos, mass, s, bt, base + k) : make_double4(0.0, 0.0, 0.0, 0.0);
+        run = d4_add(run, v[k]);
+    }
+    double4 total;
+    double4 acc = d4_add(tiles[blockIdx.x], block_exclusive_d4(run, part, total));
+    for (int k = 0; k < kScanItems; ++k) {
+        if (base + k < n) prefix[base + k] = acc;
+        acc = d4_add(acc, v[k]);
+    }
+    if (blockIdx.x == ntiles - 1 && threadIdx.x == 0) prefix[n] = tiles[ntiles];
+}
+
+// Phase 4: every cell from two prefix entries.
+__global__ void __launch_bounds__(kThreads)
+cells_from_prefix(const double4* __restrict__ prefix, Tree t, const DeviceScalars* __restrict__ s,
+                  Batch bt, const double2* __restrict__ pos, float accept_scale) {
+    const int id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= s->cells) return;
+    const int2 r = t.range[id];
+    const double4 a = prefix[r.x], b = prefix[r.y + 1];
+    const double M = b.x - a.x;
+    const double rx = (b.y - a.y) / M, ry = (b.z - a.z) / M;
+    const double2 fc = frame_center(s, bt, r.x);
+    const double2 com = make_double2(fc.x + rx, fc.y + ry);
+    t.mass[id] = M;
+    t.com[id] = com;
+    t.cell4[id] = make_float4((float)rx, (float)ry, (float)M,
+                              accept_size2(s, bt, pos, r.x, t.level[id], com, accept_scale));
+}
+
 // ---- SPLIT target groups -----------------------------------------------
 // A cell with more than gsize bodies hands its small children (cells or
 // leaves with <= gsize bodies) to groups: consecutive small children are
@@ -687,9 +817,18 @@ void launch_moments(nb_ctx* c, const BodyBuffers& b, bool split) {
     else if (second)
         tree_moments<true, true, false><<<blocks, kThreads, 0, c->stream>>>(
             c->scal, b.pos, b.mass, c->tree, c->batch, accept_scale);
-    else if (split)
-        tree_moments<true, false, false><<<blocks, kThreads, 0, c->stream>>>(
-            c->scal, b.pos, b.mass, c->tree, c->batch, accept_scale);
+    else if (split) {
+        const int n = (int)c->n;
+        const int tiles = (int)blocks_for(n, kScanTile);
+        c->launches += 3;
+        prefix_reduce<<<tiles, kThreads, 0, c->stream>>>(b.pos, b.mass, n, c->scal, c->batch,
+                                                         c->tree.prefix_tiles);
+        prefix_tiles_scan<<<1, kThreads, 0, c->stream>>>(c->tree.prefix_tiles, tiles);
+        prefix_apply<<<tiles, kThreads, 0, c->stream>>>(b.pos, b.mass, n, c->scal, c->batch,
+                                                        c->tree.prefix_tiles, tiles, c->tree.prefix);
+        cells_from_prefix<<<blocks, kThreads, 0, c->stream>>>(c->tree.prefix, c->tree, c->scal,
+                                                              c->batch, b.pos, accept_scale);
+    }
     else
         tree_moments<false, false, false><<<blocks, kThreads, 0, c->stream>>>(
             c->scal, b.pos, b.mass, c->tree, c->batch, 0.f);

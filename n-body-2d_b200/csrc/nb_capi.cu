@@ -95,6 +95,8 @@ int alloc_all(nb_ctx* c) {
         NB_CUDA(c, dalloc(&t.gcount, n));
         NB_CUDA(c, dalloc(&t.gbase, n));
         NB_CUDA(c, dalloc(&t.groups, n));
+        NB_CUDA(c, dalloc(&t.prefix, n + 1));
+        NB_CUDA(c, dalloc(&t.prefix_tiles, (n + 2047) / 2048 + 1));
     }
     if (c->p.flags & NB_FLAG_LEARNED) {
         NB_CUDA(c, dalloc(&t.t32, n));
@@ -145,7 +147,7 @@ void free_all(nb_ctx* c) {
                          t.start_of,  t.range,       t.s64,         t.cell4,      t.cellq,
                          t.body4,     t.gcount,      t.gbase,       t.groups,     t.rep_of,
                          t.t32,       t.cellh,       t.band,        t.band_count,
-                         t.start_list};
+                         t.start_list, t.prefix, t.prefix_tiles};
     for (void* q : tree_ptrs) cudaFree(q);
     cudaFree(c->scal);
     cudaFree(c->bbox_partials);

@@ -101,6 +101,11 @@ struct Tree {
     int32_t* band = nullptr;       // per group: band cells, kBandPerBody x first body onwards
     int32_t* band_count = nullptr; // per group: band cells found
     int32_t* start_list = nullptr; // cells without internal children, in any order
+    // SPLIT monopole moments: exclusive prefix sums over the sorted bodies of
+    // {m, m (x - frame centre), m (y - frame centre), 0}, n + 1 entries, and
+    // the per-tile totals of the scan that builds them
+    double4* prefix = nullptr;
+    double4* prefix_tiles = nullptr;
     // SPLIT target groups: <= split_group_size() Morton-consecutive bodies in one
     // parent cell (merged sibling cells/leaves), stored as body ranges
     int32_t* gcount = nullptr;   // groups each cell emits
