@@ -160,6 +160,7 @@ void free_all(nb_ctx* c) {
     cudaFree(c->render_table);
     cudaFree(c->acc32);
     cudaFree(c->mlp_params);
+    cudaFree(c->mlp_infer);
 }
 
 int alloc_batch(nb_ctx* c, uint32_t nuni, const uint64_t* counts) {
@@ -244,9 +245,20 @@ void enqueue_step(nb_ctx* c, int parity, bool integrate, bool store_acc, bool ti
     nb::launch_tree(c, B);
     nb::launch_batch_roots(c);
     mark(4);
+    // the target groups need only the tree: they are built on the side stream
+    // while the moments run (two branches of the captured graph)
+    if (split) {
+        cudaEventRecord(c->fork_ev, c->stream);
+        cudaStreamWaitEvent(c->side_stream, c->fork_ev, 0);
+        cudaStream_t main_stream = c->stream;
+        c->stream = c->side_stream;
+        nb::launch_groups(c);
+        c->stream = main_stream;
+        cudaEventRecord(c->join_ev, c->side_stream);
+    }
     nb::launch_moments(c, B, split);
     mark(5);
-    if (split) nb::launch_groups(c);
+    if (split) cudaStreamWaitEvent(c->stream, c->join_ev, 0);
     mark(6);
     if (split && (c->p.flags & NB_FLAG_LEARNED)) {
         nb::launch_force_split(c, B, integrate, store_acc);  // FP32 accelerations + band lists
@@ -386,6 +398,9 @@ int create_context(const nb_params* p, uint64_t n, const double* mass, const dou
         cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
         cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->side_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->fork_ev, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->join_ev, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&c->staged, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&c->copied, cudaEventDisableTiming) != cudaSuccess) {
         rc = NB_ERR_CUDA;
@@ -430,6 +445,7 @@ int nb_destroy(nb_ctx* c) {
     DeviceGuard guard(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
+    if (c->side_stream) cudaStreamSynchronize(c->side_stream);
     drop_graphs(c);
     free_all(c);
     free_batch(c);
@@ -438,6 +454,9 @@ int nb_destroy(nb_ctx* c) {
     if (c->staged) cudaEventDestroy(c->staged);
     if (c->copied) cudaEventDestroy(c->copied);
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
+    if (c->fork_ev) cudaEventDestroy(c->fork_ev);
+    if (c->join_ev) cudaEventDestroy(c->join_ev);
+    if (c->side_stream) cudaStreamDestroy(c->side_stream);
     for (auto& e : c->phase_ev)
         if (e) cudaEventDestroy(e);
     if (c->stream) cudaStreamDestroy(c->stream);

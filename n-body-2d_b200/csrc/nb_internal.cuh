@@ -149,6 +149,8 @@ struct nb_ctx {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaStream_t copy_stream = nullptr;  // nb_download_async: device-to-host copies
+    cudaStream_t side_stream = nullptr;  // the target groups, built while the moments run
+    cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
     cudaEvent_t staged = nullptr;        // the download's scatter into the staging buffers is done
     cudaEvent_t copied = nullptr;        // the staging buffers have been copied out (free again)
     cudaEvent_t phase_ev[nb::kPhases + 1] = {};
