@@ -307,7 +307,7 @@ __global__ void tree_trivial_root(const double2* __restrict__ pos, const double*
 // Moments of one cell from its children, in quadrant order, with the
 // reference's arithmetic (CU:329-343): M += m; R = fma(m, com, R); com = R / M.
 // kSplit packs the FP32 records the group traversal reads.  kSecond (the
-// quadrupole walk and the learned features) also accumulates second moments
+// quadrupole walk) also accumulates second moments
 // about the COM by the parallel-axis rule, S = sum_c [S_c + m_c d_c d_c^T]
 // with d_c = com_c - com, in FP64.  Leaves have S = 0 (a multi-body leaf
 // spans less than width / 2^30, so its own S is negligible).
@@ -370,7 +370,7 @@ __device__ __forceinline__ uint32_t bf16_pair(float lo, float hi) {
     return *reinterpret_cast<const uint32_t*>(&v);
 }
 
-template <bool kSplit, bool kSecond, bool kFeat>
+template <bool kSplit, bool kSecond>
 __device__ __forceinline__ void cell_moments(int id, const DeviceScalars* __restrict__ s,
                                              const double2* __restrict__ pos,
                                              const double* __restrict__ mass, const Tree& t,
@@ -415,7 +415,7 @@ __device__ __forceinline__ void cell_moments(int id, const DeviceScalars* __rest
         t.cell4[id] = make_float4((float)(com.x - fc.x), (float)(com.y - fc.y), (float)M,
                                   accept_size2(s, bt, pos, first, t.level[id], com, accept_scale));
     }
-    if (kSplit && kSecond && !kFeat) {
+    if (kSplit && kSecond) {
         double sxx = 0.0, sxy = 0.0, syy = 0.0;
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
@@ -442,53 +442,6 @@ __device__ __forceinline__ void cell_moments(int id, const DeviceScalars* __rest
                                   accept_size2(s, bt, pos, first, t.level[id], com, accept_scale));
         t.cellq[id] = make_float4((float)sxx, (float)sxy, (float)syy, 0.f);
     }
-    if (kSplit && kFeat) {
-        // The learned features: second and third moments about the COM by the
-        // parallel-axis shift, in FP32 (they only feed BF16 features):
-        //   S += S_c + m d d^T
-        //   T += T_c + (d_i S_c,jk + d_j S_c,ik + d_k S_c,ij) + m d_i d_j d_k
-        float sxx = 0.f, sxy = 0.f, syy = 0.f;
-        float txxx = 0.f, txxy = 0.f, txyy = 0.f, tyyy = 0.f;
-        double mmax = 0.0;
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int r = refs[q];
-            if (r == INT_MIN) continue;
-            const float m = (float)cm[q];
-            mmax = fmax(mmax, cm[q]);
-            const float dx = (float)(cmx[q] - com.x), dy = (float)(cmy[q] - com.y);
-            float4 cs = make_float4(0.f, 0.f, 0.f, 0.f), ct = cs;
-            if (r >= 0) {
-                cs = __ldcg(t.cellq + r);
-                ct = __ldcg(t.t32 + r);
-            }
-            txxx += ct.x + 3.f * dx * cs.x + m * dx * dx * dx;
-            txxy += ct.y + 2.f * dx * cs.y + dy * cs.x + m * dx * dx * dy;
-            txyy += ct.z + dx * cs.z + 2.f * dy * cs.y + m * dx * dy * dy;
-            tyyy += ct.w + 3.f * dy * cs.z + m * dy * dy * dy;
-            sxx += cs.x + m * dx * dx;
-            sxy += cs.y + m * dx * dy;
-            syy += cs.z + m * dy * dy;
-        }
-        __stcg(t.cellq + id, make_float4(sxx, sxy, syy, 0.f));
-        __stcg(t.t32 + id, make_float4(txxx, txxy, txyy, tyyy));
-        // the MLP's cell features, normalised by M and the cell width; the
-        // network reads them as BF16, so they are stored rounded
-        const int first = t.range[id].x;
-        const double w2 = cell_width2(s, bt, first, t.level[id]), w = sqrt(w2);
-        const float im2 = (float)(1.0 / (M * w2)), im3 = (float)(1.0 / (M * w2 * w));
-        const double2 fc = frame_center(s, bt, first);
-        const float4 c4 = make_float4((float)(com.x - fc.x), (float)(com.y - fc.y), (float)M,
-                                      accept_size2(s, bt, pos, first, t.level[id], com,
-                                                   accept_scale));
-        t.cell4[id] = c4;
-        t.cellh[2 * id] = make_uint4(bf16_pair((float)(mmax / M), sxx * im2),
-                                     bf16_pair(sxy * im2, syy * im2),
-                                     bf16_pair(txxx * im3, txxy * im3),
-                                     bf16_pair(txyy * im3, tyyy * im3));
-        t.cellh[2 * id + 1] = make_uint4(__float_as_uint(c4.x), __float_as_uint(c4.y),
-                                         __float_as_uint(c4.z), __float_as_uint((float)w));
-    }
 }
 
 // Arrival at a parent: release publishes this cell's moments, acquire makes
@@ -504,7 +457,7 @@ __device__ __forceinline__ int arrive_acq_rel(int* counter) {
 
 // Bottom-up pass: threads start at cells without internal children and
 // climb; the last child to arrive at a parent (atomic counter) computes it.
-template <bool kSplit, bool kSecond, bool kFeat>
+template <bool kSplit, bool kSecond>
 __global__ void tree_moments(DeviceScalars* __restrict__ s, const double2* __restrict__ pos,
                              const double* __restrict__ mass, Tree t, Batch bt,
                              float accept_scale) {
@@ -519,7 +472,7 @@ __global__ void tree_moments(DeviceScalars* __restrict__ s, const double2* __res
             atomicOr(&s->error, kErrTree);
             return;
         }
-        cell_moments<kSplit, kSecond, kFeat>(id, s, pos, mass, t, bt, accept_scale);
+        cell_moments<kSplit, kSecond>(id, s, pos, mass, t, bt, accept_scale);
         const int par = t.parent[id];
         if (par < 0) return;
         if (par >= cells) {
@@ -660,6 +613,125 @@ cells_from_prefix(const double4* __restrict__ prefix, Tree t, const DeviceScalar
     t.com[id] = com;
     t.cell4[id] = make_float4((float)rx, (float)ry, (float)M,
                               accept_size2(s, bt, pos, r.x, t.level[id], com, accept_scale));
+}
+
+// ---- learned features: second and third moments -------------------------
+// The features need S and T about each cell's centre of mass, which the
+// prefix pass has already written.  A cell with fewer than kDirectCell
+// bodies, or with only leaf children, sums them directly over its bodies;
+// a larger cell combines its children by the parallel-axis shift
+//   S = sum_c [S_c + m_c d d^T]
+//   T = sum_c [T_c + (d_i S_c,jk + d_j S_c,ik + d_k S_c,ij) + m_c d_i d_j d_k],
+// bottom-up: a directly summed cell under a larger parent arrives at the
+// parent's counter, and the last child to arrive computes the parent and
+// climbs on.  Only the few cells above the direct size climb.  FP32: the
+// moments only feed BF16 features.
+constexpr int kDirectCell = 32;
+
+__device__ __forceinline__ bool direct_cell(const Tree& t, int id) {
+    const int2 r = t.range[id];
+    return r.y - r.x < kDirectCell || t.nint[id] == 0;
+}
+
+__device__ __forceinline__ double child_mass(const Tree& t, const double* __restrict__ mass,
+                                             int r) {
+    if (r >= 0) return t.mass[r];
+    const int b = ~r;
+    return t.leaf_last[b] == b ? mass[b] : t.bucket_mass[b];
+}
+
+// The cell's feature record (the BF16 features, then COM, mass and width)
+// and its S and T for the parent's shift.
+__device__ void write_features(const Tree& t, const DeviceScalars* __restrict__ s,
+                               const Batch& bt, const double* __restrict__ mass, int id,
+                               const float* S, const float* T) {
+    const int4 ch = t.child[id];
+    const int refs[4] = {ch.x, ch.y, ch.z, ch.w};
+    double mmax = 0.0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+        if (refs[q] != INT_MIN) mmax = fmax(mmax, child_mass(t, mass, refs[q]));
+    const double M = t.mass[id];
+    const int first = t.range[id].x;
+    const double w2 = cell_width2(s, bt, first, t.level[id]), w = sqrt(w2);
+    const float im2 = (float)(1.0 / (M * w2)), im3 = (float)(1.0 / (M * w2 * w));
+    __stcg(t.cellq + id, make_float4(S[0], S[1], S[2], 0.f));
+    __stcg(t.t32 + id, make_float4(T[0], T[1], T[2], T[3]));
+    const float4 c4 = t.cell4[id];
+    t.cellh[2 * id] = make_uint4(bf16_pair((float)(mmax / M), S[0] * im2),
+                                 bf16_pair(S[1] * im2, S[2] * im2),
+                                 bf16_pair(T[0] * im3, T[1] * im3),
+                                 bf16_pair(T[2] * im3, T[3] * im3));
+    t.cellh[2 * id + 1] = make_uint4(__float_as_uint(c4.x), __float_as_uint(c4.y),
+                                     __float_as_uint(c4.z), __float_as_uint((float)w));
+}
+
+// One mass point (or a child's moments) at offset (dx, dy) from the COM.
+__device__ __forceinline__ void add_shifted(float m, float dx, float dy, const float4 cs,
+                                            const float4 ct, float* S, float* T) {
+    T[0] += ct.x + 3.f * dx * cs.x + m * dx * dx * dx;
+    T[1] += ct.y + 2.f * dx * cs.y + dy * cs.x + m * dx * dx * dy;
+    T[2] += ct.z + dx * cs.z + 2.f * dy * cs.y + m * dx * dy * dy;
+    T[3] += ct.w + 3.f * dy * cs.z + m * dy * dy * dy;
+    S[0] += cs.x + m * dx * dx;
+    S[1] += cs.y + m * dx * dy;
+    S[2] += cs.z + m * dy * dy;
+}
+
+__global__ void __launch_bounds__(kThreads)
+learned_features(DeviceScalars* __restrict__ s, const double2* __restrict__ pos,
+                 const double* __restrict__ mass, Tree t, Batch bt) {
+    int id = blockIdx.x * blockDim.x + threadIdx.x;
+    const int cells = s->cells;
+    if (id >= cells || !direct_cell(t, id)) return;
+    const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+    {
+        const double2 com = t.com[id];
+        const int2 r = t.range[id];
+        float S[3] = {0.f, 0.f, 0.f}, T[4] = {0.f, 0.f, 0.f, 0.f};
+        for (int j = r.x; j <= r.y; ++j) {
+            const double2 p = pos[j];
+            add_shifted((float)mass[j], (float)(p.x - com.x), (float)(p.y - com.y), zero, zero, S,
+                        T);
+        }
+        write_features(t, s, bt, mass, id, S, T);
+    }
+    // A path to the root crosses at most 30 cells; the bound only guards
+    // against a malformed tree.
+    for (int hop = 0;; ++hop) {
+        const int par = t.parent[id];
+        if (par < 0) return;
+        if (par >= cells || hop > kMaxLevel + 1) {
+            atomicOr(&s->error, kErrTree);
+            return;
+        }
+        if (direct_cell(t, par)) return;  // its own thread sums it
+        const int arrived = arrive_acq_rel(t.ready + par);
+        if (arrived != t.nint[par] - 1) return;
+        id = par;
+        const double2 com = t.com[id];
+        const int4 ch = t.child[id];
+        const int refs[4] = {ch.x, ch.y, ch.z, ch.w};
+        float S[3] = {0.f, 0.f, 0.f}, T[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int r = refs[q];
+            if (r == INT_MIN) continue;
+            double2 cc;
+            float4 cs = zero, ct = zero;
+            if (r >= 0) {
+                cc = t.com[r];
+                cs = __ldcg(t.cellq + r);
+                ct = __ldcg(t.t32 + r);
+            } else {
+                const int b = ~r;
+                cc = t.leaf_last[b] == b ? pos[b] : t.bucket_com[b];
+            }
+            add_shifted((float)child_mass(t, mass, r), (float)(cc.x - com.x), (float)(cc.y - com.y),
+                        cs, ct, S, T);
+        }
+        write_features(t, s, bt, mass, id, S, T);
+    }
 }
 
 // ---- SPLIT target groups -----------------------------------------------
@@ -809,18 +881,16 @@ void launch_moments(nb_ctx* c, const BodyBuffers& b, bool split) {
     const double ratio = c->p.bmax_ratio;
     const float accept_scale =
         split && ratio > 0.0 ? (float)(c->p.theta * c->p.theta / (ratio * ratio)) : 0.f;
-    c->launches += 1;
     const unsigned blocks = blocks_for(cap, kThreads);
-    if (feat)
-        tree_moments<true, true, true><<<blocks, kThreads, 0, c->stream>>>(
-            c->scal, b.pos, b.mass, c->tree, c->batch, accept_scale);
-    else if (second)
-        tree_moments<true, true, false><<<blocks, kThreads, 0, c->stream>>>(
-            c->scal, b.pos, b.mass, c->tree, c->batch, accept_scale);
-    else if (split) {
+    if (second) {
+        c->launches += 1;
+        tree_moments<true, true><<<blocks, kThreads, 0, c->stream>>>(c->scal, b.pos, b.mass, c->tree,
+                                                                     c->batch, accept_scale);
+    } else if (split) {
+        // monopoles from the prefix sums, then (learned) the features
         const int n = (int)c->n;
         const int tiles = (int)blocks_for(n, kScanTile);
-        c->launches += 3;
+        c->launches += 4;
         prefix_reduce<<<tiles, kThreads, 0, c->stream>>>(b.pos, b.mass, n, c->scal, c->batch,
                                                          c->tree.prefix_tiles);
         prefix_tiles_scan<<<1, kThreads, 0, c->stream>>>(c->tree.prefix_tiles, tiles);
@@ -828,10 +898,16 @@ void launch_moments(nb_ctx* c, const BodyBuffers& b, bool split) {
                                                         c->tree.prefix_tiles, tiles, c->tree.prefix);
         cells_from_prefix<<<blocks, kThreads, 0, c->stream>>>(c->tree.prefix, c->tree, c->scal,
                                                               c->batch, b.pos, accept_scale);
+        if (feat) {
+            c->launches += 1;
+            learned_features<<<blocks, kThreads, 0, c->stream>>>(c->scal, b.pos, b.mass, c->tree,
+                                                                 c->batch);
+        }
+    } else {
+        c->launches += 1;
+        tree_moments<false, false><<<blocks, kThreads, 0, c->stream>>>(c->scal, b.pos, b.mass,
+                                                                       c->tree, c->batch, 0.f);
     }
-    else
-        tree_moments<false, false, false><<<blocks, kThreads, 0, c->stream>>>(
-            c->scal, b.pos, b.mass, c->tree, c->batch, 0.f);
 }
 
 }  // namespace nb
