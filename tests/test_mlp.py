@@ -105,3 +105,24 @@ def test_learned_correction_beats_the_monopole_at_theta_one(nbp):
     # removes only part of the monopole error (about 10% at p50 and p99 here)
     assert e_learned[0] < 0.95 * e_mono[0], (e_learned, e_mono)
     assert e_learned[1] < 0.95 * e_mono[1], (e_learned, e_mono)
+
+
+@pytest.mark.gpu
+def test_shipped_weights_run_with_zero_softening(nbp):
+    """The committed correction on an eps^2 = 0 context: the eps^2 = 0 walk
+    variant with band lists, then the correction, stays finite."""
+    import json
+    import pathlib
+
+    wdir = pathlib.Path(nbp.__file__).resolve().parent / "weights"
+    params = np.load(wdir / "correction_theta1.npy")
+    bmax = json.loads((wdir / "correction_theta1.json").read_text())["bmax_ratio"]
+    m, p, v = nbp.universes.colliding_discs(32768, 6)
+    cfg = nbp.SimConfig(theta=1.0, epsilon_squared=0.0, mode=nbp.NB_MODE_SPLIT, learned=True,
+                        bmax_ratio=bmax)
+    with nbp.NbContext(cfg, m, p, v) as ctx:
+        ctx.set_mlp_weights(params)
+        a = ctx.accelerations()
+        ctx.step(2)
+        pos, _ = ctx.download()
+    assert np.isfinite(a).all() and np.isfinite(pos).all()

@@ -251,3 +251,13 @@ def test_bounded_wait_times_out_without_hanging(nbp):
     with nbp.NbContext(nbp.SimConfig(mode=nbp.NB_MODE_SPLIT), m, p, v) as ctx:
         ctx.step(2)
         assert np.isfinite(ctx.download()[0]).all()
+
+
+def test_fp64_mode_ignores_the_bmax_ratio(nbp):
+    m, p, v = nbp.universes.exponential_disc(3000, 4)
+    out = []
+    for ratio in (0.0, 0.75):
+        cfg = nbp.SimConfig(mode=nbp.NB_MODE_FP64, theta=0.8, bmax_ratio=ratio)
+        with nbp.NbContext(cfg, m, p, v) as ctx:
+            out.append(ctx.accelerations())
+    assert np.array_equal(out[0], out[1])

@@ -73,3 +73,16 @@ def test_allpairs_backend_step_is_drift_then_kick(nbp, orc, cpu_law):
     v_ref = v + acc * G * dt
     assert np.array_equal(p1, p_ref)
     assert np.abs(v1 - v_ref).max() <= 1e-12 * np.abs(v_ref).max()
+
+
+def test_allpairs_single_body_and_pair(nbp):
+    cfg = nbp.SimConfig(mode=nbp.NB_MODE_ALLPAIRS, epsilon_squared=1e-4)
+    with nbp.NbContext(cfg, np.ones(1), np.zeros((1, 2)), np.zeros((1, 2))) as ctx:
+        assert np.array_equal(ctx.accelerations(), np.zeros((1, 2)))
+    m = np.array([1.0, 3.0])
+    p = np.array([[0.0, 0.0], [2.0, 0.0]])
+    with nbp.NbContext(cfg, m, p, np.zeros((2, 2))) as ctx:
+        a = ctx.accelerations()
+    r3 = (4.0 + 1e-4) ** 1.5
+    assert a[0, 0] == pytest.approx(3.0 * 2.0 / r3, rel=1e-14)
+    assert a[1, 0] == pytest.approx(-1.0 * 2.0 / r3, rel=1e-14)
