@@ -167,6 +167,24 @@ def _dist():
     return world, rank, local
 
 
+E2E_HOW = ("per step: nb_upload_async of mass/pos/vel from pinned memory (upload stream), nb_step, "
+           "nb_download_async of pos/vel (copy stream); the copies overlap the neighbouring steps; "
+           "wall clock over the steps, one untimed round first")
+
+
+def e2e_loop(ctx, hm, hp, hv, op, ov, steps: int) -> None:
+    """steps x (upload, step, download) through the C ABI with pinned host
+    buffers.  Step k's upload runs on the upload stream while step k-1
+    computes, and its download on the copy stream while step k+1 computes;
+    the results alternate between two host buffers."""
+    for k in range(steps):
+        ctx.upload_async(hm, hp, hv)
+        ctx.step(1, sync=False)
+        ctx.download_async(op[k & 1], ov[k & 1])
+    ctx.download_wait()
+    ctx.sync()
+
+
 def max_over_ranks(value: float) -> float:
     """Largest value over the ranks of the default process group (the job's
     time is its slowest replica's); the value itself without one."""
@@ -387,17 +405,13 @@ def run_ours(args) -> None:
     pin = lambda shape: torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy()
     hm, hp, hv = pin((args.n,)), pin((args.n, 2)), pin((args.n, 2))
     hm[:], hp[:], hv[:] = m, p, v
-    # double-buffered results: each step's download runs on the copy stream
-    # while the next step's upload and step are enqueued
+    # double-buffered results; uploads and downloads overlap the steps (e2e_loop)
     op, ov = [pin((args.n, 2)) for _ in range(2)], [pin((args.n, 2)) for _ in range(2)]
-    e2e_steps = max(1, min(args.steps, 5))
+    e2e_steps = max(1, min(args.steps, 10))
+    e2e_loop(ctx, hm, hp, hv, op, ov, 1)  # untimed: sets up the upload staging area
     barrier()
     t0 = time.perf_counter()
-    for k in range(e2e_steps):
-        ctx.upload(hm, hp, hv)
-        ctx.step(1, sync=False)
-        ctx.download_async(op[k & 1], ov[k & 1])
-    ctx.download_wait()
+    e2e_loop(ctx, hm, hp, hv, op, ov, e2e_steps)
     e2e_t = max_over_ranks((time.perf_counter() - t0) / e2e_steps)
 
     accuracy = None
@@ -454,8 +468,7 @@ def run_ours(args) -> None:
         "e2e": {"value": world * args.n / e2e_t, "unit": "body-steps/s",
                 "h2d_bytes_per_step": 40 * args.n, "d2h_bytes_per_step": 32 * args.n,
                 "steps": e2e_steps,
-                "how": "per step: nb_upload of mass/pos/vel from pinned memory, nb_step, "
-                       "nb_download_async of pos/vel (overlaps the next upload); wall clock"},
+                "how": E2E_HOW},
         "gpu_launches": int(st.kernels_per_step) * args.steps,
         "clocks": clk,
         "accuracy": accuracy,
@@ -527,14 +540,11 @@ def run_ensemble(args) -> None:
     hm, hp, hv = pin((n,)), pin((n, 2)), pin((n, 2))
     hm[:], hp[:], hv[:] = m, p, v
     op, ov = [pin((n, 2)) for _ in range(2)], [pin((n, 2)) for _ in range(2)]
-    e2e_steps = max(1, min(args.steps, 5))
+    e2e_steps = max(1, min(args.steps, 10))
+    e2e_loop(ctx, hm, hp, hv, op, ov, 1)  # untimed: sets up the upload staging area
     barrier()
     t0 = time.perf_counter()
-    for k in range(e2e_steps):
-        ctx.upload(hm, hp, hv)
-        ctx.step(1, sync=False)
-        ctx.download_async(op[k & 1], ov[k & 1])
-    ctx.download_wait()
+    e2e_loop(ctx, hm, hp, hv, op, ov, e2e_steps)
     e2e_t = max_over_ranks((time.perf_counter() - t0) / e2e_steps)
 
     accuracy = None
@@ -605,7 +615,8 @@ def run_ensemble(args) -> None:
                      "flops_per_interaction": FLOPS_PER_INTERACTION},
         "phases_ms": {k: round(v, 4) for k, v in phases.items()},
         "e2e": {"value": world * n / e2e_t, "unit": "body-steps/s",
-                "h2d_bytes_per_step": 40 * n, "d2h_bytes_per_step": 32 * n, "steps": e2e_steps},
+                "h2d_bytes_per_step": 40 * n, "d2h_bytes_per_step": 32 * n, "steps": e2e_steps,
+                "how": E2E_HOW},
         "gpu_launches": int(st.kernels_per_step) * args.steps,
         "clocks": clk, "accuracy": accuracy, "looped_single_universe": looped,
     }

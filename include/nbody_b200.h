@@ -186,6 +186,20 @@ NB_API int nb_set_timestep(nb_ctx* ctx, double dt);
  * half of init_device_resources, BarnesHutCuda.cu:596-605). */
 NB_API int nb_upload(nb_ctx* ctx, const double* mass, const double* pos_xy, const double* vel_xy);
 
+/* Asynchronous form of nb_upload: enqueues the host-to-device copy into a
+ * device staging area on the context's upload stream and returns at once,
+ * so the copy overlaps the steps and downloads enqueued before it.  Work
+ * enqueued before the call sees the old state, work enqueued after it the
+ * new one.  The bodies are checked on the device as they are moved into the
+ * state; a rejected set leaves the state unchanged and the next nb_sync or
+ * nb_download_wait returns NB_ERR_INVALID.  The staging area (40 bytes per
+ * body) is allocated by the first call.  mass / pos_xy / vel_xy must stay
+ * valid and unchanged, and be pinned for the copy to be asynchronous, until
+ * nb_sync returns.  No counterpart in the reference, which uploads once at
+ * start-up (BarnesHutCuda.cu:596-605). */
+NB_API int nb_upload_async(nb_ctx* ctx, const double* mass, const double* pos_xy,
+                           const double* vel_xy);
+
 /* Replaces sync_from_gpu_bodies (BarnesHutCuda.cu:632-646): scatters the
  * state back to original order and copies it to the host.  Either pointer
  * may be NULL.  Blocks until the copy is done. */

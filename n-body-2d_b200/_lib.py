@@ -38,7 +38,7 @@ EXPORTS = (
     "nb_allpairs_accelerations", "nb_phase_times", "nb_phase_name", "nb_morton_sort_static",
     "nb_set_mlp_weights", "nb_mlp_samples", "nb_mlp_forward", "nb_mlp_loss_grad", "nb_mlp_train",
     "nb_batch_create", "nb_autotune", "nb_render", "nb_download_async", "nb_download_wait",
-    "nb_debug_wait_timeout",
+    "nb_debug_wait_timeout", "nb_upload_async",
 )
 
 
@@ -118,6 +118,7 @@ def load() -> C.CDLL:
     lib.nb_sync.argtypes = [_P]
     lib.nb_set_timestep.argtypes = [_P, C.c_double]
     lib.nb_upload.argtypes = [_P, _P, _P, _P]
+    lib.nb_upload_async.argtypes = [_P, _P, _P, _P]
     lib.nb_download.argtypes = [_P, _P, _P]
     lib.nb_accelerations.argtypes = [_P, _P]
     lib.nb_debug_morton.argtypes = [_P, _P, _P, _P]

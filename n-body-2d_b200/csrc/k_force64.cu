@@ -167,13 +167,37 @@ __global__ void upload_kernel(int32_t* __restrict__ orig, const double* __restri
                               int64_t n, unsigned* __restrict__ bad) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
-    orig[i] = (int32_t)i;
+    if (orig) orig[i] = (int32_t)i;
     const double m = mass[i];
     const double2 p = pos[i], v = vel[i];
     unsigned f = 0;
     if (!(isfinite(m) && isfinite(p.x) && isfinite(p.y) && isfinite(v.x) && isfinite(v.y))) f |= 1u;
     if (!(m > 0.0)) f |= 2u;
     if (__any_sync(__activemask(), f != 0) && f) atomicOr(bad, f);
+}
+
+// Moves checked staged bodies into the state in original order.  After a
+// rejected check the state keeps its bodies: when they live in another
+// buffer (keep != dst) they are copied over, since the next step reads dst.
+__global__ void upload_commit(const double* __restrict__ sm, const double2* __restrict__ sp,
+                              const double2* __restrict__ sv, BodyBuffers keep, BodyBuffers dst,
+                              int64_t n, const unsigned* __restrict__ bad,
+                              unsigned* __restrict__ err) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (*bad) {
+        if (i == 0) atomicOr(err, kErrUpload);
+        if (keep.mass == dst.mass) return;
+        dst.orig[i] = keep.orig[i];
+        dst.mass[i] = keep.mass[i];
+        dst.pos[i] = keep.pos[i];
+        dst.vel[i] = keep.vel[i];
+        return;
+    }
+    dst.orig[i] = (int32_t)i;
+    dst.mass[i] = sm[i];
+    dst.pos[i] = sp[i];
+    dst.vel[i] = sv[i];
 }
 
 __global__ void identity_kernel(int32_t* orig, int64_t n) {
@@ -211,6 +235,15 @@ void launch_scatter(nb_ctx* c, const BodyBuffers& b, double2* out_pos, double2* 
 void launch_identity(nb_ctx* c, int32_t* orig) {
     c->launches += 1;
     identity_kernel<<<blocks_for(c->n, 256), 256, 0, c->stream>>>(orig, c->n);
+}
+
+void launch_upload_commit(nb_ctx* c, const double* m, const double2* p, const double2* v,
+                          const BodyBuffers& keep, const BodyBuffers& dst, unsigned* bad) {
+    c->launches += 2;
+    cudaMemsetAsync(bad, 0, sizeof(unsigned), c->stream);
+    upload_kernel<<<blocks_for(c->n, 256), 256, 0, c->stream>>>(nullptr, m, p, v, c->n, bad);
+    upload_commit<<<blocks_for(c->n, 256), 256, 0, c->stream>>>(m, p, v, keep, dst, c->n, bad,
+                                                                 &c->scal->error);
 }
 
 void launch_upload_check(nb_ctx* c, const BodyBuffers& b, unsigned* bad) {

@@ -154,6 +154,9 @@ void free_all(nb_ctx* c) {
     cudaFree(c->acc);
     cudaFree(c->stage_pos);
     cudaFree(c->stage_vel);
+    cudaFree(c->up_mass);
+    cudaFree(c->up_pos);
+    cudaFree(c->up_vel);
     cudaFree(c->ap_partial);
     cudaFree(c->render_count);
     cudaFree(c->render_rgba);
@@ -299,6 +302,9 @@ int read_device_error(nb_ctx* c) {
     NB_CUDA(c, cudaMemsetAsync(&c->scal->error, 0, sizeof(unsigned), c->stream));
     if (flags & nb::kErrTimeout) return fail(c, NB_ERR_TIMEOUT, "a bounded device wait gave up");
     if (flags & nb::kErrStack) return fail(c, NB_ERR_CAPACITY, "traversal stack bound exceeded");
+    if (flags & nb::kErrUpload)
+        return fail(c, NB_ERR_INVALID,
+                    "asynchronous upload rejected (non-finite value or mass <= 0); state unchanged");
     return fail(c, NB_ERR_CAPACITY, "tree build saw more than four children in a cell");
 }
 
@@ -446,6 +452,7 @@ int nb_destroy(nb_ctx* c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
     if (c->side_stream) cudaStreamSynchronize(c->side_stream);
+    if (c->up_stream) cudaStreamSynchronize(c->up_stream);
     drop_graphs(c);
     free_all(c);
     free_batch(c);
@@ -457,6 +464,9 @@ int nb_destroy(nb_ctx* c) {
     if (c->fork_ev) cudaEventDestroy(c->fork_ev);
     if (c->join_ev) cudaEventDestroy(c->join_ev);
     if (c->side_stream) cudaStreamDestroy(c->side_stream);
+    if (c->up_ready) cudaEventDestroy(c->up_ready);
+    if (c->up_used) cudaEventDestroy(c->up_used);
+    if (c->up_stream) cudaStreamDestroy(c->up_stream);
     for (auto& e : c->phase_ev)
         if (e) cudaEventDestroy(e);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -485,6 +495,59 @@ int nb_upload(nb_ctx* c, const double* mass, const double* pos_xy, const double*
     NB_CUDA(c, cudaStreamSynchronize(c->stream));
     if (bad & 1u) return fail(c, NB_ERR_INVALID, "non-finite mass, position or velocity");
     if (bad & 2u) return fail(c, NB_ERR_INVALID, "masses must be positive");
+    return NB_OK;
+}
+
+// Staging area and stream are made on first use; a failed set-up leaves the
+// context as it was and nb_upload still works.
+int nb_upload_async(nb_ctx* c, const double* mass, const double* pos_xy, const double* vel_xy) {
+    if (!c || !mass || !pos_xy || !vel_xy) return NB_ERR_INVALID;
+    const size_t n = (size_t)c->n;
+    DeviceGuard guard(c->device);
+    if (!c->up_stream) {
+        cudaStream_t st = nullptr;
+        cudaEvent_t ready = nullptr, used = nullptr;
+        double* m = nullptr;
+        double2 *p = nullptr, *v = nullptr;
+        if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&ready, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&used, cudaEventDisableTiming) != cudaSuccess ||
+            dalloc(&m, n) != cudaSuccess || dalloc(&p, n) != cudaSuccess ||
+            dalloc(&v, n) != cudaSuccess) {
+            cudaFree(m);
+            cudaFree(p);
+            cudaFree(v);
+            if (ready) cudaEventDestroy(ready);
+            if (used) cudaEventDestroy(used);
+            if (st) cudaStreamDestroy(st);
+            cudaGetLastError();
+            return fail(c, NB_ERR_NOMEM, "no device memory for the upload staging area");
+        }
+        c->up_stream = st;
+        c->up_ready = ready;
+        c->up_used = used;
+        c->up_mass = m;
+        c->up_pos = p;
+        c->up_vel = v;
+    }
+    // the staging area is free once the previous asynchronous upload has
+    // been moved into the state
+    NB_CUDA(c, cudaStreamWaitEvent(c->up_stream, c->up_used, 0));
+    NB_CUDA(c, cudaMemcpyAsync(c->up_mass, mass, n * sizeof(double), cudaMemcpyHostToDevice,
+                               c->up_stream));
+    NB_CUDA(c, cudaMemcpyAsync(c->up_pos, pos_xy, n * sizeof(double2), cudaMemcpyHostToDevice,
+                               c->up_stream));
+    NB_CUDA(c, cudaMemcpyAsync(c->up_vel, vel_xy, n * sizeof(double2), cudaMemcpyHostToDevice,
+                               c->up_stream));
+    NB_CUDA(c, cudaEventRecord(c->up_ready, c->up_stream));
+    // everything enqueued before this call still sees the old state
+    NB_CUDA(c, cudaStreamWaitEvent(c->stream, c->up_ready, 0));
+    const nb::BodyBuffers keep = c->buf[c->parity];
+    c->parity = 0;
+    nb::launch_upload_commit(c, c->up_mass, c->up_pos, c->up_vel, keep, c->buf[0],
+                             &c->scal->upload_bad);
+    NB_CUDA(c, cudaGetLastError());
+    NB_CUDA(c, cudaEventRecord(c->up_used, c->stream));
     return NB_OK;
 }
 

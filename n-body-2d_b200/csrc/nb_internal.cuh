@@ -25,6 +25,7 @@ constexpr int kBandPerBody = 16;   // learned mode: band-list capacity per body 
 constexpr unsigned kErrStack = 1u;      // DFS stack bound exceeded
 constexpr unsigned kErrTree = 2u;       // tree build saw an impossible range
 constexpr unsigned kErrTimeout = 4u;    // a bounded wait gave up
+constexpr unsigned kErrUpload = 8u;     // nb_upload_async rejected its bodies
 
 // Small device-resident values written and read by kernels of one step.
 struct DeviceScalars {
@@ -153,6 +154,9 @@ struct nb_ctx {
     cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
     cudaEvent_t staged = nullptr;        // the download's scatter into the staging buffers is done
     cudaEvent_t copied = nullptr;        // the staging buffers have been copied out (free again)
+    cudaStream_t up_stream = nullptr;    // nb_upload_async: host-to-device copies
+    cudaEvent_t up_ready = nullptr;      // the staged upload has arrived on the device
+    cudaEvent_t up_used = nullptr;       // it has been moved into the state (staging free again)
     cudaEvent_t phase_ev[nb::kPhases + 1] = {};
     int parity = 0;                 // which BodyBuffers holds the state
     nb::BodyBuffers buf[2];
@@ -178,6 +182,9 @@ struct nb_ctx {
     double2* acc = nullptr;              // optional FP64 accelerations (sorted order)
     double2* stage_pos = nullptr;        // original-order staging for downloads
     double2* stage_vel = nullptr;
+    double* up_mass = nullptr;           // nb_upload_async staging, allocated on first use
+    double2* up_pos = nullptr;
+    double2* up_vel = nullptr;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};  // one step from parity 0 / 1
     double graph_dt = 0.0;
     uint64_t steps = 0;
@@ -228,6 +235,11 @@ void launch_force_split(nb_ctx* c, const BodyBuffers& b, bool kick, bool store_a
 void launch_force_fp64(nb_ctx* c, const BodyBuffers& b, bool kick, bool store_acc);
 void launch_drift(nb_ctx* c, const BodyBuffers& b);
 void launch_upload_check(nb_ctx* c, const BodyBuffers& b, unsigned* bad);
+// Checks the staged bodies (m, p, v) into *bad, then copies them into dst;
+// a rejected set leaves dst holding `keep` (or untouched when keep is dst)
+// and raises kErrUpload.
+void launch_upload_commit(nb_ctx* c, const double* m, const double2* p, const double2* v,
+                          const BodyBuffers& keep, const BodyBuffers& dst, unsigned* bad);
 void launch_render(nb_ctx* c, const double2* pos, const nb_view& v, uint32_t* count,
                    const uint8_t* table, uchar4* rgba);
 void launch_allpairs_step(nb_ctx* c, const BodyBuffers& a, const BodyBuffers& b, bool integrate,

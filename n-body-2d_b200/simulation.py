@@ -96,6 +96,7 @@ class NbContext:
         universes concatenated in mass/pos/vel (nb_batch_create)."""
         lib = load()
         self.cfg = cfg
+        self._pending_upload = None
         self.n = int(np.asarray(mass).shape[0])
         mass = _f64(mass, (self.n,))
         pos = _f64(pos, (self.n, 2))
@@ -118,6 +119,7 @@ class NbContext:
         if getattr(self, "_h", None):
             self._lib.nb_destroy(self._h)
             self._h = None
+        self._pending_upload = None
 
     def __enter__(self):
         return self
@@ -144,7 +146,10 @@ class NbContext:
             self.sync()
 
     def sync(self) -> None:
-        check(self._lib.nb_sync(self.handle), self._h)
+        try:
+            check(self._lib.nb_sync(self.handle), self._h)
+        finally:
+            self._pending_upload = None
 
     def set_timestep(self, dt: float) -> None:
         check(self._lib.nb_set_timestep(self.handle, dt), self._h)
@@ -155,6 +160,16 @@ class NbContext:
         pos = _f64(pos, (self.n, 2))
         vel = _f64(vel, (self.n, 2))
         check(self._lib.nb_upload(self.handle, ptr(mass), ptr(pos), ptr(vel)), self._h)
+
+    def upload_async(self, mass: np.ndarray, pos: np.ndarray, vel: np.ndarray) -> None:
+        """nb_upload_async: the copy overlaps the work enqueued before it; the
+        arrays (pinned, C-contiguous float64 [n], [n, 2], [n, 2]) are read
+        until sync() returns and are kept alive until then."""
+        for a, shape in ((mass, (self.n,)), (pos, (self.n, 2)), (vel, (self.n, 2))):
+            if a.shape != shape or a.dtype != np.float64 or not a.flags.c_contiguous:
+                raise ValueError("upload_async needs C-contiguous float64 [n] / [n, 2] arrays")
+        check(self._lib.nb_upload_async(self.handle, ptr(mass), ptr(pos), ptr(vel)), self._h)
+        self._pending_upload = (mass, pos, vel)
 
     def download(self, pos: np.ndarray | None = None, vel: np.ndarray | None = None):
         if pos is None:

@@ -237,6 +237,77 @@ def test_download_async_matches_download(nbp):
     assert np.array_equal(ps, outs[2][0]) and np.array_equal(vs, outs[2][1])
 
 
+def test_upload_async_matches_upload(nbp):
+    """Pipelined uploads give the steps the same bodies as synchronous ones;
+    work enqueued before an asynchronous upload still sees the old state."""
+    torch = pytest.importorskip("torch")
+    n = 20000
+    m, p, v = nbp.universes.colliding_discs(n, 4)
+    pin = lambda shape: torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy()
+    hm, hp, hv = pin((n,)), pin((n, 2)), pin((n, 2))
+    hm[:], hp[:], hv[:] = m, p, v
+    hp2 = pin((n, 2))
+    hp2[:] = p + 0.5
+    cfg = nbp.SimConfig(mode=nbp.NB_MODE_SPLIT)
+    with nbp.NbContext(cfg, m, p, v) as ctx:
+        outs = []
+        for k in range(3):
+            ctx.step(1, sync=False)  # after a step the state sits in the second buffer
+            po0, vo0 = pin((n, 2)), pin((n, 2))
+            ctx.download_async(po0, vo0)  # enqueued before the upload: old state
+            ctx.upload_async(hm, hp2 if k == 1 else hp, hv)
+            ctx.step(k + 1, sync=False)
+            po, vo = pin((n, 2)), pin((n, 2))
+            ctx.download_async(po, vo)
+            outs.append((po0, vo0, po, vo))
+        ctx.download_wait()
+        ctx.sync()
+    with nbp.NbContext(cfg, m, p, v) as ref:
+        for k in range(3):
+            ref.step(1)
+            p0, v0 = ref.download()
+            assert np.array_equal(outs[k][0], p0) and np.array_equal(outs[k][1], v0)
+            ref.upload(m, p + 0.5 if k == 1 else p, v)
+            ref.step(k + 1)
+            pr, vr = ref.download()
+            assert np.array_equal(outs[k][2], pr) and np.array_equal(outs[k][3], vr)
+
+
+@pytest.mark.parametrize("steps_before", [0, 1])
+def test_upload_async_rejects_and_keeps_state(nbp, steps_before):
+    """A rejected asynchronous upload is reported at the next sync and leaves
+    the state as it was, from either state buffer."""
+    torch = pytest.importorskip("torch")
+    n = 5000
+    m, p, v = nbp.universes.exponential_disc(n, 2)
+    pin = lambda shape: torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy()
+    hm, hp, hv = pin((n,)), pin((n, 2)), pin((n, 2))
+    hm[:], hp[:], hv[:] = m, p, v
+    hp[100, 0] = np.nan
+    with nbp.NbContext(nbp.SimConfig(mode=nbp.NB_MODE_SPLIT), m, p, v) as ctx:
+        if steps_before:
+            ctx.step(steps_before)
+        p0, v0 = ctx.download()
+        ctx.upload_async(hm, hp, hv)
+        with pytest.raises(nbp.NbError, match="asynchronous upload rejected"):
+            ctx.sync()
+        p1, v1 = ctx.download()
+        assert np.array_equal(p0, p1) and np.array_equal(v0, v1)
+        hp[100, 0] = p[100, 0]
+        hm[7] = -1.0
+        ctx.upload_async(hm, hp, hv)
+        with pytest.raises(nbp.NbError, match="asynchronous upload rejected"):
+            ctx.sync()
+        hm[7] = m[7]
+        ctx.upload_async(hm, hp, hv)
+        ctx.step(1)
+        p2, _ = ctx.download()
+    with nbp.NbContext(nbp.SimConfig(mode=nbp.NB_MODE_SPLIT), m, p, v) as ref:
+        ref.step(1)
+        pr, _ = ref.download()
+    assert np.array_equal(p2, pr)
+
+
 def test_bounded_wait_times_out_without_hanging(nbp):
     """The radix sort's look-back waits on a predecessor tile; with one that
     never publishes, the wait gives up after its iteration bound, the kernel
