@@ -255,9 +255,10 @@ __device__ __forceinline__ void walk_group(WarpLists& L, const Tree& t, int root
         float4 c4 = make_float4(0.f, 0.f, 0.f, 0.f);
         float band_d2 = 0.f;
         if (lane < k) {
+            // the tree is read-only while the walk runs: non-coherent loads
             if (ref >= 0) {
-                c4 = t.cell4[ref];
-                const int2 rg = t.range[ref];
+                c4 = __ldg(t.cell4 + ref);
+                const int2 rg = __ldg(t.range + ref);
                 const bool overlap = !(rg.y < g0 || rg.x > g1);
                 const float dx = fmaxf(fabsf(c4.x - gcx) - ghx, 0.f);
                 const float dy = fmaxf(fabsf(c4.y - gcy) - ghy, 0.f);
@@ -271,7 +272,7 @@ __device__ __forceinline__ void walk_group(WarpLists& L, const Tree& t, int root
                     bcnt = rg.y - rg.x + 1;
                 } else {
                     act = 3;
-                    ch = t.child[ref];
+                    ch = __ldg(t.child + ref);
                 }
             } else {
                 const int b = ~ref;
@@ -351,7 +352,7 @@ __device__ __forceinline__ void walk_group(WarpLists& L, const Tree& t, int root
             const int added = min(32, btot - base);
             __syncwarp();
             if (lane < added) {
-                const float4 b4 = t.body4[j];
+                const float4 b4 = __ldg(t.body4 + j);
                 put_entry(L.bxy, L.bm, bcount + lane, b4.x, b4.y, b4.z);
             }
             bcount += added;
