@@ -798,13 +798,16 @@ mlp_correct_kick(const InferW* __restrict__ Wg, Tree t, const DeviceScalars* __r
         const int nband = min(t.band_count[gi], kBandPerBody * (g1 - g0 + 1));
         const int* band = t.band + (int64_t)kBandPerBody * g0;
         float cxs = 0.f, cys = 0.f;
+        // the next batch's band index is loaded one batch ahead
+        int ref_next = lane < nband ? band[lane] : 0;
         for (int base = 0; base < nband; base += 32) {
             // lane l builds row l % 16 of tile l / 16
             const int r = base + lane;
+            const int ref = ref_next;
+            ref_next = r + 32 < nband ? band[r + 32] : 0;
             uint4 lo = make_uint4(0u, 0u, 0u, 0u), hi = lo;
             float sc = 0.f;
             if (r < nband) {
-                const int ref = band[r];
                 // one 32-byte record: the BF16 features, then COM, mass, width
                 lo = t.cellh[2 * ref];
                 const uint4 gb = t.cellh[2 * ref + 1];
