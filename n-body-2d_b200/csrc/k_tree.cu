@@ -522,17 +522,41 @@ __device__ double4 block_sum_d4(double4 v, double4* red) {
     return tot;  // valid in thread 0
 }
 
+// Bodies of a tile are read in coalesced rows: warp w takes the kWarpItems
+// bodies [w kWarpItems, (w + 1) kWarpItems) of the tile, lane l the bodies
+// 32 k + l of them.
+constexpr int kWarpItems = 32 * kScanItems;
+
 // Phase 1: per tile of kScanTile bodies, the total.
 __global__ void __launch_bounds__(kThreads)
 prefix_reduce(const double2* __restrict__ pos, const double* __restrict__ mass, int n,
               const DeviceScalars* __restrict__ s, Batch bt, double4* __restrict__ tiles) {
     __shared__ double4 red[kThreads / 32];
-    const int base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int base = blockIdx.x * kScanTile + warp * kWarpItems + lane;
     double4 v = make_double4(0.0, 0.0, 0.0, 0.0);
+#pragma unroll
     for (int k = 0; k < kScanItems; ++k)
-        if (base + k < n) v = d4_add(v, body_term(pos, mass, s, bt, base + k));
+        if (base + 32 * k < n) v = d4_add(v, body_term(pos, mass, s, bt, base + 32 * k));
     const double4 tot = block_sum_d4(v, red);
     if (threadIdx.x == 0) tiles[blockIdx.x] = tot;
+}
+
+// Inclusive scan across the warp of the three components body_term fills.
+__device__ __forceinline__ double4 warp_inclusive_d4(double4 v) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const double x = __shfl_up_sync(kFull, v.x, o);
+        const double y = __shfl_up_sync(kFull, v.y, o);
+        const double z = __shfl_up_sync(kFull, v.z, o);
+        if (lane >= o) {
+            v.x += x;
+            v.y += y;
+            v.z += z;
+        }
+    }
+    return v;
 }
 
 // Exclusive scan, in thread order, of one value per thread of the block.
@@ -576,23 +600,42 @@ __global__ void __launch_bounds__(kThreads) prefix_tiles_scan(double4* __restric
 }
 
 // Phase 3: prefix[i] = sum over bodies before i; prefix[n] = the total.
+// Each row of 32 bodies is scanned with shuffles; the rows' totals carry
+// within the warp, and the warps' totals (one barrier) within the tile.
 __global__ void __launch_bounds__(kThreads)
 prefix_apply(const double2* __restrict__ pos, const double* __restrict__ mass, int n,
              const DeviceScalars* __restrict__ s, Batch bt, const double4* __restrict__ tiles,
              int ntiles, double4* __restrict__ prefix) {
-    __shared__ double4 part[kThreads];
-    const int base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
-    double4 v[kScanItems];
-    double4 run = make_double4(0.0, 0.0, 0.0, 0.0);
+    __shared__ double4 wtot[kThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int base = blockIdx.x * kScanTile + warp * kWarpItems + lane;
+    const double4 zero = make_double4(0.0, 0.0, 0.0, 0.0);
+    double4 ex[kScanItems];   // exclusive prefix within the row, then within the warp
+    double4 carry = zero;     // total of the rows before
+#pragma unroll
     for (int k = 0; k < kScanItems; ++k) {
-        v[k] = base + k < n ? body_term(pos, mass, s, bt, base + k) : make_double4(0.0, 0.0, 0.0, 0.0);
-        run = d4_add(run, v[k]);
+        const int i = base + 32 * k;
+        const double4 v = i < n ? body_term(pos, mass, s, bt, i) : zero;
+        const double4 inc = warp_inclusive_d4(v);
+        double4 e;
+        e.x = __shfl_up_sync(kFull, inc.x, 1);
+        e.y = __shfl_up_sync(kFull, inc.y, 1);
+        e.z = __shfl_up_sync(kFull, inc.z, 1);
+        e.w = 0.0;
+        if (lane == 0) e = zero;
+        ex[k] = d4_add(carry, e);
+        const double4 row = make_double4(__shfl_sync(kFull, inc.x, 31), __shfl_sync(kFull, inc.y, 31),
+                                         __shfl_sync(kFull, inc.z, 31), 0.0);
+        carry = d4_add(carry, row);
     }
-    double4 total;
-    double4 acc = d4_add(tiles[blockIdx.x], block_exclusive_d4(run, part, total));
+    if (lane == 0) wtot[warp] = carry;
+    __syncthreads();
+    double4 off = tiles[blockIdx.x];
+    for (int w = 0; w < warp; ++w) off = d4_add(off, wtot[w]);
+#pragma unroll
     for (int k = 0; k < kScanItems; ++k) {
-        if (base + k < n) prefix[base + k] = acc;
-        acc = d4_add(acc, v[k]);
+        const int i = base + 32 * k;
+        if (i < n) prefix[i] = d4_add(off, ex[k]);
     }
     if (blockIdx.x == ntiles - 1 && threadIdx.x == 0) prefix[n] = tiles[ntiles];
 }
