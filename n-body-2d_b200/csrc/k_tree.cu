@@ -130,15 +130,19 @@ __device__ int block_exclusive(int v, int* wsum, int* total) {
     return r;
 }
 
+// Items of a tile are read in coalesced rows: warp w takes the 32 *
+// kScanItems items [w 32 kScanItems, (w + 1) 32 kScanItems) of the tile,
+// lane l the items 32 k + l of them.
 __global__ void __launch_bounds__(kThreads)
 scan_reduce(const int32_t* __restrict__ in, int n, int32_t* __restrict__ block_sums) {
     __shared__ int wsum[kThreads / 32];
     __shared__ int total;
-    const int base = blockIdx.x * kScanTile;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int base = blockIdx.x * kScanTile + warp * 32 * kScanItems + lane;
     int v = 0;
 #pragma unroll
     for (int k = 0; k < kScanItems; ++k) {
-        const int i = base + k * kThreads + threadIdx.x;
+        const int i = base + 32 * k;
         if (i < n) v += in[i];
     }
     block_exclusive(v, wsum, &total);
@@ -161,29 +165,37 @@ scan_block_sums(int32_t* __restrict__ block_sums, int blocks, int32_t* __restric
     if (threadIdx.x == 0) *total_out = carry;
 }
 
+// Each row of 32 items is scanned with shuffles; the rows' totals carry
+// within the warp, and the warps' totals (one barrier) within the tile.
 __global__ void __launch_bounds__(kThreads)
 scan_apply(const int32_t* __restrict__ in, int n, const int32_t* __restrict__ block_sums,
            int32_t* __restrict__ out, int32_t* __restrict__ index_of) {
     __shared__ int wsum[kThreads / 32];
-    __shared__ int total;
-    // Items of a thread are consecutive so one block scan covers the tile.
-    const int base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
-    int v[kScanItems];
-    int sum = 0;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int base = blockIdx.x * kScanTile + warp * 32 * kScanItems + lane;
+    int v[kScanItems], ex[kScanItems];
+    int carry = 0;
 #pragma unroll
     for (int k = 0; k < kScanItems; ++k) {
-        v[k] = base + k < n ? in[base + k] : 0;
-        sum += v[k];
+        const int i = base + 32 * k;
+        v[k] = i < n ? in[i] : 0;
+        const int inc = warp_inclusive(v[k]);
+        ex[k] = carry + inc - v[k];
+        carry += __shfl_sync(kFull, inc, 31);
     }
-    int run = block_exclusive(sum, wsum, &total) + block_sums[blockIdx.x];
+    if (lane == 0) wsum[warp] = carry;
+    __syncthreads();
+    int off = block_sums[blockIdx.x];
+    for (int w = 0; w < warp; ++w) off += wsum[w];
 #pragma unroll
     for (int k = 0; k < kScanItems; ++k) {
-        if (base + k < n) {
-            out[base + k] = run;
+        const int i = base + 32 * k;
+        if (i < n) {
+            const int run = off + ex[k];
+            out[i] = run;
             // with 0/1 inputs, index_of lists the flagged positions in order
-            if (index_of && v[k]) index_of[run] = base + k;
+            if (index_of && v[k]) index_of[run] = i;
         }
-        run += v[k];
     }
 }
 
