@@ -645,7 +645,7 @@ def run_variants(args, nb, m, p, v, device, plain_value, plain_accuracy) -> dict
     workload, same timing method), plus the analytic-quadrupole and plain
     theta = 1.0 walks, each with its p50/p99 force error against FP64
     all-pairs.  The learned step falls back to plain theta = 0.5 when its p99
-    is worse than the plain step's (the judge of the learned mode)."""
+    is worse than the plain step's (the learned mode's fallback rule)."""
     from nbody_b200 import accuracy as acc_mod
 
     weights = PKG / "weights" / "correction_theta1.npy"
@@ -682,8 +682,8 @@ def run_variants(args, nb, m, p, v, device, plain_value, plain_accuracy) -> dict
                      "correction_ms": round(phases.get("drift", 0.0), 4)}
     if "learned_theta1.0" in out and plain_accuracy:
         lv = out["learned_theta1.0"]
-        lv["judge"] = ("kept" if lv["p99"] <= plain_accuracy["p99"]
-                       else "falls back to plain theta=0.5 (p99 above the plain step's)")
+        lv["fallback_rule"] = ("kept" if lv["p99"] <= plain_accuracy["p99"]
+                               else "falls back to plain theta=0.5 (p99 above the plain step's)")
     return out
 
 
