@@ -279,7 +279,9 @@ NB_API int nb_mlp_samples(nb_ctx* ctx, uint64_t ntargets, uint64_t seed, uint64_
                           float* features, float* residuals, uint64_t* count);
 
 /* Batched MLP on the GPU: out[n][2] = network(features[n][12]) (without the
- * output scale).  Host arrays. */
+ * output scale).  Host arrays.  Runs on the tcgen05 tensor cores in 128-row
+ * tiles (BF16 operands, FP32 accumulation, tanh on BF16 pairs as the step's
+ * correction applies it); NB_ERR_TIMEOUT if a bounded wait for an MMA ran out. */
 NB_API int nb_mlp_forward(int32_t device, const float* params, uint64_t n, const float* features,
                           float* out);
 

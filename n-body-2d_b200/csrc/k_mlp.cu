@@ -25,6 +25,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
 #include <climits>
 #include <cmath>
 #include <cstring>
@@ -195,51 +196,7 @@ __device__ void fill_weights(const float* __restrict__ p, MlpWeights& W) {
     if (threadIdx.x == 0) W.yscale = p[kYS];
 }
 
-// One 16 x 16 BF16 input tile staged in shared memory per warp.
-struct XTile {
-    __nv_bfloat16 x[16][16];
-};
-
-// ---- batched forward (tests and offline evaluation) --------------------
 constexpr int kWarps = 4;
-
-__global__ void __launch_bounds__(kWarps * 32)
-mlp_forward_kernel(const float* __restrict__ params, const float* __restrict__ X, int64_t n,
-                   float* __restrict__ Y) {
-    __shared__ MlpWeights W;
-    __shared__ XTile tiles[kWarps];
-    fill_weights(params, W);
-    __syncthreads();
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    XTile& T = tiles[warp];
-    const int64_t ntiles = (n + 15) / 16;
-    for (int64_t tile = blockIdx.x * (int64_t)kWarps + warp; tile < ntiles;
-         tile += (int64_t)gridDim.x * kWarps) {
-        for (int e = lane; e < 256; e += 32) {
-            const int r = e >> 4, k = e & 15;
-            const int64_t s = tile * 16 + r;
-            T.x[r][k] = __float2bfloat16_rn(s < n && k < kNin ? X[s * kNin + k] : 0.f);
-        }
-        __syncwarp();
-        uint32_t a[4];
-        load_a(&T.x[0][0], 16, 0, a);
-        Fwd f;
-        mlp_forward(W, a, f);
-        const int g = lane >> 2, q = lane & 3;
-        if (q == 0) {
-            const int64_t s0 = tile * 16 + g, s1 = s0 + 8;
-            if (s0 < n) {
-                Y[2 * s0] = f.y[0];
-                Y[2 * s0 + 1] = f.y[1];
-            }
-            if (s1 < n) {
-                Y[2 * s1] = f.y[2];
-                Y[2 * s1 + 1] = f.y[3];
-            }
-        }
-        __syncwarp();
-    }
-}
 
 // ---- training: loss and gradients of a batch ---------------------------
 // Loss = mean over the batch of |y - t|^2 (t already divided by yscale).
@@ -868,6 +825,294 @@ mlp_correct_kick(const InferW* __restrict__ Wg, Tree t, const DeviceScalars* __r
     }
 }
 
+// ---- the network on the 5th-generation tensor cores (tcgen05) --------------
+// 128-row tiles: row r of a tile is TMEM lane r, so warp w of a four-warp CTA
+// writes rows 32w..32w+31 and reads back exactly those lanes.  One thread
+// issues the three layers as tcgen05.mma (M = 128; N = 64, 64, 16; K = 16,
+// 64, 64) with BF16 operands in shared memory and FP32 accumulators in TMEM.
+// The step's correction (mlp_correct_kick) stays on mma.sync: there every
+// warp feeds its own group's 32 band cells at a time, and the three MMA round
+// trips and barriers a 128-row tile needs made it slower (0.83 against
+// 0.64 ms at 4M bodies, measured), while bulk evaluation fills whole tiles.
+//
+// Shared-memory operands use the no-swizzle K-major layout of 8-row x 16-byte
+// core matrices: element (row, k) of an operand with K columns sits at byte
+//   (row / 8) * SBO + (k / 8) * 128 + (row % 8) * 16 + (k % 8) * 2,
+// SBO = 16 K bytes; a K step of 16 starts 256 bytes further on.
+constexpr int kTcRows = 128;
+constexpr int kTcWarps = kTcRows / 32;  // one warp per 32 rows (TMEM lanes)
+constexpr uint32_t kTcCols = 64;    // TMEM columns a CTA allocates; the three layers share them
+constexpr int kTcBlocksPerSm = 6;   // shared memory allows six CTAs per SM, TMEM eight
+constexpr int kTcSpin = 1 << 20;    // bound on each wait for an MMA to complete
+
+struct UmmaW {
+    uint4 w1[kH * 16 / 8];     // B of layer 1: n = hidden (64) x k = input column (16)
+    uint4 w2[kH * kH / 8];     // B of layer 2: n = out (64) x k = in (64)
+    uint4 w3[16 * kH / 8];     // B of layer 3: n = out (2 used of 16) x k = hidden (64)
+    float b1[kH], b2[kH], b3[2], yscale, pad;
+};
+
+__host__ __device__ constexpr int umma_off(int row, int k, int sbo) {
+    return (row / 8) * sbo + (k / 8) * 128 + (row % 8) * 16 + (k % 8) * 2;
+}
+
+__global__ void mlp_prepare_umma(const float* __restrict__ p, UmmaW* __restrict__ W) {
+    auto put = [](uint4* img, int off, float v) {
+        reinterpret_cast<__nv_bfloat16*>(img)[off / 2] = __float2bfloat16_rn(v);
+    };
+    for (int e = threadIdx.x; e < kH * 16; e += blockDim.x) {
+        const int n = e / 16, k = e % 16, f = infer_feature(k);
+        put(W->w1, umma_off(n, k, 256), f < 0 ? 0.f : p[kW1 + n * kNin + f]);
+    }
+    for (int e = threadIdx.x; e < kH * kH; e += blockDim.x) {
+        const int n = e / kH, k = e % kH;
+        put(W->w2, umma_off(n, k, 1024), p[kW2 + n * kH + k]);
+    }
+    for (int e = threadIdx.x; e < 16 * kH; e += blockDim.x) {
+        const int n = e / kH, k = e % kH;
+        put(W->w3, umma_off(n, k, 1024), n < 2 ? p[kW3 + n * kH + k] : 0.f);
+    }
+    for (int e = threadIdx.x; e < kH; e += blockDim.x) {
+        W->b1[e] = p[kB1 + e];
+        W->b2[e] = p[kB2 + e];
+    }
+    if (threadIdx.x == 0) {
+        W->b3[0] = p[kB3];
+        W->b3[1] = p[kB3 + 1];
+        W->yscale = p[kYS];
+        W->pad = 0.f;
+    }
+}
+
+struct TcSmem {
+    UmmaW W;
+    alignas(128) uint4 a1[kTcRows * 16 / 8];   // layer-1 input rows (K = 16)
+    alignas(128) uint4 a2[kTcRows * kH / 8];   // hidden rows (K = 64), both layers
+    alignas(8) uint64_t mbar;                  // MMA completion
+    uint32_t tmem;                             // TMEM base address from tcgen05.alloc
+    int fail;                                  // a wait for an MMA ran out
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* ptr) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(ptr));
+}
+
+// shared-memory matrix descriptor (sm_100 format): start, LBO and SBO in
+// 16-byte units, version 1, no swizzle
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// instruction descriptor: FP32 accumulator, BF16 A and B, both K-major, M x N
+constexpr uint32_t umma_idesc(int m, int n) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) |
+           ((uint32_t)(m >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc,
+                                          uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+        :: "r"(d_tmem), "l"(a), "l"(b), "r"(idesc), "r"(accumulate) : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                 :: "r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+// generic-proxy stores to shared memory become visible to the MMA's reads
+__device__ __forceinline__ void fence_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// waits for phase `parity` of the barrier; false when the bound ran out
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+    const uint32_t a = smem_u32(bar);
+    for (int i = 0; i < kTcSpin; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred P1;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, P1;\n\t}"
+            : "=r"(done) : "r"(a), "r"(parity) : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+// 16 consecutive FP32 columns of this thread's TMEM lane; the wait is tied to
+// the registers so that no use moves above it
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+        "%11, %12, %13, %14, %15}, [%16];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+          "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+          "=r"(v[14]), "=r"(v[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+r"(v[0]), "+r"(v[1]), "+r"(v[2]), "+r"(v[3]), "+r"(v[4]), "+r"(v[5]),
+                   "+r"(v[6]), "+r"(v[7]), "+r"(v[8]), "+r"(v[9]), "+r"(v[10]), "+r"(v[11]),
+                   "+r"(v[12]), "+r"(v[13]), "+r"(v[14]), "+r"(v[15])
+                 :: "memory");
+}
+
+__device__ __forceinline__ void tmem_ld2(uint32_t taddr, uint32_t& a, uint32_t& b) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x2.b32 {%0, %1}, [%2];"
+                 : "=r"(a), "=r"(b) : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" : "+r"(a), "+r"(b) :: "memory");
+}
+
+// Bias, tanh and BF16 packing of this thread's 64 hidden columns at TMEM
+// column col0; the row is stored as the next layer's A operand.
+__device__ __forceinline__ void tc_hidden_row(uint32_t tlane, uint32_t col0, const float* bias,
+                                              uint4* a2, int row) {
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        uint32_t v[16];
+        tmem_ld16(tlane + col0 + 16 * c, v);
+        uint32_t h[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+            h[j] = tanh_bf16x2(pack_bf16(__uint_as_float(v[2 * j]) + bias[16 * c + 2 * j],
+                                         __uint_as_float(v[2 * j + 1]) + bias[16 * c + 2 * j + 1]));
+        uint4* dst = a2 + umma_off(row, 16 * c, 1024) / 16;
+        dst[0] = make_uint4(h[0], h[1], h[2], h[3]);
+        dst[8] = make_uint4(h[4], h[5], h[6], h[7]);  // the next 8 columns: +128 bytes
+    }
+}
+
+// Bulk evaluation of n independent feature rows (nb_mlp_forward): every tile
+// is 128 rows, row r of the tile in TMEM lane r.  Per tile one thread issues
+// the three layers as tcgen05.mma; between them every thread loads its row
+// from TMEM, adds the bias, applies tanh to packed BF16 pairs and stores the
+// row as the next layer's A operand.  The input columns are in the order of
+// the correction's records (infer_feature), so the weight image is shared.
+__global__ void __launch_bounds__(kTcWarps * 32, kTcBlocksPerSm)
+mlp_forward_tc(const UmmaW* __restrict__ Wg, const float* __restrict__ X, int64_t n,
+               float* __restrict__ Y, unsigned* __restrict__ err) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    TcSmem& S = *reinterpret_cast<TcSmem*>(smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u));
+    const int tid = threadIdx.x, warp = tid >> 5;
+    {
+        const uint4* src = reinterpret_cast<const uint4*>(Wg);
+        uint4* dst = reinterpret_cast<uint4*>(&S.W);
+        for (int k = tid; k < (int)(sizeof(UmmaW) / 16); k += blockDim.x) dst[k] = src[k];
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&S.mbar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        S.fail = 0;
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     :: "r"(smem_u32(&S.tmem)), "r"(kTcCols) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    fence_async_smem();  // the weights, stored through the generic proxy, feed the MMAs
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = S.tmem;
+    const uint32_t tlane = tmem + ((uint32_t)(32 * warp) << 16);  // this warp's lanes
+    const uint32_t a1_addr = smem_u32(S.a1), a2_addr = smem_u32(S.a2);
+    const uint32_t w1_addr = smem_u32(S.W.w1), w2_addr = smem_u32(S.W.w2),
+                   w3_addr = smem_u32(S.W.w3);
+    const int row = tid;  // this thread's tile row and TMEM lane
+    uint32_t phase = 0;
+    for (int64_t tile = blockIdx.x; tile * kTcRows < n; tile += gridDim.x) {
+        if (S.fail) break;  // uniform: set before the barrier that ended the last tile
+        const int64_t sr = tile * kTcRows + row;
+        uint32_t x[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const int f0 = infer_feature(2 * k), f1 = infer_feature(2 * k + 1);
+            const float v0 = sr < n && f0 >= 0 ? X[sr * kNin + f0] : 0.f;
+            const float v1 = sr < n && f1 >= 0 ? X[sr * kNin + f1] : 0.f;
+            x[k] = pack_bf16(v0, v1);
+        }
+        {
+            uint4* dst = S.a1 + umma_off(row, 0, 256) / 16;
+            dst[0] = make_uint4(x[0], x[1], x[2], x[3]);
+            dst[8] = make_uint4(x[4], x[5], x[6], x[7]);
+        }
+        fence_async_smem();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+            umma_bf16(tmem, umma_desc(a1_addr, 128, 256), umma_desc(w1_addr, 128, 256),
+                      umma_idesc(kTcRows, kH), 0u);
+            umma_commit(&S.mbar);
+        }
+        if (!mbar_wait(&S.mbar, phase)) S.fail = 1;
+        phase ^= 1u;
+        tc_fence_after();
+        tc_hidden_row(tlane, 0u, S.W.b1, S.a2, row);
+
+        tc_fence_before();
+        fence_async_smem();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                umma_bf16(tmem, umma_desc(a2_addr + 256u * j, 128, 1024),
+                          umma_desc(w2_addr + 256u * j, 128, 1024), umma_idesc(kTcRows, kH),
+                          j > 0 ? 1u : 0u);
+            umma_commit(&S.mbar);
+        }
+        if (!mbar_wait(&S.mbar, phase)) S.fail = 1;
+        phase ^= 1u;
+        tc_fence_after();
+        tc_hidden_row(tlane, 0u, S.W.b2, S.a2, row);
+
+        tc_fence_before();
+        fence_async_smem();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                umma_bf16(tmem, umma_desc(a2_addr + 256u * j, 128, 1024),
+                          umma_desc(w3_addr + 256u * j, 128, 1024), umma_idesc(kTcRows, 16),
+                          j > 0 ? 1u : 0u);
+            umma_commit(&S.mbar);
+        }
+        if (!mbar_wait(&S.mbar, phase)) S.fail = 1;
+        phase ^= 1u;
+        tc_fence_after();
+        uint32_t y0, y1;
+        tmem_ld2(tlane, y0, y1);
+        if (sr < n) {
+            Y[2 * sr] = __uint_as_float(y0) + S.W.b3[0];
+            Y[2 * sr + 1] = __uint_as_float(y1) + S.W.b3[1];
+        }
+        tc_fence_before();
+        __syncthreads();  // TMEM columns and operand rows are free for the next tile
+    }
+    if (S.fail) {
+        // the last MMAs may still run: wait for them (bounded) before freeing TMEM
+        mbar_wait(&S.mbar, phase ^ 1u);
+        if (tid == 0) atomicOr(err, kErrTimeout);
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
+                     :: "r"(tmem), "r"(kTcCols) : "memory");
+    }
+}
+
 inline unsigned blocks_for(int64_t n, int per) { return (unsigned)((n + per - 1) / per); }
 
 }  // namespace
@@ -906,10 +1151,18 @@ void launch_mlp_samples(nb_ctx* c, const BodyBuffers& b, const int* pick, int np
         c->p.epsilon_squared, X, Y, count, cap);
 }
 
-int mlp_forward_device(const float* params, const float* X, int64_t n, float* Y,
-                       cudaStream_t st) {
-    mlp_forward_kernel<<<(unsigned)std::min<int64_t>((n + 63) / 64, 4096), kWarps * 32, 0, st>>>(
-        params, X, n, Y);
+size_t mlp_forward_image_bytes() { return sizeof(UmmaW); }
+
+int mlp_forward_device(const float* params, const float* X, int64_t n, float* Y, void* image,
+                       unsigned* err, int sm_count, cudaStream_t st) {
+    UmmaW* W = static_cast<UmmaW*>(image);
+    mlp_prepare_umma<<<1, 256, 0, st>>>(params, W);
+    // 1 KB of slack to align the operands to 1024 bytes
+    const int smem = (int)(sizeof(TcSmem) + 1024);
+    cudaFuncSetAttribute(mlp_forward_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    const int64_t tiles = (n + kTcRows - 1) / kTcRows;
+    const int grid = (int)std::min<int64_t>(tiles, (int64_t)sm_count * kTcBlocksPerSm);
+    mlp_forward_tc<<<grid, kTcWarps * 32, smem, st>>>(W, X, n, Y, err);
     return cudaGetLastError() == cudaSuccess ? NB_OK : NB_ERR_CUDA;
 }
 

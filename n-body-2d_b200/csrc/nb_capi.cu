@@ -948,13 +948,23 @@ int nb_mlp_forward(int32_t device, const float* params, uint64_t n, const float*
     DeviceScope scope(device);
     if (scope.rc != NB_OK) return scope.rc;
     DBuf<float> p(NB_MLP_PARAMS), x(12 * n), y(2 * n);
-    if (!p.p || !x.p || !y.p) return NB_ERR_NOMEM;
+    DBuf<unsigned char> image(nb::mlp_forward_image_bytes());
+    DBuf<unsigned> err(1);
+    if (!p.p || !x.p || !y.p || !image.p || !err.p) return NB_ERR_NOMEM;
+    int sm_count = 0;
+    if (cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
+        return NB_ERR_CUDA;
     cudaMemcpy(p.p, params, sizeof(float) * NB_MLP_PARAMS, cudaMemcpyHostToDevice);
     cudaMemcpy(x.p, features, sizeof(float) * 12 * n, cudaMemcpyHostToDevice);
-    if (nb::mlp_forward_device(p.p, x.p, (int64_t)n, y.p, nullptr) != NB_OK) return NB_ERR_CUDA;
-    if (cudaMemcpy(out, y.p, sizeof(float) * 2 * n, cudaMemcpyDeviceToHost) != cudaSuccess)
+    cudaMemset(err.p, 0, sizeof(unsigned));
+    if (nb::mlp_forward_device(p.p, x.p, (int64_t)n, y.p, image.p, err.p, sm_count, nullptr) !=
+        NB_OK)
         return NB_ERR_CUDA;
-    return NB_OK;
+    unsigned flags = 0;
+    if (cudaMemcpy(out, y.p, sizeof(float) * 2 * n, cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(&flags, err.p, sizeof(unsigned), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return NB_ERR_CUDA;
+    return (flags & nb::kErrTimeout) ? NB_ERR_TIMEOUT : NB_OK;
 }
 
 int nb_mlp_loss_grad(int32_t device, const float* params, uint64_t n, const float* features,

@@ -225,7 +225,10 @@ size_t mlp_infer_bytes();
 void mlp_prepare_inference(nb_ctx* c);
 void launch_mlp_samples(nb_ctx* c, const BodyBuffers& b, const int* slots, int nslots, float* X,
                         float* Y, unsigned* count, unsigned cap);
-int mlp_forward_device(const float* params, const float* X, int64_t n, float* Y, cudaStream_t st);
+// bulk forward on tcgen05: image = mlp_forward_image_bytes() of device scratch
+size_t mlp_forward_image_bytes();
+int mlp_forward_device(const float* params, const float* X, int64_t n, float* Y, void* image,
+                       unsigned* err, int sm_count, cudaStream_t st);
 int mlp_grad_device(const float* params, const float* X, const float* Yt, const int64_t* idx,
                     int64_t n, float* grad, float* loss, int blocks, cudaStream_t st);
 int mlp_adam_device(float* p, const float* g, float* m, float* v, float lr, int step,
