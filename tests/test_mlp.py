@@ -35,7 +35,8 @@ def test_forward_matches_oracle(nbp):
     from oracle import mlp_oracle as mo
 
     p = mo.init(7)
-    X = _data(8, 1000)
+    # 2^17 + 5 rows: 1025 tiles of 128 for the tcgen05 kernel, the last one ragged
+    X = _data(8, (1 << 17) + 5)
     y = nbp.mlp_forward(p.astype(np.float32), X)
     y_o, _ = mo.forward(p.astype(np.float32), X)
     assert np.abs(y - y_o).max() < 2e-2 * max(1.0, np.abs(y_o).max())
