@@ -479,6 +479,17 @@ def run_ours(args) -> None:
     ctx.close()
     if rank == 0 and args.variants:
         line["variants"] = run_variants(args, nb, m, p, v, local, value, accuracy)
+    elif (rank == 0 and accuracy and not args.no_learned_comparison and args.workload == "collision4m"
+          and args.mode == "split" and not args.learned and not args.quad and not args.bmax):
+        # the headline comparison: the learned theta = 1.0 step against this plain step
+        lv = run_variants(args, nb, m, p, v, local, value, accuracy,
+                          only=("learned_theta1.0",)).get("learned_theta1.0")
+        if lv:
+            line["learned_vs_plain"] = {
+                "learned_value": lv["value"], "learned_ms_per_step": lv["ms_per_step"],
+                "ratio": lv["speedup_vs_plain"], "learned_p50": lv["p50"], "learned_p99": lv["p99"],
+                "plain_p99": accuracy["p99"], "fallback_rule": lv["fallback_rule"],
+                "target_ratio": 2.0}
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.n, args.theta, m, p, v)
     if world > 1:
@@ -640,7 +651,7 @@ def _learned_weights():
     return np.load(weights), bmax
 
 
-def run_variants(args, nb, m, p, v, device, plain_value, plain_accuracy) -> dict:
+def run_variants(args, nb, m, p, v, device, plain_value, plain_accuracy, only=None) -> dict:
     """The learned theta = 1.0 step next to the plain theta = 0.5 one (same
     workload, same timing method), plus the analytic-quadrupole and plain
     theta = 1.0 walks, each with its p50/p99 force error against FP64
@@ -661,6 +672,8 @@ def run_variants(args, nb, m, p, v, device, plain_value, plain_accuracy) -> dict
         # the walk the network was trained on (the b_max ratio of its record)
         bmax = json.loads(record.read_text()).get("bmax_ratio", 0.0) if record.exists() else 0.0
         specs.insert(0, ("learned_theta1.0", dict(theta=1.0, learned=True, bmax_ratio=bmax)))
+    if only is not None:
+        specs = [(name, kw) for name, kw in specs if name in only]
     for name, kw in specs:
         cfg = nb.SimConfig(timestep=1e-4, epsilon_squared=1e-4, G=1.0, mode=nb.NB_MODE_SPLIT,
                            device=device, **kw)
@@ -711,6 +724,8 @@ def main(argv=None):
     ap.add_argument("--leaf", type=int, default=0, help="SPLIT: direct-sum cell size (0=default)")
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--error-sample", type=int, default=65536)
+    ap.add_argument("--no-learned-comparison", action="store_true",
+                    help="skip the learned theta=1.0 step timed next to the default plain step")
     ap.add_argument("--variants", action="store_true",
                     help="also time the learned, quadrupole and plain theta=1.0 walks")
     ap.add_argument("--universes", type=int, default=512, help="ensemble512: universe count")
