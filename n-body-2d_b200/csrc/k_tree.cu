@@ -928,10 +928,16 @@ void launch_tree(nb_ctx* c, const BodyBuffers& b) {
     tree_trivial_root<<<1, 1, 0, c->stream>>>(b.pos, b.mass, n, c->tree, c->scal);
 }
 
+void launch_features(nb_ctx* c, const BodyBuffers& b) {
+    const int cap = (int)(c->n > 1 ? c->n - 1 : 1);
+    c->launches += 1;
+    learned_features<<<blocks_for(cap, kThreads), kThreads, 0, c->stream>>>(c->scal, b.pos, b.mass,
+                                                                           c->tree, c->batch);
+}
+
 void launch_moments(nb_ctx* c, const BodyBuffers& b, bool split) {
     // Cells never exceed n - 1; threads beyond the live count exit at once.
     const int cap = (int)(c->n > 1 ? c->n - 1 : 1);
-    const bool feat = split && c->tree.cellh != nullptr;
     const bool second = split && (c->p.flags & NB_FLAG_QUADRUPOLE);
     const double ratio = c->p.bmax_ratio;
     const float accept_scale =
@@ -942,7 +948,7 @@ void launch_moments(nb_ctx* c, const BodyBuffers& b, bool split) {
         tree_moments<true, true><<<blocks, kThreads, 0, c->stream>>>(c->scal, b.pos, b.mass, c->tree,
                                                                      c->batch, accept_scale);
     } else if (split) {
-        // monopoles from the prefix sums, then (learned) the features
+        // monopoles from the prefix sums
         const int n = (int)c->n;
         const int tiles = (int)blocks_for(n, kScanTile);
         c->launches += 4;
@@ -953,11 +959,6 @@ void launch_moments(nb_ctx* c, const BodyBuffers& b, bool split) {
                                                         c->tree.prefix_tiles, tiles, c->tree.prefix);
         cells_from_prefix<<<blocks, kThreads, 0, c->stream>>>(c->tree.prefix, c->tree, c->scal,
                                                               c->batch, b.pos, accept_scale);
-        if (feat) {
-            c->launches += 1;
-            learned_features<<<blocks, kThreads, 0, c->stream>>>(c->scal, b.pos, b.mass, c->tree,
-                                                                 c->batch);
-        }
     } else {
         c->launches += 1;
         tree_moments<false, false><<<blocks, kThreads, 0, c->stream>>>(c->scal, b.pos, b.mass,

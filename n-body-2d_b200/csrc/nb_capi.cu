@@ -264,8 +264,18 @@ void enqueue_step(nb_ctx* c, int parity, bool integrate, bool store_acc, bool ti
     if (split) cudaStreamWaitEvent(c->stream, c->join_ev, 0);
     mark(6);
     if (split && (c->p.flags & NB_FLAG_LEARNED)) {
+        // the features need only the monopoles, and only the correction reads
+        // them: they are built on the side stream while the walk runs
+        cudaEventRecord(c->feat_fork_ev, c->stream);
+        cudaStreamWaitEvent(c->side_stream, c->feat_fork_ev, 0);
+        cudaStream_t main_stream = c->stream;
+        c->stream = c->side_stream;
+        nb::launch_features(c, B);
+        c->stream = main_stream;
+        cudaEventRecord(c->feat_join_ev, c->side_stream);
         nb::launch_force_split(c, B, integrate, store_acc);  // FP32 accelerations + band lists
         mark(7);
+        cudaStreamWaitEvent(c->stream, c->feat_join_ev, 0);
         nb::launch_mlp_correct(c, B, integrate, store_acc);  // learned term, kick, drift
     } else if (split) {
         nb::launch_force_split(c, B, integrate, store_acc);  // kick and drift fused
@@ -407,6 +417,8 @@ int create_context(const nb_params* p, uint64_t n, const double* mass, const dou
         cudaStreamCreateWithFlags(&c->side_stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&c->fork_ev, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&c->join_ev, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->feat_fork_ev, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->feat_join_ev, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&c->staged, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&c->copied, cudaEventDisableTiming) != cudaSuccess) {
         rc = NB_ERR_CUDA;
@@ -463,6 +475,8 @@ int nb_destroy(nb_ctx* c) {
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     if (c->fork_ev) cudaEventDestroy(c->fork_ev);
     if (c->join_ev) cudaEventDestroy(c->join_ev);
+    if (c->feat_fork_ev) cudaEventDestroy(c->feat_fork_ev);
+    if (c->feat_join_ev) cudaEventDestroy(c->feat_join_ev);
     if (c->side_stream) cudaStreamDestroy(c->side_stream);
     if (c->up_ready) cudaEventDestroy(c->up_ready);
     if (c->up_used) cudaEventDestroy(c->up_used);
@@ -894,6 +908,7 @@ int nb_mlp_samples(nb_ctx* c, uint64_t ntargets, uint64_t seed, uint64_t capacit
     nb::launch_gather(c, A, B, c->tree.body4);
     nb::launch_tree(c, B);
     nb::launch_moments(c, B, true);
+    nb::launch_features(c, B);
     nb::launch_groups(c);
     NB_CUDA(c, cudaGetLastError());
     c->parity ^= 1;

@@ -152,6 +152,7 @@ struct nb_ctx {
     cudaStream_t copy_stream = nullptr;  // nb_download_async: device-to-host copies
     cudaStream_t side_stream = nullptr;  // the target groups, built while the moments run
     cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
+    cudaEvent_t feat_fork_ev = nullptr, feat_join_ev = nullptr;  // learned features beside the walk
     cudaEvent_t staged = nullptr;        // the download's scatter into the staging buffers is done
     cudaEvent_t copied = nullptr;        // the staging buffers have been copied out (free again)
     cudaStream_t up_stream = nullptr;    // nb_upload_async: host-to-device copies
@@ -219,6 +220,8 @@ unsigned sort_timeout_probe(cudaStream_t st);                                   
 void launch_gather(nb_ctx* c, const BodyBuffers& src, const BodyBuffers& dst, float4* body4);
 void launch_tree(nb_ctx* c, const BodyBuffers& b);
 void launch_moments(nb_ctx* c, const BodyBuffers& b, bool split);
+// learned mode: second and third moments and the BF16 feature records
+void launch_features(nb_ctx* c, const BodyBuffers& b);
 int split_group_size(const nb_ctx* c);   // bodies per SPLIT traversal group
 void launch_mlp_correct(nb_ctx* c, const BodyBuffers& b, bool kick, bool store_acc);
 size_t mlp_infer_bytes();
