@@ -192,8 +192,8 @@ NB_API int nb_upload(nb_ctx* ctx, const double* mass, const double* pos_xy, cons
  * enqueued before the call sees the old state, work enqueued after it the
  * new one.  The bodies are checked on the device as they are moved into the
  * state; a rejected set leaves the state unchanged and the next nb_sync or
- * nb_download_wait returns NB_ERR_INVALID.  The staging area (40 bytes per
- * body) is allocated by the first call.  mass / pos_xy / vel_xy must stay
+ * nb_download_wait returns NB_ERR_INVALID.  Two staging areas (40 bytes per
+ * body each, used in turn) are allocated by the first call.  mass / pos_xy / vel_xy must stay
  * valid and unchanged, and be pinned for the copy to be asynchronous, until
  * nb_sync returns.  No counterpart in the reference, which uploads once at
  * start-up (BarnesHutCuda.cu:596-605). */

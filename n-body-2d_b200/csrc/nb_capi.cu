@@ -154,9 +154,11 @@ void free_all(nb_ctx* c) {
     cudaFree(c->acc);
     cudaFree(c->stage_pos);
     cudaFree(c->stage_vel);
-    cudaFree(c->up_mass);
-    cudaFree(c->up_pos);
-    cudaFree(c->up_vel);
+    for (auto& u : c->up) {
+        cudaFree(u.mass);
+        cudaFree(u.pos);
+        cudaFree(u.vel);
+    }
     cudaFree(c->ap_partial);
     cudaFree(c->render_count);
     cudaFree(c->render_rgba);
@@ -478,8 +480,10 @@ int nb_destroy(nb_ctx* c) {
     if (c->feat_fork_ev) cudaEventDestroy(c->feat_fork_ev);
     if (c->feat_join_ev) cudaEventDestroy(c->feat_join_ev);
     if (c->side_stream) cudaStreamDestroy(c->side_stream);
-    if (c->up_ready) cudaEventDestroy(c->up_ready);
-    if (c->up_used) cudaEventDestroy(c->up_used);
+    for (auto& u : c->up) {
+        if (u.ready) cudaEventDestroy(u.ready);
+        if (u.used) cudaEventDestroy(u.used);
+    }
     if (c->up_stream) cudaStreamDestroy(c->up_stream);
     for (auto& e : c->phase_ev)
         if (e) cudaEventDestroy(e);
@@ -512,56 +516,59 @@ int nb_upload(nb_ctx* c, const double* mass, const double* pos_xy, const double*
     return NB_OK;
 }
 
-// Staging area and stream are made on first use; a failed set-up leaves the
-// context as it was and nb_upload still works.
+// Staging areas and stream are made on first use; a failed set-up leaves the
+// context as it was and nb_upload still works.  Two areas are used in turn, so
+// an upload's copy can start while the previous one waits for the step before
+// it to finish.
 int nb_upload_async(nb_ctx* c, const double* mass, const double* pos_xy, const double* vel_xy) {
     if (!c || !mass || !pos_xy || !vel_xy) return NB_ERR_INVALID;
     const size_t n = (size_t)c->n;
     DeviceGuard guard(c->device);
     if (!c->up_stream) {
         cudaStream_t st = nullptr;
-        cudaEvent_t ready = nullptr, used = nullptr;
-        double* m = nullptr;
-        double2 *p = nullptr, *v = nullptr;
-        if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess ||
-            cudaEventCreateWithFlags(&ready, cudaEventDisableTiming) != cudaSuccess ||
-            cudaEventCreateWithFlags(&used, cudaEventDisableTiming) != cudaSuccess ||
-            dalloc(&m, n) != cudaSuccess || dalloc(&p, n) != cudaSuccess ||
-            dalloc(&v, n) != cudaSuccess) {
-            cudaFree(m);
-            cudaFree(p);
-            cudaFree(v);
-            if (ready) cudaEventDestroy(ready);
-            if (used) cudaEventDestroy(used);
+        nb_ctx::UploadSlot slot[2];
+        bool ok = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) == cudaSuccess;
+        for (auto& u : slot)
+            ok = ok && cudaEventCreateWithFlags(&u.ready, cudaEventDisableTiming) == cudaSuccess &&
+                 cudaEventCreateWithFlags(&u.used, cudaEventDisableTiming) == cudaSuccess &&
+                 dalloc(&u.mass, n) == cudaSuccess && dalloc(&u.pos, n) == cudaSuccess &&
+                 dalloc(&u.vel, n) == cudaSuccess;
+        if (!ok) {
+            for (auto& u : slot) {
+                cudaFree(u.mass);
+                cudaFree(u.pos);
+                cudaFree(u.vel);
+                if (u.ready) cudaEventDestroy(u.ready);
+                if (u.used) cudaEventDestroy(u.used);
+            }
             if (st) cudaStreamDestroy(st);
             cudaGetLastError();
-            return fail(c, NB_ERR_NOMEM, "no device memory for the upload staging area");
+            return fail(c, NB_ERR_NOMEM, "no device memory for the upload staging areas");
         }
         c->up_stream = st;
-        c->up_ready = ready;
-        c->up_used = used;
-        c->up_mass = m;
-        c->up_pos = p;
-        c->up_vel = v;
+        c->up[0] = slot[0];
+        c->up[1] = slot[1];
+        c->up_next = 0;
     }
-    // the staging area is free once the previous asynchronous upload has
-    // been moved into the state
-    NB_CUDA(c, cudaStreamWaitEvent(c->up_stream, c->up_used, 0));
-    NB_CUDA(c, cudaMemcpyAsync(c->up_mass, mass, n * sizeof(double), cudaMemcpyHostToDevice,
+    nb_ctx::UploadSlot& u = c->up[c->up_next];
+    c->up_next ^= 1;
+    // the area is free once the upload that used it before has been moved
+    // into the state
+    NB_CUDA(c, cudaStreamWaitEvent(c->up_stream, u.used, 0));
+    NB_CUDA(c, cudaMemcpyAsync(u.mass, mass, n * sizeof(double), cudaMemcpyHostToDevice,
                                c->up_stream));
-    NB_CUDA(c, cudaMemcpyAsync(c->up_pos, pos_xy, n * sizeof(double2), cudaMemcpyHostToDevice,
+    NB_CUDA(c, cudaMemcpyAsync(u.pos, pos_xy, n * sizeof(double2), cudaMemcpyHostToDevice,
                                c->up_stream));
-    NB_CUDA(c, cudaMemcpyAsync(c->up_vel, vel_xy, n * sizeof(double2), cudaMemcpyHostToDevice,
+    NB_CUDA(c, cudaMemcpyAsync(u.vel, vel_xy, n * sizeof(double2), cudaMemcpyHostToDevice,
                                c->up_stream));
-    NB_CUDA(c, cudaEventRecord(c->up_ready, c->up_stream));
+    NB_CUDA(c, cudaEventRecord(u.ready, c->up_stream));
     // everything enqueued before this call still sees the old state
-    NB_CUDA(c, cudaStreamWaitEvent(c->stream, c->up_ready, 0));
+    NB_CUDA(c, cudaStreamWaitEvent(c->stream, u.ready, 0));
     const nb::BodyBuffers keep = c->buf[c->parity];
     c->parity = 0;
-    nb::launch_upload_commit(c, c->up_mass, c->up_pos, c->up_vel, keep, c->buf[0],
-                             &c->scal->upload_bad);
+    nb::launch_upload_commit(c, u.mass, u.pos, u.vel, keep, c->buf[0], &c->scal->upload_bad);
     NB_CUDA(c, cudaGetLastError());
-    NB_CUDA(c, cudaEventRecord(c->up_used, c->stream));
+    NB_CUDA(c, cudaEventRecord(u.used, c->stream));
     return NB_OK;
 }
 

@@ -156,8 +156,6 @@ struct nb_ctx {
     cudaEvent_t staged = nullptr;        // the download's scatter into the staging buffers is done
     cudaEvent_t copied = nullptr;        // the staging buffers have been copied out (free again)
     cudaStream_t up_stream = nullptr;    // nb_upload_async: host-to-device copies
-    cudaEvent_t up_ready = nullptr;      // the staged upload has arrived on the device
-    cudaEvent_t up_used = nullptr;       // it has been moved into the state (staging free again)
     cudaEvent_t phase_ev[nb::kPhases + 1] = {};
     int parity = 0;                 // which BodyBuffers holds the state
     nb::BodyBuffers buf[2];
@@ -183,9 +181,15 @@ struct nb_ctx {
     double2* acc = nullptr;              // optional FP64 accelerations (sorted order)
     double2* stage_pos = nullptr;        // original-order staging for downloads
     double2* stage_vel = nullptr;
-    double* up_mass = nullptr;           // nb_upload_async staging, allocated on first use
-    double2* up_pos = nullptr;
-    double2* up_vel = nullptr;
+    // nb_upload_async staging, two areas used in turn (allocated on first use)
+    struct UploadSlot {
+        double* mass = nullptr;
+        double2* pos = nullptr;
+        double2* vel = nullptr;
+        cudaEvent_t ready = nullptr;     // the staged bodies have arrived on the device
+        cudaEvent_t used = nullptr;      // they have been moved into the state (area free again)
+    } up[2];
+    int up_next = 0;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};  // one step from parity 0 / 1
     double graph_dt = 0.0;
     uint64_t steps = 0;
