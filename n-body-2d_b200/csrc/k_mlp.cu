@@ -12,10 +12,12 @@
 // cells (d ~ eps) have residuals that depend on it far more than on any
 // higher moment.
 //
-// Tensor-core layout: mma.sync m16n8k16 BF16 with FP32 accumulators.  A 16-row
-// tile (16 samples, or 16 cells of one target group) runs through the three
-// layers in registers; the accumulator fragment of one layer is, element for
-// element, the A fragment of the next, so no shuffles are needed.
+// Tensor-core layout: mma.sync m16n8k16 BF16 with FP32 accumulators for
+// training and for the step's correction.  A 16-row tile (16 samples, or 16
+// cells of one target group) runs through the three layers in registers; the
+// accumulator fragment of one layer is, element for element, the A fragment of
+// the next, so no shuffles are needed.  Bulk evaluation (nb_mlp_forward) runs
+// on tcgen05 in 128-row tiles (mlp_forward_tc, further down).
 //
 // Inference is per target group: the traversal lists each group's band cells;
 // mlp_correct_kick evaluates the MLP at the group's centre for all of them in
