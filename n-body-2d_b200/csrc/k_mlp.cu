@@ -835,7 +835,8 @@ mlp_correct_kick(const InferW* __restrict__ Wg, Tree t, const DeviceScalars* __r
 // The step's correction (mlp_correct_kick) stays on mma.sync: there every
 // warp feeds its own group's 32 band cells at a time, and the three MMA round
 // trips and barriers a 128-row tile needs made it slower (0.83 against
-// 0.64 ms at 4M bodies, measured), while bulk evaluation fills whole tiles.
+// 0.64 ms at 4M bodies, measured; 1.04 ms with two tiles in flight per CTA),
+// while bulk evaluation fills whole tiles.
 //
 // Shared-memory operands use the no-swizzle K-major layout of 8-row x 16-byte
 // core matrices: element (row, k) of an operand with K columns sits at byte
