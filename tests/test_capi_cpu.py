@@ -52,6 +52,14 @@ def test_invalid_arguments_rejected_before_any_device_call(nbp):
     assert lib.nb_create(C.byref(p), 0, one, one, one, C.byref(h)) == 1
     assert lib.nb_create(None, 1, one, one, one, C.byref(h)) == 1
     assert lib.nb_destroy(None) == 0
+    # context calls with no context, and empty or missing arrays
+    assert lib.nb_upload_async(None, one, one, one) == 1
+    assert lib.nb_download_async(None, one, one) == 1
+    params = (C.c_float * nbp.NB_MLP_PARAMS)()
+    feats = (C.c_float * 12)()
+    out = (C.c_float * 2)()
+    assert lib.nb_mlp_forward(0, params, 0, feats, out) == 1
+    assert lib.nb_mlp_forward(0, None, 1, feats, out) == 1
 
 
 def test_batch_create_rejects_bad_batches_before_any_device_call(nbp):

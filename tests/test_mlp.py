@@ -44,6 +44,23 @@ def test_forward_matches_oracle(nbp):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("n", [1, 5, 127, 128, 129, 255])
+def test_forward_ragged_tiles(nbp, n):
+    """Tiles of 128 rows with empty rows: each row's output depends on its
+    own features only, so any n gives the rows of a larger batch."""
+    from oracle import mlp_oracle as mo
+
+    p = mo.init(3).astype(np.float32)
+    X = _data(4, 256)
+    y_all = nbp.mlp_forward(p, X)
+    y = nbp.mlp_forward(p, X[:n])
+    assert y.shape == (n, 2) and np.isfinite(y).all()
+    assert np.array_equal(y, y_all[:n])
+    y_o, _ = mo.forward(p, X[:n])
+    assert np.abs(y - y_o).max() < 2e-2 * max(1.0, np.abs(y_o).max())
+
+
+@pytest.mark.gpu
 def test_gradients_match_oracle(nbp):
     from oracle import mlp_oracle as mo
 
