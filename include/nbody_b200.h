@@ -227,6 +227,25 @@ NB_API int nb_debug_state(nb_ctx* ctx, double* mass, double* pos_xy, double* vel
 NB_API int nb_debug_tree(nb_ctx* ctx, double* cell_mass, double* cell_com_xy, int32_t* level,
                   int32_t* first_body, int32_t* last_body, int32_t* root_ref);
 
+/* Debug view of the FP64 force pass (NB_MODE_FP64 only): runs the force pass
+ * of the current state without integrating, as nb_accelerations does, and
+ * writes each body's interaction counts in original order -- cell_terms[i]
+ * monopole terms of cells and multi-body leaves, body_terms[i] body-body terms
+ * (the per-body counterparts of the counters the reference keeps implicitly in
+ * its DFS, BarnesHutCuda.cu:382-486) -- and the deepest traversal stack any
+ * body used (entries; the bound is 96, the reference's is 32, CU:400).  Any
+ * pointer may be NULL.  The first call allocates 8 bytes per body. */
+NB_API int nb_debug_interactions(nb_ctx* ctx, uint32_t* cell_terms, uint32_t* body_terms,
+                                 int32_t* stack_high_water);
+
+/* Debug view of the SPLIT traversal's target groups of the last step (no
+ * counterpart in the reference, which walks the tree once per body): *count
+ * receives the number of groups, and the first min(count, capacity) groups'
+ * first and last body slots (device order) go to first_body / last_body
+ * (either may be NULL).  NB_MODE_SPLIT only. */
+NB_API int nb_debug_groups(nb_ctx* ctx, int32_t* first_body, int32_t* last_body, uint64_t capacity,
+                           uint64_t* count);
+
 NB_API int nb_get_stats(nb_ctx* ctx, nb_stats* out);
 
 /* Device time of each phase of the most recent graph-launched step, from CUDA
@@ -317,11 +336,13 @@ NB_API int nb_mlp_train(int32_t device, uint64_t n, const float* features, const
  * {x_min, x_max, y_min, y_max}.  Returns once the work is enqueued.
  *
  * Calls no cudaMalloc/cudaFree: the scratch is a static device array in the
- * library (NB_STATIC_SORT_MAX_BODIES x 24 bytes + about 20 KB on every GPU
- * that loads it, held until exit).  n above NB_STATIC_SORT_MAX_BODIES is
+ * library (NB_STATIC_SORT_MAX_BODIES x 24 bytes + about 100 KB, 6.4 MB in all,
+ * on every GPU that loads it, held until exit).  n above NB_STATIC_SORT_MAX_BODIES is
  * rejected with NB_ERR_CAPACITY, n == 0 or a NULL pointer with
- * NB_ERR_INVALID.  The first call on a device looks up the array's device
- * address, so make it before any stream capture.  All calls on a device share
+ * NB_ERR_INVALID.  Every call looks up the array's device address in the
+ * current context (so a cudaDeviceReset in between is harmless); the first
+ * call on a device also loads the library's device image, so make it before
+ * any stream capture.  All calls on a device share
  * the scratch: calls that overlap on the GPU race and must be serialised by
  * the caller. */
 NB_API int nb_morton_sort_static(const double* pos_xy, uint64_t n, uint64_t* codes,

@@ -38,7 +38,7 @@ EXPORTS = (
     "nb_allpairs_accelerations", "nb_phase_times", "nb_phase_name", "nb_morton_sort_static",
     "nb_set_mlp_weights", "nb_mlp_samples", "nb_mlp_forward", "nb_mlp_loss_grad", "nb_mlp_train",
     "nb_batch_create", "nb_autotune", "nb_render", "nb_download_async", "nb_download_wait",
-    "nb_debug_wait_timeout", "nb_upload_async",
+    "nb_debug_wait_timeout", "nb_upload_async", "nb_debug_interactions", "nb_debug_groups",
 )
 
 
@@ -125,6 +125,8 @@ def load() -> C.CDLL:
     lib.nb_debug_state.argtypes = [_P, _P, _P, _P, _P]
     lib.nb_debug_tree.argtypes = [_P, _P, _P, _P, _P, _P, _P]
     lib.nb_get_stats.argtypes = [_P, C.POINTER(NbStats)]
+    lib.nb_debug_interactions.argtypes = [_P, _P, _P, _P]
+    lib.nb_debug_groups.argtypes = [_P, _P, _P, C.c_uint64, _P]
     lib.nb_last_error.argtypes = [_P]
     lib.nb_last_error.restype = C.c_char_p
     lib.nb_status_string.argtypes = [C.c_int]

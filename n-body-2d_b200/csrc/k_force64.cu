@@ -37,18 +37,20 @@ __device__ __forceinline__ void plummer(double dx, double dy, double m, double e
 __global__ void __launch_bounds__(kThreads)
 force_fp64(const double2* __restrict__ pos, const double* __restrict__ mass, double2* __restrict__ vel,
            double2* __restrict__ acc_out, int n, Tree t, DeviceScalars* __restrict__ s, double eps2,
-           double theta_sq, double G_dt, int kick) {
+           double theta_sq, double G_dt, int kick, uint2* __restrict__ terms_out) {
     __shared__ double wsq[kMaxLevel + 1];
     if (threadIdx.x <= kMaxLevel) wsq[threadIdx.x] = s->wsq[threadIdx.x];
     __syncthreads();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int cells = s->cells;
     unsigned long long ncell = 0, pairs = 0;
+    int deepest = 0;  // stack entries in use after the fullest push
     if (i < n) {
         const double2 me = pos[i];
         double ax = 0.0, ay = 0.0;
         int stack[kStackDepth];
         int top = 0;
+        deepest = 1;
         stack[0] = s->root;
         while (top >= 0) {
             const int ref = stack[top--];
@@ -78,6 +80,7 @@ force_fp64(const double2* __restrict__ pos, const double* __restrict__ mass, dou
                 if (ch.z != INT_MIN) stack[++top] = ch.z;
                 if (ch.y != INT_MIN) stack[++top] = ch.y;
                 stack[++top] = ch.x;
+                deepest = max(deepest, top + 1);
                 continue;
             }
             const int b = ~ref;
@@ -117,6 +120,7 @@ force_fp64(const double2* __restrict__ pos, const double* __restrict__ mass, dou
             }
         }
         if (acc_out) acc_out[i] = make_double2(ax, ay);
+        if (terms_out) terms_out[i] = make_uint2((unsigned)ncell, (unsigned)pairs);
         if (kick) {
             double2 v = vel[i];
             v.x += ax * G_dt;
@@ -127,10 +131,12 @@ force_fp64(const double2* __restrict__ pos, const double* __restrict__ mass, dou
     for (int o = 16; o > 0; o >>= 1) {
         ncell += __shfl_xor_sync(kFull, ncell, o);
         pairs += __shfl_xor_sync(kFull, pairs, o);
+        deepest = max(deepest, __shfl_xor_sync(kFull, deepest, o));
     }
     if ((threadIdx.x & 31) == 0) {
         atomicAdd(&s->cell_terms, ncell);
         atomicAdd(&s->body_terms, pairs);
+        atomicMax(&s->stack_hw, deepest);
     }
 }
 
@@ -217,7 +223,7 @@ void launch_force_fp64(nb_ctx* c, const BodyBuffers& b, bool kick, bool store_ac
     c->launches += 1;
     force_fp64<<<blocks_for(c->n, kThreads), kThreads, 0, c->stream>>>(
         b.pos, b.mass, b.vel, store_acc ? c->acc : nullptr, (int)c->n, c->tree, c->scal,
-        c->p.epsilon_squared, theta_sq, G_dt, kick ? 1 : 0);
+        c->p.epsilon_squared, theta_sq, G_dt, kick ? 1 : 0, c->want_terms ? c->dbg_terms : nullptr);
 }
 
 void launch_drift(nb_ctx* c, const BodyBuffers& b) {

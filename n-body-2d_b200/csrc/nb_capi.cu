@@ -152,6 +152,7 @@ void free_all(nb_ctx* c) {
     cudaFree(c->scal);
     cudaFree(c->bbox_partials);
     cudaFree(c->acc);
+    cudaFree(c->dbg_terms);
     cudaFree(c->stage_pos);
     cudaFree(c->stage_vel);
     for (auto& u : c->up) {
@@ -230,7 +231,8 @@ void enqueue_step(nb_ctx* c, int parity, bool integrate, bool store_acc, bool ti
         if (timed) cudaEventRecordWithFlags(c->phase_ev[k], c->stream, cudaEventRecordExternal);
     };
     mark(0);
-    cudaMemsetAsync(&c->scal->cell_terms, 0, 2 * sizeof(unsigned long long), c->stream);
+    // cell_terms, body_terms and stack_hw start every force pass at zero
+    cudaMemsetAsync(&c->scal->cell_terms, 0, 3 * sizeof(unsigned long long), c->stream);
     if (c->p.mode == NB_MODE_ALLPAIRS) {
         // AllPairsSim: drift into the other buffer, then the all-pairs kick there
         for (int k = 1; k < 7; ++k) mark(k);
@@ -713,6 +715,60 @@ int nb_debug_morton(nb_ctx* c, uint64_t* codes, int32_t* order, double* box_out)
                                    c->stream));
     NB_CUDA(c, cudaStreamSynchronize(c->stream));
     return read_device_error(c);
+}
+
+int nb_debug_interactions(nb_ctx* c, uint32_t* cell_terms, uint32_t* body_terms,
+                          int32_t* stack_high_water) {
+    if (!c) return NB_ERR_INVALID;
+    if (c->p.mode != NB_MODE_FP64)
+        return fail(c, NB_ERR_INVALID, "per-body interaction counts come from the FP64 walk");
+    DeviceGuard guard(c->device);
+    const size_t n = (size_t)c->n;
+    if (!c->dbg_terms) NB_CUDA(c, dalloc(&c->dbg_terms, n));
+    c->want_terms = true;
+    enqueue_step(c, c->parity, false, false);
+    c->want_terms = false;
+    NB_CUDA(c, cudaGetLastError());
+    c->parity ^= 1;
+    std::vector<uint2> terms(n);
+    std::vector<int32_t> orig(n);
+    NB_CUDA(c, cudaMemcpyAsync(terms.data(), c->dbg_terms, n * sizeof(uint2), cudaMemcpyDeviceToHost,
+                               c->stream));
+    NB_CUDA(c, cudaMemcpyAsync(orig.data(), c->buf[c->parity].orig, n * sizeof(int32_t),
+                               cudaMemcpyDeviceToHost, c->stream));
+    nb::DeviceScalars s;
+    NB_CUDA(c, cudaMemcpyAsync(&s, c->scal, sizeof(s), cudaMemcpyDeviceToHost, c->stream));
+    NB_CUDA(c, cudaStreamSynchronize(c->stream));
+    for (size_t i = 0; i < n; ++i) {
+        const int32_t o = orig[i];
+        if (o < 0 || (size_t)o >= n) return fail(c, NB_ERR_CUDA, "corrupt body permutation");
+        if (cell_terms) cell_terms[o] = terms[i].x;
+        if (body_terms) body_terms[o] = terms[i].y;
+    }
+    if (stack_high_water) *stack_high_water = s.stack_hw;
+    return read_device_error(c);
+}
+
+int nb_debug_groups(nb_ctx* c, int32_t* first_body, int32_t* last_body, uint64_t capacity,
+                    uint64_t* count) {
+    if (!c || !count) return NB_ERR_INVALID;
+    if (c->p.mode != NB_MODE_SPLIT)
+        return fail(c, NB_ERR_INVALID, "target groups exist only in SPLIT mode");
+    DeviceGuard guard(c->device);
+    NB_CUDA(c, cudaStreamSynchronize(c->stream));
+    nb::DeviceScalars s;
+    NB_CUDA(c, cudaMemcpy(&s, c->scal, sizeof(s), cudaMemcpyDeviceToHost));
+    *count = (uint64_t)(s.groups > 0 ? s.groups : 0);
+    const size_t m = (size_t)std::min<uint64_t>(*count, capacity);
+    if (m && (first_body || last_body)) {
+        std::vector<int2> g(m);
+        NB_CUDA(c, cudaMemcpy(g.data(), c->tree.groups, m * sizeof(int2), cudaMemcpyDeviceToHost));
+        for (size_t k = 0; k < m; ++k) {
+            if (first_body) first_body[k] = g[k].x;
+            if (last_body) last_body[k] = g[k].y;
+        }
+    }
+    return NB_OK;
 }
 
 int nb_debug_state(nb_ctx* c, double* mass, double* pos_xy, double* vel_xy, int32_t* orig) {

@@ -40,6 +40,8 @@ struct DeviceScalars {
     unsigned bbox_ticket;     // last-block-done counter of the bbox reduction
     unsigned long long cell_terms;
     unsigned long long body_terms;
+    int32_t stack_hw;         // FP64 walk: deepest stack (entries) of the last force pass
+    int32_t stack_pad_;
     int32_t nstart;           // cells whose children are all leaves (climb starts)
     unsigned upload_bad;      // nb_upload's checks: bit 0 non-finite, bit 1 mass <= 0
 };
@@ -179,6 +181,8 @@ struct nb_ctx {
     nb::Batch batch;                     // batched universes (nuni > 0)
     int bpl = 2;                         // SPLIT: bodies per lane (group of 32 x bpl)
     double2* acc = nullptr;              // optional FP64 accelerations (sorted order)
+    uint2* dbg_terms = nullptr;          // nb_debug_interactions: per-body {cell, body} terms
+    bool want_terms = false;             // the force pass writes dbg_terms
     double2* stage_pos = nullptr;        // original-order staging for downloads
     double2* stage_vel = nullptr;
     // nb_upload_async staging, two areas used in turn (allocated on first use)

@@ -11,14 +11,13 @@
 // of cudaMalloc'd memory.
 //
 // The array is part of the library image, so every GPU that loads the library
-// holds it (NB_STATIC_SORT_MAX_BODIES x 24 bytes plus about 20 KB) until the
-// process exits.  All calls on a device share it and it keeps the contents of
+// holds it (NB_STATIC_SORT_MAX_BODIES x 24 bytes plus about 100 KB of per-tile
+// digit counts and reduction partials: 6.4 MB in all) until the process
+// exits.  All calls on a device share it and it keeps the contents of
 // the last call; calls that overlap on the GPU (two streams, or two host
 // threads) race on it and must be serialised by the caller.
 #include <cuda_runtime.h>
 #include <stdint.h>
-
-#include <mutex>
 
 #include "nb_internal.cuh"
 
@@ -27,7 +26,6 @@ namespace {
 constexpr int64_t kMaxBodies = NB_STATIC_SORT_MAX_BODIES;
 constexpr int kMaxTiles = (int)((kMaxBodies + nb::kSortTile - 1) / nb::kSortTile);
 constexpr int kBoxBlocks = 256;
-constexpr int kMaxDevices = 64;
 
 // Scratch layout (all offsets multiples of 256 bytes).
 constexpr size_t kKeyBytes = sizeof(uint64_t) * kMaxBodies;
@@ -41,6 +39,8 @@ constexpr size_t kOffTotals = kOffCounts + sizeof(uint32_t) * 256 * kMaxTiles;
 constexpr size_t kOffPartials = kOffTotals + sizeof(uint32_t) * 256;
 constexpr size_t kOffScalars = kOffPartials + sizeof(double) * 4 * kBoxBlocks;
 constexpr size_t kScratchBytes = kOffScalars + ((sizeof(nb::DeviceScalars) + 255) / 256) * 256;
+static_assert(kScratchBytes - kOffCounts < 100 * 1024 && kScratchBytes < 6400 * 1000,
+              "the documented size of the scratch array (6.4 MB, ~100 KB beyond the keys) is stale");
 static_assert(kOffKey1 % 256 == 0 && kOffVal0 % 256 == 0 && kOffVal1 % 256 == 0 &&
                   kOffCounts % 256 == 0 && kOffTotals % 256 == 0 && kOffPartials % 256 == 0 &&
                   kOffScalars % 256 == 0,
@@ -48,22 +48,17 @@ static_assert(kOffKey1 % 256 == 0 && kOffVal0 % 256 == 0 && kOffVal1 % 256 == 0 
 
 static __device__ __align__(256) unsigned char g_sort_scratch[kScratchBytes];
 
-std::mutex g_setup_mutex;
-unsigned char* g_scratch_addr[kMaxDevices] = {};
-
-// Device address of the scratch array on the current device, looked up once
-// per device (host code only sees a host-side stand-in for the symbol).
+// Device address of the scratch array in the current device's context.  Host
+// code only holds a host-side stand-in for the symbol, so the address is
+// asked for on every call: a cached value would go stale after
+// cudaDeviceReset or under another context, and the lookup is cheap once the
+// library's device image is loaded (the first call on a device loads it).
 int scratch_for_current_device(unsigned char** out) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return NB_ERR_NOTFOUND;
-    if (dev < 0 || dev >= kMaxDevices) return NB_ERR_NOTFOUND;
-    std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_addr[dev]) {
-        void* p = nullptr;
-        if (cudaGetSymbolAddress(&p, g_sort_scratch) != cudaSuccess || !p) return NB_ERR_CUDA;
-        g_scratch_addr[dev] = static_cast<unsigned char*>(p);
-    }
-    *out = g_scratch_addr[dev];
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_sort_scratch) != cudaSuccess || !p) return NB_ERR_CUDA;
+    *out = static_cast<unsigned char*>(p);
     return NB_OK;
 }
 

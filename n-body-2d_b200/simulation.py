@@ -225,6 +225,28 @@ class NbContext:
         return dict(mass=cm[:m], com=cc[:m], level=lv[:m], first=fb[:m], last=lb[:m],
                     root=root.value)
 
+    def debug_interactions(self):
+        """FP64 mode: per-body (cell terms, body terms) of a force pass of the
+        current state, in original order, and the deepest stack it used."""
+        cells = np.empty(self.n, dtype=np.uint32)
+        bodies = np.empty(self.n, dtype=np.uint32)
+        hw = C.c_int32()
+        check(self._lib.nb_debug_interactions(self.handle, ptr(cells), ptr(bodies),
+                                              C.addressof(hw)), self._h)
+        return cells, bodies, hw.value
+
+    def debug_groups(self) -> np.ndarray:
+        """SPLIT mode: [groups, 2] first and last body slot of each target group
+        of the last step (device order)."""
+        cnt = C.c_uint64()
+        check(self._lib.nb_debug_groups(self.handle, None, None, 0, C.byref(cnt)), self._h)
+        k = cnt.value
+        first = np.empty(max(k, 1), dtype=np.int32)
+        last = np.empty(max(k, 1), dtype=np.int32)
+        check(self._lib.nb_debug_groups(self.handle, ptr(first), ptr(last), k, C.byref(cnt)),
+              self._h)
+        return np.stack([first[:k], last[:k]], axis=1)
+
     def phase_times(self) -> dict[str, float]:
         """Per-phase device ms of the last graph-launched step."""
         ms = np.zeros(16)

@@ -54,6 +54,10 @@ def load():
                                      C.c_double, C.c_double, C.c_int, _P, _P, _P, C.c_int,
                                      C.POINTER(Stats)]
         lib.orc_ref_step.restype = C.c_int
+        lib.orc_ref_walk_targets.argtypes = [C.c_int64, _P, _P, _P, _P, C.c_double, C.c_double,
+                                             C.c_int64, _P, _P, _P, _P, _P, C.c_int,
+                                             C.POINTER(Stats)]
+        lib.orc_ref_walk_targets.restype = C.c_int
         lib.orc_allpairs_plummer.argtypes = [C.c_int64, _P, _P, C.c_int64, _P, C.c_double, _P,
                                              C.c_int]
         lib.orc_allpairs_plummer_abs.argtypes = [C.c_int64, _P, _P, C.c_int64, _P, C.c_double,
@@ -126,6 +130,27 @@ class RefState:
         if rc != 0:
             raise MemoryError("oracle step failed to allocate")
         return dict(acc=acc, codes=codes, order=order, stats=st.as_dict())
+
+    def walk_targets(self, targets, eps2=1e-4, theta=0.5, nthreads=None):
+        """Sorts the state as a step does (no integration) and walks only the
+        bodies whose original indices are `targets`: per target the FP64
+        acceleration, cell terms, body terms and deepest DFS stack."""
+        tgt = np.ascontiguousarray(targets, dtype=np.int64)
+        k = tgt.shape[0]
+        acc = np.empty((k, 2))
+        cells = np.empty(k, dtype=np.int64)
+        pairs = np.empty(k, dtype=np.int64)
+        stack = np.empty(k, dtype=np.int64)
+        st = Stats()
+        rc = load().orc_ref_walk_targets(self.n, _p(self.mass), _p(self.pos), _p(self.vel),
+                                         _p(self.orig), eps2, theta, k, _p(tgt), _p(acc),
+                                         _p(cells), _p(pairs), _p(stack), _threads(nthreads),
+                                         C.byref(st))
+        if rc == -2:
+            raise IndexError("target index outside [0, n)")
+        if rc != 0:
+            raise MemoryError("oracle walk failed to allocate")
+        return dict(acc=acc, cells=cells, pairs=pairs, stack=stack, stats=st.as_dict())
 
     def original_order(self):
         """(pos, vel, acc-permutation) mapped back to original body order."""

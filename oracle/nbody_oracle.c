@@ -319,18 +319,16 @@ static void body_force(const orc_tree* t, const double* pos, const double* mass,
 /* One step, in the order of BarnesHutCuda::simulate                          */
 /* (src/Simulation/src/BarnesHutCuda.cpp:30-40).                              */
 /* ------------------------------------------------------------------------ */
-int orc_ref_step(int64_t n, double* mass, double* pos, double* vel, int32_t* orig, double G,
-                 double dt, double eps2, double theta, int do_integrate, double* acc_out,
-                 uint64_t* codes_out, int32_t* order_out, int nthreads, orc_stats* st) {
-    if (n <= 0) return -1;
-#ifdef _OPENMP
-    if (nthreads > 0) omp_set_num_threads(nthreads);
-#else
-    (void)nthreads;
-#endif
-    orc_stats local;
-    memset(&local, 0, sizeof(local));
+static void free_tree(orc_tree* t) {
+    free(t->wsq); free(t->c0); free(t->bs); free(t->be); free(t->mass); free(t->cx); free(t->cy);
+}
 
+/* Stages 1-4 of a step, in place on device-order arrays: bbox, Morton codes,
+ * stable sort and gather (CU:648-711), the level-wise tree (CU:713-777) and
+ * the bottom-up COM (CU:787-807).  On success *t holds the tree (free it
+ * with free_tree). */
+static int build_ref_tree(int64_t n, double* mass, double* pos, double* vel, int32_t* orig,
+                          uint64_t* codes_out, int32_t* order_out, orc_tree* t, orc_stats* local) {
     /* 1. bounding box (CU:648-680) */
     orc_box box;
     orc_bbox_squared(n, pos, &box);
@@ -360,23 +358,22 @@ int orc_ref_step(int64_t n, double* mass, double* pos, double* vel, int32_t* ori
     free(order);
 
     /* 3. tree (CU:713-777) in a 5n node pool; the level lists live in one array */
-    orc_tree t;
-    t.cap = 5 * n;
-    t.wsq = (double*)malloc(sizeof(double) * (size_t)t.cap);
-    t.c0 = (int32_t*)malloc(sizeof(int32_t) * (size_t)t.cap);
-    t.bs = (int32_t*)malloc(sizeof(int32_t) * (size_t)t.cap);
-    t.be = (int32_t*)malloc(sizeof(int32_t) * (size_t)t.cap);
-    t.mass = (double*)malloc(sizeof(double) * (size_t)t.cap);
-    t.cx = (double*)malloc(sizeof(double) * (size_t)t.cap);
-    t.cy = (double*)malloc(sizeof(double) * (size_t)t.cap);
-    int32_t* lists = (int32_t*)malloc(sizeof(int32_t) * (size_t)t.cap);
-    if (!t.wsq || !t.c0 || !t.bs || !t.be || !t.mass || !t.cx || !t.cy || !lists) return -1;
+    t->cap = 5 * n;
+    t->wsq = (double*)malloc(sizeof(double) * (size_t)t->cap);
+    t->c0 = (int32_t*)malloc(sizeof(int32_t) * (size_t)t->cap);
+    t->bs = (int32_t*)malloc(sizeof(int32_t) * (size_t)t->cap);
+    t->be = (int32_t*)malloc(sizeof(int32_t) * (size_t)t->cap);
+    t->mass = (double*)malloc(sizeof(double) * (size_t)t->cap);
+    t->cx = (double*)malloc(sizeof(double) * (size_t)t->cap);
+    t->cy = (double*)malloc(sizeof(double) * (size_t)t->cap);
+    int32_t* lists = (int32_t*)malloc(sizeof(int32_t) * (size_t)t->cap);
+    if (!t->wsq || !t->c0 || !t->bs || !t->be || !t->mass || !t->cx || !t->cy || !lists) return -1;
     const double w = box.x_max - box.x_min;
-    t.wsq[0] = pow(w, 2.0); /* CU:717 */
-    t.c0[0] = -1;
-    t.bs[0] = 0;
-    t.be[0] = (int32_t)(n - 1);
-    t.alloc = 1;
+    t->wsq[0] = pow(w, 2.0); /* CU:717 */
+    t->c0[0] = -1;
+    t->bs[0] = 0;
+    t->be[0] = (int32_t)(n - 1);
+    t->alloc = 1;
     int64_t level_off[32], level_cnt[32];
     int nlev = 0;
     lists[0] = 0;
@@ -389,29 +386,47 @@ int orc_ref_step(int64_t n, double* mass, double* pos, double* vel, int32_t* ori
         const int64_t next_off = cur + cnt;
         int64_t next_cnt = 0;
         for (int64_t k = 0; k < cnt; ++k)
-            split_node(&t, sorted, lists[cur + k], level, lists + next_off, &next_cnt);
+            split_node(t, sorted, lists[cur + k], level, lists + next_off, &next_cnt);
         cur = next_off;
         cnt = next_cnt;
     }
-    local.levels = nlev;
-    local.nodes_allocated = t.alloc;
-    local.nodes_nonempty = cur;
+    free(sorted);
+    local->levels = nlev;
+    local->nodes_allocated = t->alloc;
+    local->nodes_nonempty = cur;
 
     /* 4. COM bottom-up (CU:787-807) */
     for (int lvl = nlev - 1; lvl >= 0; --lvl) {
         for (int64_t k = 0; k < level_cnt[lvl]; ++k) {
             const int32_t nid = lists[level_off[lvl] + k];
-            if (t.c0[nid] < 0) {
-                leaf_com(&t, pos, mass, nid, &local.multi_leaves);
-                if (lvl > local.max_level) local.max_level = lvl;
+            if (t->c0[nid] < 0) {
+                leaf_com(t, pos, mass, nid, &local->multi_leaves);
+                if (lvl > local->max_level) local->max_level = lvl;
             }
         }
         for (int64_t k = 0; k < level_cnt[lvl]; ++k) {
             const int32_t nid = lists[level_off[lvl] + k];
-            if (t.c0[nid] >= 0) internal_com(&t, nid);
+            if (t->c0[nid] >= 0) internal_com(t, nid);
         }
     }
     free(lists);
+    return 0;
+}
+
+int orc_ref_step(int64_t n, double* mass, double* pos, double* vel, int32_t* orig, double G,
+                 double dt, double eps2, double theta, int do_integrate, double* acc_out,
+                 uint64_t* codes_out, int32_t* order_out, int nthreads, orc_stats* st) {
+    if (n <= 0) return -1;
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#else
+    (void)nthreads;
+#endif
+    orc_stats local;
+    memset(&local, 0, sizeof(local));
+    orc_tree t;
+    memset(&t, 0, sizeof(t));
+    if (build_ref_tree(n, mass, pos, vel, orig, codes_out, order_out, &t, &local) != 0) return -1;
 
     /* 5. force + kick (CU:812-822, CU:484-485) */
     const double theta_sq = theta * theta;
@@ -443,8 +458,54 @@ int orc_ref_step(int64_t n, double* mass, double* pos, double* vel, int32_t* ori
             pos[2 * i + 1] = fma(vel[2 * i + 1], dt, pos[2 * i + 1]);
         }
 
-    free(t.wsq); free(t.c0); free(t.bs); free(t.be); free(t.mass); free(t.cx); free(t.cy);
-    free(sorted);
+    free_tree(&t);
+    if (st) *st = local;
+    return 0;
+}
+
+int orc_ref_walk_targets(int64_t n, double* mass, double* pos, double* vel, int32_t* orig,
+                         double eps2, double theta, int64_t k, const int64_t* targets,
+                         double* acc_out, int64_t* cells_out, int64_t* pairs_out,
+                         int64_t* stack_out, int nthreads, orc_stats* st) {
+    if (n <= 0 || k < 0) return -1;
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#else
+    (void)nthreads;
+#endif
+    for (int64_t q = 0; q < k; ++q)
+        if (targets[q] < 0 || targets[q] >= n) return -2;
+    orc_stats local;
+    memset(&local, 0, sizeof(local));
+    orc_tree t;
+    memset(&t, 0, sizeof(t));
+    if (build_ref_tree(n, mass, pos, vel, orig, NULL, NULL, &t, &local) != 0) return -1;
+    int32_t* slot = (int32_t*)malloc(sizeof(int32_t) * (size_t)n); /* original index -> slot */
+    if (!slot) return -1;
+    for (int64_t i = 0; i < n; ++i) slot[orig[i]] = (int32_t)i;
+    const double theta_sq = theta * theta;
+    int64_t cells = 0, pairs = 0, max_stack = 0;
+#pragma omp parallel for schedule(dynamic, 64) reduction(+ : cells, pairs) reduction(max : max_stack)
+    for (int64_t q = 0; q < k; ++q) {
+        double ax, ay;
+        int64_t c = 0, p = 0, ms = 0;
+        body_force(&t, pos, mass, slot[targets[q]], eps2, theta_sq, &ax, &ay, &c, &p, &ms);
+        if (acc_out) {
+            acc_out[2 * q] = ax;
+            acc_out[2 * q + 1] = ay;
+        }
+        if (cells_out) cells_out[q] = c;
+        if (pairs_out) pairs_out[q] = p;
+        if (stack_out) stack_out[q] = ms;
+        cells += c;
+        pairs += p;
+        if (ms > max_stack) max_stack = ms;
+    }
+    local.cell_interactions = cells;
+    local.body_interactions = pairs;
+    local.max_stack = max_stack;
+    free(slot);
+    free_tree(&t);
     if (st) *st = local;
     return 0;
 }

@@ -67,6 +67,23 @@ int orc_ref_step(int64_t n, double* mass, double* pos_xy, double* vel_xy, int32_
                  orc_stats* stats);
 
 /*
+ * The force pass of orc_ref_step for chosen targets only: stages 1-4 of the
+ * step (bbox, Morton, stable sort + gather, tree, COM; CU:648-809) run in
+ * place on the device-order arrays exactly as in orc_ref_step with
+ * do_integrate == 0, then the per-body DFS of CU:382-486 walks only the k
+ * bodies whose ORIGINAL indices are targets[0..k).  Per target q: the
+ * acceleration (without G) in acc_out[2q..2q+1], the monopole terms of cells
+ * and multi-body leaves in cells_out[q], the body-body terms in pairs_out[q],
+ * and the deepest DFS stack in stack_out[q] (entries, the quantity bounded
+ * by CU:400's int32_t stack[32]).  Output pointers may be NULL.  Returns 0,
+ * -1 on allocation failure, -2 for a target outside [0, n).
+ */
+int orc_ref_walk_targets(int64_t n, double* mass, double* pos_xy, double* vel_xy, int32_t* orig,
+                         double eps2, double theta, int64_t k, const int64_t* targets,
+                         double* acc_out, int64_t* cells_out, int64_t* pairs_out,
+                         int64_t* stack_out, int nthreads, orc_stats* stats);
+
+/*
  * FP64 all-pairs accelerations with the reference GPU pair law
  * (CU:427-431): a_i = sum_{j != i} m_j d_ij (|d_ij|^2 + eps2)^(-3/2),
  * evaluated for the k targets tgt[0..k) against all n sources.

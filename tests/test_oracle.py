@@ -130,3 +130,25 @@ def test_cpu_law_allpairs(orc):
     m = np.array([1.0, 2.0])
     a = orc.allpairs_cpulaw(m, p, G=1.5, eps2=1.0)
     assert np.allclose(a[0], 1.5 * 2.0 / 26.0 * np.array([0.6, 0.8]))
+
+
+def test_walk_targets_equals_the_full_step(orc, nbp):
+    # the targets-only walk sorts and builds exactly as the full step does and
+    # walks the chosen bodies with the same DFS: same accelerations (bit for
+    # bit), and per-target counts that add up to the step's totals
+    m, p, v = nbp.universes.colliding_discs(6000, 4)
+    full = orc.RefState(m, p, v)
+    r = full.step(theta=0.7, eps2=1e-4, integrate=False, want_acc=True)
+    acc_full = full.in_original_order(r["acc"])
+    tgt = np.random.default_rng(1).permutation(6000)
+    part = orc.RefState(m, p, v)
+    w = part.walk_targets(tgt, eps2=1e-4, theta=0.7)
+    assert np.array_equal(w["acc"], acc_full[tgt])
+    assert np.array_equal(part.orig, full.orig)
+    assert w["cells"].sum() == r["stats"]["cell_interactions"]
+    assert w["pairs"].sum() == r["stats"]["body_interactions"]
+    assert w["stack"].max() == r["stats"]["max_stack"]
+    few = orc.RefState(m, p, v).walk_targets(tgt[:17], eps2=1e-4, theta=0.7)
+    assert np.array_equal(few["acc"], acc_full[tgt[:17]])
+    with pytest.raises(IndexError):
+        orc.RefState(m, p, v).walk_targets(np.array([6000]))
