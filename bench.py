@@ -39,13 +39,21 @@ PKG = ROOT / "n-body-2d_b200"
 FLOPS_PER_INTERACTION = 14  # dx,dy,d2,+eps,r^-3 (3 mul),m*,2 fma: FP64/FP32 flops, rsqrt as 1
 FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
 # Algorithmic HBM bytes per body for each memory-bound phase (FP64 state,
-# u64 codes, u32 payload): bbox 16 + Morton 16 in / 12 out; 8 radix passes of
-# 12 in + 12 out; gather 44 in + 44 out; tree build about 8 x 3 reads + 32
-# writes per cell at 1.72 cells per body (96); moments 24 per body + 24 per
-# cell (65); drift 32 in + 16 out (FP64 mode only: SPLIT fuses it into the
-# force kernel, and the learned step's last phase is the correction kernel).
-PHASE_BYTES_PER_BODY = {"bbox+morton": 16 + 28, "sort": 8 * 24, "gather": 88, "tree": 96,
+# u64 codes, u32 payload): bbox 16 + Morton 16 in / 12 out; the sort's
+# histogram read (8) and P radix passes of 12 in + 12 out (P = 8 here;
+# sort_bytes() gives the bytes of a sort that took fewer passes); gather 44 in
+# + 44 out; tree build about 8 x 3 reads + 32 writes per cell at 1.72 cells per
+# body (96); moments 24 per body + 24 per cell (65); drift 32 in + 16 out (FP64
+# mode only: SPLIT fuses it into the force kernel, and the learned step's last
+# phase is the correction kernel).
+PHASE_BYTES_PER_BODY = {"bbox+morton": 16 + 28, "sort": 8 + 8 * 24, "gather": 88, "tree": 96,
                         "moments": 65, "drift": 48}
+
+
+def sort_bytes(passes: int) -> int:
+    """Bytes per body of a sort over the top `passes` key bytes: histogram read,
+    the passes, and the tie pass's read of the sorted keys when passes < 8."""
+    return 8 + 24 * passes + (8 if passes < 8 else 0)
 
 
 def _package():
@@ -59,16 +67,13 @@ def _package():
     return mod
 
 
-def _force_traffic(n: int):
-    """DRAM bytes per launch of the SPLIT force kernel, from the committed ncu
-    summary (captured at 1M bodies, scaled linearly to 4M there), scaled to n."""
-    f = ROOT / "profiles" / "force_split_collision1m.md"
-    if not f.exists():
-        return None
-    for ln in f.read_text().splitlines():
-        if ln.startswith("traffic_bytes_per_launch_4m:"):
-            return float(ln.split(":")[1]) * n / 4194304
-    return None
+# DRAM bytes one launch of the SPLIT monopole force kernel moves per body:
+# ncu dram__bytes_read.sum + dram__bytes_write.sum of one force_split launch
+# on the 1,048,576-body collision (77.5 MB + 7.1 MB = 84.6 MB, --clock-control
+# none).  Bodies and cells both grow linearly with N, so the figure scales by
+# N; it is a property of the kernel's access pattern, re-measured when the
+# kernel changes.
+FORCE_TRAFFIC_BYTES_PER_BODY = 84.6e6 / 1048576
 
 
 def _peaks() -> tuple[dict, str]:
@@ -401,6 +406,7 @@ def run_ours(args) -> None:
     st = ctx.stats()
     ms = st.ms_last_step
     phases = ctx.phase_times()
+    passes = ctx.debug_sort_passes() if args.mode != "allpairs" else 0
     ms = max_over_ranks(ms)
     value = world * args.n / (ms * 1e-3)
 
@@ -438,7 +444,7 @@ def run_ours(args) -> None:
     achieved = FLOPS_PER_INTERACTION * interactions / (force_ms * 1e-3) / 1e12
     hbm = peaks.get("hbm_gbs", FALLBACK_PEAKS["hbm_gbs"])
     rooflines = {}
-    for name, bpb in PHASE_BYTES_PER_BODY.items():
+    for name, bpb in dict(PHASE_BYTES_PER_BODY, sort=sort_bytes(passes or 8)).items():
         if name == "drift" and args.mode != "fp64":
             continue
         if args.mode == "allpairs" and name != "force":
@@ -457,9 +463,11 @@ def run_ours(args) -> None:
         "roofline": {"kernel": "force", "bound": "fp32" if args.mode == "split" else "fp64",
                      "achieved": round(achieved, 3), "peak": round(fp_peak, 2),
                      "unit": "TFLOP/s", "frac": round(achieved / fp_peak, 4),
-                     "traffic": _force_traffic(args.n) if args.mode == "split" else None,
-                     "traffic_source": "ncu dram__bytes_read+write of force_split at 1M bodies "
-                                       "(profiles/force_split_collision1m.md), scaled by n",
+                     "traffic": (FORCE_TRAFFIC_BYTES_PER_BODY * args.n
+                                 if args.mode == "split" and not args.quad and not args.learned
+                                 else None),
+                     "traffic_source": "ncu dram__bytes_read+write of one force_split launch at "
+                                       "1M bodies (FORCE_TRAFFIC_BYTES_PER_BODY), scaled by n",
                      "peak_source": f"nominal {lanes} FMA/clk/SM x 148 SMs at the sampled "
                                     f"median SM clock {sm_mhz} MHz",
                      "interactions_per_s": interactions / (force_ms * 1e-3),
@@ -468,6 +476,7 @@ def run_ours(args) -> None:
         "rooflines_hbm": rooflines, "hbm_peak_source": f"{peak_kind} MEASURED_PEAKS.json hbm_gbs"
         if peak_kind == "measured" else "fallback 6.65 TB/s",
         "phases_ms": {k: round(v, 4) for k, v in phases.items()},
+        "sort_passes": passes,
         "e2e": {"value": world * args.n / e2e_t, "unit": "body-steps/s",
                 "h2d_bytes_per_step": 40 * args.n, "d2h_bytes_per_step": 32 * args.n,
                 "steps": e2e_steps,
@@ -492,6 +501,8 @@ def run_ours(args) -> None:
                 "target_ratio": 2.0}
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.n, args.theta, m, p, v)
+    if rank == 0 and args.workload == "collision4m" and not args.no_sub_configs:
+        line["configs"] = sub_configs(args, nb, local)
     if world > 1:
         import torch.distributed as dist
 
@@ -499,6 +510,117 @@ def run_ours(args) -> None:
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def _hbm_rooflines(phases: dict, n: int, fp64: bool, passes: int = 8) -> dict:
+    peaks, kind = _peaks()
+    hbm = peaks.get("hbm_gbs", FALLBACK_PEAKS["hbm_gbs"])
+    out = {}
+    for name, bpb in dict(PHASE_BYTES_PER_BODY, sort=sort_bytes(passes)).items():
+        if name == "drift" and not fp64:
+            continue
+        if phases.get(name, 0) > 0:
+            gbs = bpb * n / (phases[name] * 1e-3) / 1e9
+            out[name] = {"achieved_gbs": round(gbs, 1), "frac": round(gbs / hbm, 4),
+                         "ms": round(phases[name], 4)}
+    out["peak_gbs"] = hbm
+    out["peak_source"] = f"{kind} hbm_gbs"
+    return out
+
+
+def _timed_context(nb, cfg, m, p, v, warmup: int, steps: int, counts=None, error_sample=65536,
+                   accuracy=True, autotune=False) -> dict:
+    """W + K graph-launched steps of one context, device-timed, with the phase
+    times and (optionally) the p50/p99 force error of the state after them."""
+    from nbody_b200 import accuracy as acc_mod
+
+    with nb.NbContext(cfg, m, p, v, counts=counts) as ctx:
+        tuned = ctx.autotune(2) if autotune else None
+        ctx.step(warmup)
+        ctx.step(steps, sync=False)
+        ctx.sync()
+        st = ctx.stats()
+        phases = ctx.phase_times()
+        passes = ctx.debug_sort_passes()
+        rec = {"ms_per_step": st.ms_last_step, "sort_passes": passes, "value": m.shape[0] / (st.ms_last_step * 1e-3),
+               "unit": "body-steps/s", "steps": steps, "warmup": warmup,
+               "phases_ms": {k: round(x, 4) for k, x in phases.items()},
+               "interactions_per_body": (st.cell_interactions + st.body_interactions)
+               / m.shape[0]}
+        if tuned:
+            rec["autotuned"] = {"leaf_size": tuned[0], "bodies_per_lane": tuned[1]}
+        if accuracy:
+            acc_now = ctx.accelerations()
+            pos_now, _ = ctx.download()
+            if counts is None:
+                err = acc_mod.force_errors(acc_now, m, pos_now, cfg.epsilon_squared,
+                                           k=error_sample, device=cfg.device)
+            else:
+                err = acc_mod.ensemble_force_errors(acc_now, m, pos_now, counts,
+                                                    cfg.epsilon_squared, k=error_sample,
+                                                    device=cfg.device)
+            rec["p50"], rec["p99"] = err["p50"], err["p99"]
+    rec["rooflines_hbm"] = _hbm_rooflines(phases, m.shape[0], cfg.mode == nb.NB_MODE_FP64, passes)
+    return rec
+
+
+def sub_configs(args, nb, device: int) -> dict:
+    """The other benchmark configurations, each bounded to a few seconds, so
+    the default run carries them: the 16,384-body disc (SPLIT and the FP64
+    parity walk), the 16,777,216-body Plummer disc (SPLIT next to all-FP64),
+    and the 512-universe ensemble (one batched context against one context
+    per universe launched in turn).  Errors against FP64 all-pairs on 65,536
+    targets (per universe for the ensemble)."""
+    out = {}
+    mk = lambda mode, **kw: nb.SimConfig(timestep=1e-4, theta=0.5, epsilon_squared=1e-4, G=1.0,
+                                         mode=mode, device=device, **kw)
+    m, p, v = nb.universes.make("disc", 16384, 0)
+    out["disc16k"] = {
+        "split": _timed_context(nb, mk(nb.NB_MODE_SPLIT), m, p, v, 3, 200),
+        "fp64": _timed_context(nb, mk(nb.NB_MODE_FP64), m, p, v, 3, 200),
+        "config": "one exponential disc, N=16,384, seed 0, theta=0.5"}
+    m, p, v = nb.universes.make("plummer", 16777216, 0)
+    out["plummer16m"] = {
+        "split": _timed_context(nb, mk(nb.NB_MODE_SPLIT), m, p, v, 3, 5),
+        "fp64": _timed_context(nb, mk(nb.NB_MODE_FP64), m, p, v, 3, 3),
+        "config": "projected Plummer disc, N=16,777,216, seed 0, theta=0.5; SPLIT (FP32 "
+                  "traversal, FP64 box/COM/integrator) next to the all-FP64 walk"}
+    del m, p, v
+    m, p, v, counts = nb.universes.ensemble_batch(512, seed=0)
+    batched = _timed_context(nb, mk(nb.NB_MODE_SPLIT), m, p, v, 3, 5, counts=counts,
+                             autotune=True)
+    off = np.concatenate([[0], np.cumsum(counts.astype(np.int64))])
+    tuned = batched.get("autotuned", {}).get("leaf_size", 0)
+    import torch
+
+    ctxs = [nb.NbContext(mk(nb.NB_MODE_SPLIT, leaf_size=tuned), m[off[u]:off[u + 1]],
+                         p[off[u]:off[u + 1]], v[off[u]:off[u + 1]]) for u in range(len(counts))]
+    try:
+        for c in ctxs:
+            c.step(2)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        lsteps = 3
+        for _ in range(lsteps):
+            for c in ctxs:
+                c.step(1, sync=False)
+        for c in ctxs:
+            c.sync()
+        lt = (time.perf_counter() - t0) / lsteps
+    finally:
+        for c in ctxs:
+            c.close()
+    n = int(m.shape[0])
+    out["ensemble512"] = {
+        "batched": batched,
+        "looped": {"value": n / lt, "unit": "body-steps/s", "ms_per_step_wall": lt * 1e3,
+                   "steps": lsteps,
+                   "how": "one context per universe, each step launched universe after "
+                          "universe; wall clock from the first launch to the last sync"},
+        "speedup_batched_vs_looped": batched["value"] / (n / lt),
+        "config": f"512 exponential discs, {n} bodies, sizes {int(counts.min())}.."
+                  f"{int(counts.max())}, theta=0.5"}
+    return out
 
 
 def run_ensemble(args) -> None:
@@ -723,6 +845,9 @@ def main(argv=None):
     ap.add_argument("--quad", action="store_true", help="SPLIT: add quadrupole terms")
     ap.add_argument("--leaf", type=int, default=0, help="SPLIT: direct-sum cell size (0=default)")
     ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--no-sub-configs", action="store_true",
+                    help="skip the bounded 16K-disc / 16.7M-Plummer / 512-universe records "
+                         "of the default run")
     ap.add_argument("--error-sample", type=int, default=65536)
     ap.add_argument("--no-learned-comparison", action="store_true",
                     help="skip the learned theta=1.0 step timed next to the default plain step")

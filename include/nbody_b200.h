@@ -238,6 +238,16 @@ NB_API int nb_debug_tree(nb_ctx* ctx, double* cell_mass, double* cell_com_xy, in
 NB_API int nb_debug_interactions(nb_ctx* ctx, uint32_t* cell_terms, uint32_t* body_terms,
                                  int32_t* stack_high_water);
 
+/* Debug control of the sort stage (no counterpart in the reference, whose CUB
+ * sort always orders all 64 bits, BarnesHutCuda.cu:692): each step's radix
+ * sort orders the top P bytes of the keys, P chosen from the previous tree's
+ * neighbouring codes, and a tie pass then orders keys that agree in those
+ * bytes by their low bytes, so the permutation is the full stable sort's for
+ * any P.  passes = 1..8 forces P for the following sorts, 0 returns to the
+ * automatic choice, -1 changes nothing.  *last_passes (nullable) receives the
+ * P of the last sort (0 before the first). */
+NB_API int nb_debug_sort_passes(nb_ctx* ctx, int32_t passes, int32_t* last_passes);
+
 /* Debug view of the SPLIT traversal's target groups of the last step (no
  * counterpart in the reference, which walks the tree once per body): *count
  * receives the number of groups, and the first min(count, capacity) groups'

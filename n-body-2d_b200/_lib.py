@@ -39,6 +39,7 @@ EXPORTS = (
     "nb_set_mlp_weights", "nb_mlp_samples", "nb_mlp_forward", "nb_mlp_loss_grad", "nb_mlp_train",
     "nb_batch_create", "nb_autotune", "nb_render", "nb_download_async", "nb_download_wait",
     "nb_debug_wait_timeout", "nb_upload_async", "nb_debug_interactions", "nb_debug_groups",
+    "nb_debug_sort_passes",
 )
 
 
@@ -127,6 +128,7 @@ def load() -> C.CDLL:
     lib.nb_get_stats.argtypes = [_P, C.POINTER(NbStats)]
     lib.nb_debug_interactions.argtypes = [_P, _P, _P, _P]
     lib.nb_debug_groups.argtypes = [_P, _P, _P, C.c_uint64, _P]
+    lib.nb_debug_sort_passes.argtypes = [_P, C.c_int32, _P]
     lib.nb_last_error.argtypes = [_P]
     lib.nb_last_error.restype = C.c_char_p
     lib.nb_status_string.argtypes = [C.c_int]

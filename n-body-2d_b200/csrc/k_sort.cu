@@ -26,6 +26,19 @@ __device__ __forceinline__ double warp_max(double v) {
     return v;
 }
 
+// Chooses this step's radix passes (the top bytes of the key the sort orders
+// by) and resets the counters of the tie pass; the histogram of the last tree
+// is consumed.  Without `adaptive` (or with a forced count) no histogram is
+// used.
+__device__ __forceinline__ void start_sort(DeviceScalars* s, int64_t n, int adaptive) {
+    int passes = adaptive ? choose_sort_passes(s->lcp_hist, n) : 8;
+    if (s->sort_passes_forced > 0) passes = min(s->sort_passes_forced, 8);
+    s->sort_passes = passes;
+    for (int d = 0; d <= 32; ++d) s->lcp_hist[d] = 0;
+    s->tie_count[0] = 0;
+    s->tie_count[1] = 0;
+}
+
 // Exact FP64 min/max of all positions, reduced per block, then folded and
 // squared by the last block to finish (CU:78-114 + the host squaring at
 // CU:665-677, done here on the device in the same FP64 operations).  Min and
@@ -58,7 +71,7 @@ __device__ __forceinline__ void box_fold(double& xmin, double& xmax, double& ymi
 
 __global__ void __launch_bounds__(kBoxThreads)
 bbox_kernel(const double2* __restrict__ pos, int64_t n, double* __restrict__ partials,
-            DeviceScalars* __restrict__ s) {
+            DeviceScalars* __restrict__ s, int adaptive) {
     double xmin = INFINITY, xmax = -INFINITY, ymin = INFINITY, ymax = -INFINITY;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -134,6 +147,7 @@ bbox_kernel(const double2* __restrict__ pos, int64_t n, double* __restrict__ par
             wsq *= 0.25;
         }
         s->bbox_ticket = 0;
+        start_sort(s, n, adaptive);
     }
 }
 
@@ -148,12 +162,19 @@ __device__ __forceinline__ uint64_t expand_bits_2d(uint32_t v) {
 }
 
 // CU:117-132: code from (p - min) * (1 / width), quantised to 32 bits per axis
-// with round-down; x bits land on odd positions.  val = current slot.
+// with round-down; x bits land on odd positions.  val = current slot.  The
+// codes go to the buffer the first radix pass reads: pass k reads buffer
+// k & 1, and the first of the step's sort_passes passes is 8 - sort_passes,
+// so the last one always writes buffer 0.
 __global__ void morton_kernel(const double2* __restrict__ pos, int64_t n,
-                              const DeviceScalars* __restrict__ s, uint64_t* __restrict__ key,
-                              uint32_t* __restrict__ val) {
+                              const DeviceScalars* __restrict__ s, uint64_t* __restrict__ key0,
+                              uint64_t* __restrict__ key1, uint32_t* __restrict__ val0,
+                              uint32_t* __restrict__ val1) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
+    const bool odd = s->sort_passes & 1;
+    uint64_t* __restrict__ key = odd ? key1 : key0;
+    uint32_t* __restrict__ val = odd ? val1 : val0;
     const double x0 = s->box[0], x1 = s->box[1], y0 = s->box[2], y1 = s->box[3];
     const double inv_w = 1.0 / (x1 - x0);
     const double inv_h = 1.0 / (y1 - y0);
@@ -212,8 +233,9 @@ bbox_batch_kernel(const double2* __restrict__ pos, int64_t n, Batch b) {
 
 // Squares every universe's box as the single-universe path does, and resets
 // the reduction slots for the next step.
-__global__ void bbox_batch_finish(Batch b) {
+__global__ void bbox_batch_finish(Batch b, DeviceScalars* __restrict__ s, int64_t n) {
     const int u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u == 0) start_sort(s, n, 1);
     if (u >= b.nuni) return;
     unsigned long long* e = b.boxbits + 4 * u;
     double x0 = from_ordered(e[0]), x1 = from_ordered(~e[1]);
@@ -239,9 +261,14 @@ __global__ void bbox_batch_finish(Batch b) {
 }
 
 __global__ void morton_batch_kernel(const double2* __restrict__ pos, int64_t n, Batch b,
-                                    uint64_t* __restrict__ key, uint32_t* __restrict__ val) {
+                                    const DeviceScalars* __restrict__ s,
+                                    uint64_t* __restrict__ key0, uint64_t* __restrict__ key1,
+                                    uint32_t* __restrict__ val0, uint32_t* __restrict__ val1) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
+    const bool odd = s->sort_passes & 1;
+    uint64_t* __restrict__ key = odd ? key1 : key0;
+    uint32_t* __restrict__ val = odd ? val1 : val0;
     const int u = b.uid[i];
     const double2 lo = b.lo[u];
     const double inv_w = 1.0 / sqrt(b.w2[u]);
@@ -434,7 +461,10 @@ constexpr int kSpinLimit = 1 << 22;
 constexpr int kHistRun = 16;
 
 __global__ void __launch_bounds__(kSortThreads)
-onesweep_histogram(const uint64_t* __restrict__ key, int64_t n, uint32_t* __restrict__ hist) {
+onesweep_histogram(const uint64_t* __restrict__ key0, const uint64_t* __restrict__ key1, int64_t n,
+                   const DeviceScalars* __restrict__ s, uint32_t* __restrict__ hist) {
+    // the Morton pass wrote the codes where the first radix pass reads them
+    const uint64_t* __restrict__ key = (s->sort_passes & 1) ? key1 : key0;
     __shared__ uint32_t h[8][256];
     for (int k = threadIdx.x; k < 8 * 256; k += kSortThreads) (&h[0][0])[k] = 0;
     __syncthreads();
@@ -504,39 +534,116 @@ __device__ __forceinline__ void st_status(uint32_t* p, uint32_t v) {
     asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
+// ---- one-CTA bulk copies (cp.async.bulk, no multicast) into shared memory --
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
+    // the barrier must be visible to the async proxy before a copy signals it
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+// bytes: a multiple of 16; both addresses 16-byte aligned
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ bool mbar_test(uint64_t* bar, unsigned phase) {
+    unsigned done;
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, P1;\n\t}"
+        : "=r"(done)
+        : "r"(smem_u32(bar)), "r"(phase)
+        : "memory");
+    return done != 0;
+}
+// Bounded wait for phase 0 of a barrier; false if it ran out.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar) {
+    for (int k = 0; k < kSpinLimit; ++k)
+        if (mbar_test(bar, 0)) return true;
+    return false;
+}
+
 // Four blocks per SM (at most 64 registers): tiles of 3072 keys keep enough
-// loads in flight per block, and the occupancy hides the look-back.
+// loads in flight per block, and the occupancy hides the look-back.  The
+// tile's keys and values arrive in shared memory by two bulk copies (the
+// copy engine moves the 36 KB while the block's threads are free), then each
+// thread ranks its 12 keys, and the tile leaves sorted by digit through the
+// same shared buffers with coalesced stores.  The scatter itself cannot be a
+// bulk copy: a digit's run starts at an arbitrary 8-byte offset of the output.
+// Passes below the step's first pass (shift < 64 - 8 sort_passes) return at
+// once; passes == nullptr runs every pass.
 __global__ void __launch_bounds__(kSortThreads, 4)
 onesweep_pass(const uint64_t* __restrict__ key_in, const uint32_t* __restrict__ val_in,
               uint64_t* __restrict__ key_out, uint32_t* __restrict__ val_out, int64_t n, int shift,
               const uint32_t* __restrict__ bins, uint32_t* __restrict__ status,
-              unsigned* __restrict__ tile_counter, unsigned* __restrict__ err) {
+              unsigned* __restrict__ tile_counter, unsigned* __restrict__ err,
+              const int32_t* __restrict__ passes) {
+    if (passes && shift < 64 - 8 * *passes) return;
     __shared__ uint32_t whist[kWarps][256];
     __shared__ uint32_t tile_start[256];
     __shared__ uint32_t goff[256];
     __shared__ uint32_t warp_tot[kWarps];
-    __shared__ uint64_t skey[kSortTile];
-    __shared__ uint32_t sval[kSortTile];
+    __shared__ __align__(16) uint64_t skey[kSortTile];
+    __shared__ __align__(16) uint32_t sval[kSortTile];
+    __shared__ __align__(8) uint64_t bar;
     __shared__ int tile_sh;
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    if (tid == 0) tile_sh = (int)atomicAdd(tile_counter, 1u);
+    if (tid == 0) {
+        const int tile = (int)atomicAdd(tile_counter, 1u);
+        tile_sh = tile;
+        const int64_t base = (int64_t)tile * kSortTile;
+        const int tile_n = (int)min((int64_t)kSortTile, n - base);
+        const int bulk = tile_n & ~3;  // whole 16-byte chunks of both arrays
+        mbar_init(&bar);
+        mbar_expect_tx(&bar, (unsigned)bulk * 12u);
+        if (bulk > 0) {
+            bulk_load(skey, key_in + base, (unsigned)bulk * 8u, &bar);
+            bulk_load(sval, val_in + base, (unsigned)bulk * 4u, &bar);
+        }
+    }
 #pragma unroll
     for (int w = 0; w < kWarps; ++w) whist[w][tid] = 0;
     __syncthreads();
     const int tile = tile_sh;
     const int64_t base = (int64_t)tile * kSortTile;
-    const int64_t seg = base + warp * (32 * kSortTileItems);
+    const int tile_n = (int)min((int64_t)kSortTile, n - base);
+    {
+        const int bulk = tile_n & ~3;
+        if (tid < tile_n - bulk) {  // the last tile's ragged end, at most 3 keys
+            skey[bulk + tid] = key_in[base + bulk + tid];
+            sval[bulk + tid] = val_in[base + bulk + tid];
+        }
+        bool ok = mbar_wait_bounded(&bar);
+        if (!ok) {
+            atomicOr(err, kErrTimeout);
+            ok = mbar_wait_bounded(&bar);  // let the copies land before the block moves on
+        }
+    }
+    __syncthreads();
+    const int seg = warp * (32 * kSortTileItems);
     uint64_t k_reg[kSortTileItems];
     uint32_t v_reg[kSortTileItems];
     uint32_t r_reg[kSortTileItems];
     const unsigned below = lanemask_lt();
 #pragma unroll
     for (int k = 0; k < kSortTileItems; ++k) {
-        const int64_t i = seg + k * 32 + lane;
-        const bool valid = i < n;
-        k_reg[k] = valid ? key_in[i] : 0ull;
-        v_reg[k] = valid ? val_in[i] : 0u;
+        const int li = seg + k * 32 + lane;
+        const bool valid = li < tile_n;
+        k_reg[k] = valid ? skey[li] : 0ull;
+        v_reg[k] = valid ? sval[li] : 0u;
         const uint32_t d = (uint32_t)((k_reg[k] >> shift) & 0xFF);
         const unsigned peers = digit_peers(d, valid);
         const int leader = __ffs(peers) - 1;
@@ -589,8 +696,8 @@ onesweep_pass(const uint64_t* __restrict__ key_in, const uint32_t* __restrict__ 
     __syncthreads();
 #pragma unroll
     for (int k = 0; k < kSortTileItems; ++k) {
-        const int64_t i = seg + k * 32 + lane;
-        if (i < n) {
+        const int li = seg + k * 32 + lane;
+        if (li < tile_n) {
             const uint32_t d = (uint32_t)((k_reg[k] >> shift) & 0xFF);
             const uint32_t lp = tile_start[d] + whist[warp][d] + r_reg[k];
             skey[lp] = k_reg[k];
@@ -598,13 +705,171 @@ onesweep_pass(const uint64_t* __restrict__ key_in, const uint32_t* __restrict__ 
         }
     }
     __syncthreads();
-    const int tile_n = (int)min((int64_t)kSortTile, n - base);
     for (int p = tid; p < tile_n; p += kSortThreads) {
         const uint64_t kk = skey[p];
         const uint32_t d = (uint32_t)((kk >> shift) & 0xFF);
         const uint32_t gp = goff[d] + (uint32_t)p - tile_start[d];
         key_out[gp] = kk;
         val_out[gp] = sval[p];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Tie pass.  After radix passes over the top P bytes only, keys that agree in
+// those bytes sit together in their input order; putting each such group in
+// order of its low bytes (ties kept in input order) gives exactly the full
+// stable sort.  tie_mark lists the groups, tie_sort_small orders groups of
+// up to 32 keys one warp each in registers, tie_sort_big orders larger ones
+// one warp each by an LSD radix sort of the low bytes through the free
+// ping-pong buffers.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+tie_mark(const uint64_t* __restrict__ key, int64_t n, DeviceScalars* __restrict__ s,
+         uint2* __restrict__ small, uint2* __restrict__ big) {
+    const int passes = s->sort_passes;
+    if (passes >= 8) return;
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int sh = 64 - 8 * passes;
+    bool start = false;
+    int64_t e = i;
+    if (i + 1 < n) {
+        const uint64_t top = key[i] >> sh;
+        start = (key[i + 1] >> sh) == top && (i == 0 || (key[i - 1] >> sh) != top);
+        if (start) {  // last key of the group: galloping search
+            int64_t step = 1, good = i + 1;
+            while (good + step < n && (key[good + step] >> sh) == top) {
+                good += step;
+                step <<= 1;
+            }
+            int64_t lo = good, hi = min(n - 1, good + step - 1);
+            while (lo < hi) {
+                const int64_t mid = (lo + hi + 1) >> 1;
+                if ((key[mid] >> sh) == top) lo = mid; else hi = mid - 1;
+            }
+            e = lo;
+        }
+    }
+    const unsigned size = (unsigned)(e - i + 1);
+    const bool is_small = start && size <= 32, is_big = start && size > 32;
+    const unsigned ms = __ballot_sync(kFull, is_small), mb = __ballot_sync(kFull, is_big);
+    const int lane = threadIdx.x & 31;
+    unsigned b0 = 0, b1 = 0;
+    if (lane == 0) {
+        if (ms) b0 = atomicAdd(&s->tie_count[0], __popc(ms));
+        if (mb) b1 = atomicAdd(&s->tie_count[1], __popc(mb));
+    }
+    b0 = __shfl_sync(kFull, b0, 0);
+    b1 = __shfl_sync(kFull, b1, 0);
+    const unsigned lt = lanemask_lt();
+    if (is_small) small[b0 + __popc(ms & lt)] = make_uint2((unsigned)i, size);
+    if (is_big) big[b1 + __popc(mb & lt)] = make_uint2((unsigned)i, size);
+}
+
+// Groups of 2..32 keys: lane l holds key l of the group and counts the keys
+// that go before it (smaller, or equal and earlier).  The keys share their top
+// bytes, so comparing whole keys compares the low bytes.
+__global__ void __launch_bounds__(256)
+tie_sort_small(uint64_t* __restrict__ key, uint32_t* __restrict__ val,
+               const uint2* __restrict__ small, const DeviceScalars* __restrict__ s) {
+    if (s->sort_passes >= 8) return;
+    const unsigned count = s->tie_count[0];
+    const int lane = threadIdx.x & 31;
+    const unsigned warps = gridDim.x * (blockDim.x >> 5);
+    for (unsigned g = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); g < count; g += warps) {
+        const uint2 grp = small[g];
+        const bool on = lane < (int)grp.y;
+        const uint64_t k = on ? key[grp.x + lane] : ~0ull;
+        const uint32_t v = on ? val[grp.x + lane] : 0u;
+        int rank = 0;
+        for (int j = 0; j < (int)grp.y; ++j) {
+            const uint64_t kj = __shfl_sync(kFull, k, j);
+            rank += (kj < k || (kj == k && j < lane)) ? 1 : 0;
+        }
+        __syncwarp();
+        if (on) {
+            key[grp.x + rank] = k;
+            val[grp.x + rank] = v;
+        }
+    }
+}
+
+// Groups of more than 32 keys (rare: many bodies within 2^-4P of the box
+// width of each other): one warp per group, a stable LSD radix sort of the
+// 8 - P low bytes, 32 keys at a time, between the group's range of the
+// sorted buffers and the same range of the free ping-pong buffers.
+__global__ void __launch_bounds__(128)
+tie_sort_big(uint64_t* __restrict__ key0, uint32_t* __restrict__ val0, uint64_t* __restrict__ key1,
+             uint32_t* __restrict__ val1, const uint2* __restrict__ big,
+             const DeviceScalars* __restrict__ s) {
+    const int passes = s->sort_passes;
+    if (passes >= 8) return;
+    __shared__ uint32_t off[4][256];
+    const unsigned count = s->tie_count[1];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const unsigned below = lanemask_lt();
+    for (unsigned g = blockIdx.x * 4 + w; g < count; g += gridDim.x * 4) {
+        const uint2 grp = big[g];
+        const unsigned first = grp.x, size = grp.y;
+        for (int d = 0; d < 8 - passes; ++d) {
+            const int sh = 8 * d;
+            const bool from0 = (d & 1) == 0;
+            const uint64_t* ks = from0 ? key0 : key1;
+            const uint32_t* vs = from0 ? val0 : val1;
+            uint64_t* kd = from0 ? key1 : key0;
+            uint32_t* vd = from0 ? val1 : val0;
+            for (int b = lane; b < 256; b += 32) off[w][b] = 0;
+            __syncwarp();
+            for (unsigned b = 0; b < size; b += 32) {
+                if (b + lane < size) atomicAdd(&off[w][(ks[first + b + lane] >> sh) & 0xFF], 1u);
+            }
+            __syncwarp();
+            // exclusive scan of the 256 bins, 8 per lane
+            uint32_t c[8], tot = 0;
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                c[q] = off[w][lane * 8 + q];
+                tot += c[q];
+            }
+            uint32_t inc = tot;
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t t = __shfl_up_sync(kFull, inc, o);
+                if (lane >= o) inc += t;
+            }
+            uint32_t run = inc - tot;
+            __syncwarp();
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                off[w][lane * 8 + q] = run;
+                run += c[q];
+            }
+            __syncwarp();
+            for (unsigned b = 0; b < size; b += 32) {
+                const bool on = b + lane < size;
+                const uint64_t k = on ? ks[first + b + lane] : 0ull;
+                const uint32_t v = on ? vs[first + b + lane] : 0u;
+                const uint32_t dg = (uint32_t)((k >> sh) & 0xFF);
+                const unsigned peers = digit_peers(dg, on);
+                const int leader = __ffs(peers) - 1;
+                uint32_t pos = 0;
+                if (on && lane == leader) {
+                    pos = off[w][dg];
+                    off[w][dg] = pos + __popc(peers);
+                }
+                pos = __shfl_sync(kFull, pos, leader) + __popc(peers & below);
+                if (on) {
+                    kd[first + pos] = k;
+                    vd[first + pos] = v;
+                }
+                __syncwarp();
+            }
+        }
+        if ((8 - passes) & 1) {  // the result is in the second buffers: copy it back
+            for (unsigned b = lane; b < size; b += 32) {
+                key0[first + b] = key1[first + b];
+                val0[first + b] = val1[first + b];
+            }
+        }
+        __syncwarp();
     }
 }
 
@@ -639,22 +904,25 @@ void launch_bbox(nb_ctx* c, const double2* pos) {
     if (c->batch.nuni > 0) {
         c->launches += 2;
         bbox_batch_kernel<<<2 * c->sm_count * 8, 256, 0, c->stream>>>(pos, c->n, c->batch);
-        bbox_batch_finish<<<blocks_for(c->batch.nuni, 128), 128, 0, c->stream>>>(c->batch);
+        bbox_batch_finish<<<blocks_for(c->batch.nuni, 128), 128, 0, c->stream>>>(c->batch, c->scal,
+                                                                                c->n);
         return;
     }
     c->launches += 1;
-    bbox_kernel<<<c->bbox_blocks, kBoxThreads, 0, c->stream>>>(pos, c->n, c->bbox_partials, c->scal);
+    bbox_kernel<<<c->bbox_blocks, kBoxThreads, 0, c->stream>>>(pos, c->n, c->bbox_partials, c->scal,
+                                                               1);
 }
 
 void launch_morton(nb_ctx* c, const double2* pos) {
     c->launches += 1;
     if (c->batch.nuni > 0) {
         morton_batch_kernel<<<blocks_for(c->n, 256), 256, 0, c->stream>>>(
-            pos, c->n, c->batch, c->sort.key[0], c->sort.val[0]);
+            pos, c->n, c->batch, c->scal, c->sort.key[0], c->sort.key[1], c->sort.val[0],
+            c->sort.val[1]);
         return;
     }
-    morton_kernel<<<blocks_for(c->n, 256), 256, 0, c->stream>>>(pos, c->n, c->scal, c->sort.key[0],
-                                                               c->sort.val[0]);
+    morton_kernel<<<blocks_for(c->n, 256), 256, 0, c->stream>>>(
+        pos, c->n, c->scal, c->sort.key[0], c->sort.key[1], c->sort.val[0], c->sort.val[1]);
 }
 
 // One radix pass over two tiles of keys in which only the second tile runs:
@@ -683,7 +951,7 @@ unsigned sort_timeout_probe(cudaStream_t st) {
         const unsigned one = 1u;  // the single block takes tile 1
         cudaMemcpyAsync(counter, &one, sizeof(unsigned), cudaMemcpyHostToDevice, st);
         onesweep_pass<<<1, kSortThreads, 0, st>>>(key_in, val_in, key_out, val_out, n, 0, hist, status,
-                                                  counter, err);
+                                                  counter, err, nullptr);
         cudaMemcpyAsync(&flags, err, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
         if (cudaStreamSynchronize(st) != cudaSuccess) flags = ~0u;
     }
@@ -700,21 +968,29 @@ unsigned sort_timeout_probe(cudaStream_t st) {
 
 void launch_sort(nb_ctx* c) {
     const int tiles = c->sort.tiles;
-    c->launches += 2 + 8;
+    c->launches += 2 + 8 + 3;
     // histograms, per-pass status words and tile counters start at zero
     cudaMemsetAsync(c->sort.hist, 0, sizeof(uint32_t) * 8 * 256, c->stream);
     cudaMemsetAsync(c->sort.status, 0, sizeof(uint32_t) * 8 * 256 * (size_t)tiles, c->stream);
     cudaMemsetAsync(c->sort.tile_counter, 0, sizeof(unsigned) * 8, c->stream);
-    onesweep_histogram<<<2 * c->sm_count, kSortThreads, 0, c->stream>>>(c->sort.key[0], c->n,
-                                                                        c->sort.hist);
+    onesweep_histogram<<<2 * c->sm_count, kSortThreads, 0, c->stream>>>(
+        c->sort.key[0], c->sort.key[1], c->n, c->scal, c->sort.hist);
     onesweep_bins<<<8, kSortThreads, 0, c->stream>>>(c->sort.hist);
     for (int pass = 0; pass < 8; ++pass) {
         const int src = pass & 1, dst = src ^ 1;
         onesweep_pass<<<tiles, kSortThreads, 0, c->stream>>>(
             c->sort.key[src], c->sort.val[src], c->sort.key[dst], c->sort.val[dst], c->n, 8 * pass,
             c->sort.hist + 256 * pass, c->sort.status + (size_t)pass * 256 * tiles,
-            c->sort.tile_counter + pass, &c->scal->error);
+            c->sort.tile_counter + pass, &c->scal->error, &c->scal->sort_passes);
     }
+    // keys tied in the sorted top bytes, in order of their low bytes
+    tie_mark<<<blocks_for(c->n, 256), 256, 0, c->stream>>>(c->sort.key[0], c->n, c->scal,
+                                                           c->sort.ties_small, c->sort.ties_big);
+    tie_sort_small<<<c->sm_count * 8, 256, 0, c->stream>>>(c->sort.key[0], c->sort.val[0],
+                                                          c->sort.ties_small, c->scal);
+    tie_sort_big<<<c->sm_count, 128, 0, c->stream>>>(c->sort.key[0], c->sort.val[0],
+                                                     c->sort.key[1], c->sort.val[1],
+                                                     c->sort.ties_big, c->scal);
 }
 
 void launch_morton_sort_raw(const double2* pos, int64_t n, uint64_t* const key[2],
@@ -722,8 +998,8 @@ void launch_morton_sort_raw(const double2* pos, int64_t n, uint64_t* const key[2
                             uint32_t* counts, uint32_t* totals, double* partials, int bbox_blocks,
                             DeviceScalars* scal, cudaStream_t st) {
     const int tiles = (int)((n + kSortTile - 1) / kSortTile);
-    bbox_kernel<<<bbox_blocks, kBoxThreads, 0, st>>>(pos, n, partials, scal);
-    morton_kernel<<<blocks_for(n, 256), 256, 0, st>>>(pos, n, scal, key[0], val[0]);
+    bbox_kernel<<<bbox_blocks, kBoxThreads, 0, st>>>(pos, n, partials, scal, 0);  // all 8 passes
+    morton_kernel<<<blocks_for(n, 256), 256, 0, st>>>(pos, n, scal, key[0], key[1], val[0], val[1]);
     for (int pass = 0; pass < 8; ++pass) {
         const int src = pass & 1, dst = src ^ 1;
         const int shift = 8 * pass;

@@ -84,23 +84,32 @@ __device__ int gallop_right(const uint64_t* __restrict__ key, int i, int hi, int
     return a;
 }
 
-// Pass 1: flag the boundaries that create a cell.
+// Pass 1: flag the boundaries that create a cell.  It also counts, for the
+// next step's sort, how many neighbouring codes share d leading digits
+// (choose_sort_passes reads the histogram).
 __global__ void tree_mark(const uint64_t* __restrict__ key, int n, int32_t* __restrict__ flag,
-                          int32_t* __restrict__ start_of) {
+                          int32_t* __restrict__ start_of, unsigned* __restrict__ lcp_hist) {
+    __shared__ unsigned hist[33];
+    if (threadIdx.x < 33) hist[threadIdx.x] = 0;
+    __syncthreads();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    int f = 0, s = 0;
-    if (i < n - 1) {
-        const uint64_t ki = key[i];
-        const int c = lcp_digits(ki, key[i + 1]);
-        if (c < kMaxLevel) {
-            s = c == 0 ? 0 : gallop_left(key, 0, i, c);
-            // i opens the cell iff bodies s..i all sit in its first child.
-            f = share(key[s], ki, c + 1) ? 1 : 0;
+    if (i < n) {
+        int f = 0, s = 0;
+        if (i < n - 1) {
+            const uint64_t ki = key[i];
+            const int c = lcp_digits(ki, key[i + 1]);
+            atomicAdd(&hist[c], 1u);
+            if (c < kMaxLevel) {
+                s = c == 0 ? 0 : gallop_left(key, 0, i, c);
+                // i opens the cell iff bodies s..i all sit in its first child.
+                f = share(key[s], ki, c + 1) ? 1 : 0;
+            }
         }
+        flag[i] = f;
+        start_of[i] = s;
     }
-    flag[i] = f;
-    start_of[i] = s;
+    __syncthreads();
+    if (threadIdx.x < 33 && hist[threadIdx.x]) atomicAdd(lcp_hist + threadIdx.x, hist[threadIdx.x]);
 }
 
 // ---- exclusive scan of flag[] -> cell_of[], total -> scal->cells ----------
@@ -932,7 +941,8 @@ void launch_tree(nb_ctx* c, const BodyBuffers& b) {
     const uint64_t* key = c->sort.key[0];
     c->launches += 6;
     tree_mark<<<blocks_for(n, kThreads), kThreads, 0, c->stream>>>(key, n, c->tree.flag,
-                                                                    c->tree.start_of);
+                                                                    c->tree.start_of,
+                                                                    c->scal->lcp_hist);
     const int sblocks = (int)blocks_for(n, kScanTile);
     scan_reduce<<<sblocks, kThreads, 0, c->stream>>>(c->tree.flag, n, c->scan.block_sums);
     scan_block_sums<<<1, kThreads, 0, c->stream>>>(c->scan.block_sums, sblocks, &c->scal->cells);

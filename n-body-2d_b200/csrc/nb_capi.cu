@@ -71,6 +71,8 @@ int alloc_all(nb_ctx* c) {
     NB_CUDA(c, dalloc(&c->sort.hist, 8 * 256));
     NB_CUDA(c, dalloc(&c->sort.status, (size_t)8 * 256 * c->sort.tiles));
     NB_CUDA(c, dalloc(&c->sort.tile_counter, 8));
+    NB_CUDA(c, dalloc(&c->sort.ties_small, n / 2 + 1));
+    NB_CUDA(c, dalloc(&c->sort.ties_big, n / 33 + 1));
     c->scan.blocks = (int)((n + 2047) / 2048);
     NB_CUDA(c, dalloc(&c->scan.block_sums, (size_t)c->scan.blocks));
     nb::Tree& t = c->tree;
@@ -139,6 +141,8 @@ void free_all(nb_ctx* c) {
     cudaFree(c->sort.hist);
     cudaFree(c->sort.status);
     cudaFree(c->sort.tile_counter);
+    cudaFree(c->sort.ties_small);
+    cudaFree(c->sort.ties_big);
     cudaFree(c->scan.block_sums);
     nb::Tree& t = c->tree;
     void* tree_ptrs[] = {t.first,     t.last,        t.level,       t.child,      t.parent,
@@ -747,6 +751,19 @@ int nb_debug_interactions(nb_ctx* c, uint32_t* cell_terms, uint32_t* body_terms,
     }
     if (stack_high_water) *stack_high_water = s.stack_hw;
     return read_device_error(c);
+}
+
+int nb_debug_sort_passes(nb_ctx* c, int32_t passes, int32_t* last_passes) {
+    if (!c || passes < -1 || passes > 8) return NB_ERR_INVALID;
+    DeviceGuard guard(c->device);
+    nb::DeviceScalars s;
+    NB_CUDA(c, cudaMemcpyAsync(&s, c->scal, sizeof(s), cudaMemcpyDeviceToHost, c->stream));
+    if (passes >= 0)
+        NB_CUDA(c, cudaMemcpyAsync(&c->scal->sort_passes_forced, &passes, sizeof(int32_t),
+                                   cudaMemcpyHostToDevice, c->stream));
+    NB_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (last_passes) *last_passes = s.sort_passes;
+    return NB_OK;
 }
 
 int nb_debug_groups(nb_ctx* c, int32_t* first_body, int32_t* last_body, uint64_t capacity,

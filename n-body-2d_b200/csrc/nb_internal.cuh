@@ -44,6 +44,15 @@ struct DeviceScalars {
     int32_t stack_pad_;
     int32_t nstart;           // cells whose children are all leaves (climb starts)
     unsigned upload_bad;      // nb_upload's checks: bit 0 non-finite, bit 1 mass <= 0
+    // Radix sort over the top sort_passes bytes of the keys only (1..8), chosen
+    // per step from the previous tree's histogram of shared leading digits of
+    // neighbouring codes; keys that agree in those bytes are then put in order
+    // of their low bytes by the tie pass, so the order stays the full stable
+    // sort.  sort_passes_forced != 0 overrides the choice (tests).
+    int32_t sort_passes;
+    int32_t sort_passes_forced;
+    unsigned lcp_hist[33];    // neighbouring codes sharing d leading 2-bit digits (d = 32: equal)
+    unsigned tie_count[2];    // tie groups of <= 32 keys / of more keys, this step
 };
 
 // Batched universes (nb_batch_create): bodies of universe u occupy the fixed
@@ -134,6 +143,8 @@ struct SortBuffers {
     uint32_t* hist = nullptr;     // [8][256] digit histograms -> exclusive bin offsets
     uint32_t* status = nullptr;   // [8][tiles][256] look-back status words
     unsigned* tile_counter = nullptr;  // [8]
+    uint2* ties_small = nullptr;  // tie groups of 2..32 keys: {first, size}, n / 2 + 1
+    uint2* ties_big = nullptr;    // tie groups of more than 32 keys, n / 33 + 1
     int tiles = 0;
 };
 
@@ -217,6 +228,21 @@ __device__ __forceinline__ double cell_width2(const DeviceScalars* s, const Batc
     if (b.nuni == 0) return s->wsq[level];
     if (level < kBatchUidDigits) return __longlong_as_double(0x7ff0000000000000ll);  // +inf
     return ldexp(b.w2[b.uid[i]], -2 * (level - kBatchUidDigits));
+}
+
+// Number of radix passes (top bytes of the key) a sort should take, from the
+// histogram of shared leading digits of neighbouring sorted codes: the fewest
+// passes that leave at most n / 32 neighbouring pairs tied; 8 without data.
+__device__ __forceinline__ int choose_sort_passes(const unsigned* hist, int64_t n) {
+    unsigned long long total = 0;
+    for (int d = 0; d <= 32; ++d) total += hist[d];
+    if (total == 0) return 8;
+    for (int p = 1; p < 8; ++p) {
+        unsigned long long tied = 0;  // pairs that agree in p bytes but are not equal
+        for (int d = 4 * p; d < 32; ++d) tied += hist[d];
+        if (tied * 32 <= (unsigned long long)n) return p;
+    }
+    return 8;
 }
 
 // Kernel launchers (all enqueue on ctx->stream, no host synchronisation).

@@ -235,6 +235,14 @@ class NbContext:
                                               C.addressof(hw)), self._h)
         return cells, bodies, hw.value
 
+    def debug_sort_passes(self, passes: int = -1) -> int:
+        """The radix passes (top key bytes) the last sort took.  passes = 1..8
+        forces that many for the following sorts, 0 returns to the automatic
+        choice, -1 leaves the setting as it is."""
+        last = C.c_int32()
+        check(self._lib.nb_debug_sort_passes(self.handle, passes, C.addressof(last)), self._h)
+        return last.value
+
     def debug_groups(self) -> np.ndarray:
         """SPLIT mode: [groups, 2] first and last body slot of each target group
         of the last step (device order)."""

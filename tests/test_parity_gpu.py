@@ -332,3 +332,49 @@ def test_fp64_mode_ignores_the_bmax_ratio(nbp):
         with nbp.NbContext(cfg, m, p, v) as ctx:
             out.append(ctx.accelerations())
     assert np.array_equal(out[0], out[1])
+
+
+def _sort_cases(rng):
+    yield "random", rng.normal(size=(100_003, 2)) * [4.0, 1.0]
+    # half the bodies inside a square 1e-7 wide: groups tied in any number of
+    # top bytes, of every size up to 50,000 (the one-warp radix path)
+    p = rng.random((100_000, 2)) * 10.0
+    p[:50_000] = 3.0 + rng.random((50_000, 2)) * 1e-7
+    yield "cluster", p
+    # exact copies: equal keys keep their input order
+    p = rng.random((15_001, 2))
+    p[:15_000] = np.repeat(rng.random((5, 2)), 3000, axis=0)
+    yield "coincident", rng.permutation(p)
+
+
+@pytest.mark.parametrize("passes", [1, 2, 3, 4, 5, 6, 7, 8])
+def test_sort_with_any_pass_count_is_the_full_stable_sort(nbp, orc, passes):
+    # the radix passes order only the top `passes` bytes; the tie pass must
+    # turn that into the stable sort of all 64 bits
+    rng = np.random.default_rng(100 + passes)
+    for name, p in _sort_cases(rng):
+        n = p.shape[0]
+        with ctx_for(nbp, np.ones(n), p, np.zeros((n, 2))) as ctx:
+            ctx.debug_sort_passes(passes)
+            codes, order, box = ctx.debug_morton()
+            assert ctx.debug_sort_passes() == passes
+        codes_o, order_o = orc.stable_sort(orc.morton(p))
+        assert np.array_equal(codes, codes_o), name
+        assert np.array_equal(order, order_o), name
+
+
+def test_automatic_pass_count_follows_the_tree(nbp, orc):
+    # the first sort has no tree to learn from and takes all 8 passes; later
+    # sorts take fewer on a smooth disc, and stay exact
+    m, p, v = nbp.universes.colliding_discs(262_144, 9)
+    with ctx_for(nbp, m, p, v, mode=nbp.NB_MODE_SPLIT) as ctx:
+        ctx.debug_morton()
+        assert ctx.debug_sort_passes() == 8
+        ctx.step(2)
+        codes, order, _ = ctx.debug_morton()
+        auto = ctx.debug_sort_passes()
+        mass, pos, vel, orig = ctx.debug_state()
+    assert 1 <= auto < 8
+    codes_o, order_o = orc.stable_sort(orc.morton(pos))
+    assert np.array_equal(codes, codes_o)
+    assert np.array_equal(order, order_o)
