@@ -241,6 +241,32 @@ def cpu_baseline(n: int, theta: float, mass, pos, vel) -> dict:
                       f"GPU step, {cores} OpenMP threads"}
 
 
+def gpu_baseline(nb, device: int) -> dict:
+    """The reference's own GPU step on the same B200 beside this library's, on
+    the one workload the reference kernel runs safely (its 32-entry traversal
+    stack, CU:400, overflows on the discs: the oracle's replay needs 43
+    entries at 4M bodies).  Both are timed on the jittered 262,144-body grid:
+    the reference by the harness driver's host clock, this library by CUDA
+    events (FP64 parity walk and SPLIT)."""
+    if str(ROOT) not in sys.path:
+        sys.path.insert(0, str(ROOT))
+    from oracle import refgpu
+
+    m, p, v = nb.universes.make("grid", 262144, 0)
+    ref = _ref_gpu_record(refgpu.time_steps(m, p, v, theta=0.5, steps=5), 262144)
+    mk = lambda mode: nb.SimConfig(timestep=1e-4, theta=0.5, epsilon_squared=1e-4, G=1.0,
+                                   mode=mode, device=device)
+    fp64 = _timed_context(nb, mk(nb.NB_MODE_FP64), m, p, v, 3, 20, accuracy=False)
+    split = _timed_context(nb, mk(nb.NB_MODE_SPLIT), m, p, v, 3, 20, accuracy=False)
+    rec = {"case": GRID_CASE, "reference": ref,
+           "ours_fp64": {k: fp64[k] for k in ("value", "ms_per_step", "phases_ms")},
+           "ours_split": {k: split[k] for k in ("value", "ms_per_step", "phases_ms")}}
+    if "value" in ref:
+        rec["ratio_fp64_vs_reference"] = fp64["value"] / ref["value"]
+        rec["ratio_split_vs_reference"] = split["value"] / ref["value"]
+    return rec
+
+
 def run_reference(args) -> None:
     """The reference arm: the reference's own CPU Barnes-Hut on the host cores,
     W untimed then K timed steps of the full workload in one process."""
@@ -276,19 +302,7 @@ def run_reference(args) -> None:
         sample = (f"{args.steps} timed steps of the full N={args.n} workload, CPU restatement "
                   f"of the reference GPU step, {cores} OpenMP threads")
     value = args.n / t
-    ref_gpu = None
-    if args.workload == "disc16k":
-        # config 0 is small enough for the reference's own GPU kernels, on the
-        # same inputs (the stack bound is checked by the oracle first)
-        from oracle import refgpu
-
-        r = refgpu.time_steps(m, p, v, theta=args.theta, steps=args.steps)
-        ref_gpu = ({"value": args.n / r["seconds_per_step"], "unit": "body-steps/s",
-                    "ms_per_step": r["seconds_per_step"] * 1e3, "max_stack": r["max_stack"],
-                    "how": "the reference's CUDA kernels (BarnesHutCuda.cu, unmodified) under the "
-                           "harness driver, host clock over K steps after one untimed step, "
-                           "without the per-step download of the bodies"}
-                   if "seconds_per_step" in r else r)
+    ref_gpu = reference_gpu_records(args, m, p, v)
     line = {
         "impl": "reference", "metric": "body-steps/s", "value": value, "unit": "body-steps/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
@@ -302,6 +316,42 @@ def run_reference(args) -> None:
     if ref_gpu is not None:
         line["reference_gpu"] = ref_gpu
     print(json.dumps(line), flush=True)
+
+
+REF_GPU_HOW = ("the reference's CUDA kernels (BarnesHutCuda.cu, unmodified) under the harness "
+               "driver, host clock over K steps after one untimed step (the reference's step "
+               "synchronises with the host at every tree level), without the per-step download "
+               "of the bodies")
+GRID_CASE = ("jittered grid, 512 x 512 = 262,144 bodies, seed 0, theta 0.5: the CPU oracle's "
+             "replay finds at most 28 of the reference kernel's 32 traversal-stack entries in use")
+
+
+def _ref_gpu_record(r: dict, n: int) -> dict:
+    if "seconds_per_step" not in r:
+        return r
+    return {"value": n / r["seconds_per_step"], "unit": "body-steps/s",
+            "ms_per_step": r["seconds_per_step"] * 1e3, "max_stack": r["max_stack"],
+            "how": REF_GPU_HOW}
+
+
+def reference_gpu_records(args, m, p, v) -> dict:
+    """The reference's own GPU path, where its 32-entry stack (CU:400) holds:
+    the benchmark workload when the oracle's replay certifies it (else the
+    refusal, with the stack depth the replay found), and always the jittered
+    262,144-body grid, which it certifies."""
+    from oracle import refgpu
+
+    out = {}
+    steps = max(1, min(args.steps, 5))
+    if args.kind != "grid":
+        out[args.workload] = _ref_gpu_record(
+            refgpu.time_steps(m, p, v, theta=args.theta, steps=steps), args.n)
+    nb = _package()
+    gm, gp, gv = nb.universes.make("grid", 262144, 0)
+    rec = _ref_gpu_record(refgpu.time_steps(gm, gp, gv, theta=0.5, steps=steps), 262144)
+    rec["case"] = GRID_CASE
+    out["grid256k"] = rec
+    return out
 
 
 def run_reference_ensemble(args, refcpu, cores: int, world: int) -> None:
@@ -501,6 +551,7 @@ def run_ours(args) -> None:
                 "target_ratio": 2.0}
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.n, args.theta, m, p, v)
+        line["gpu_baseline"] = gpu_baseline(nb, local)
     if rank == 0 and args.workload == "collision4m" and not args.no_sub_configs:
         line["configs"] = sub_configs(args, nb, local)
     if world > 1:
@@ -827,6 +878,7 @@ WORKLOADS = {
     "disc16k": ("disc", 16384, 0.5),
     "plummer16m": ("plummer", 16777216, 0.5),
     "ensemble512": ("ensemble", 0, 0.5),
+    "grid256k": ("grid", 262144, 0.5),
 }
 
 

@@ -84,6 +84,9 @@ typedef struct nb_params {
     double bmax_ratio;      /* SPLIT: a cell is accepted only if also b_max < bmax_ratio * d,
                                b_max = distance from its COM to its farthest corner
                                (Barnes' b_max test); 0 = off.  FP64 mode ignores it */
+    double band_theta;      /* learned mode: the opening angle of the plain walk the
+                               correction stands in for; cells accepted at theta that
+                               this angle would open get the network's term (0 = 0.5) */
 } nb_params;
 
 typedef struct nb_stats {
@@ -99,7 +102,8 @@ typedef struct nb_stats {
 
 typedef struct nb_ctx nb_ctx;
 
-/* Fills *p with G=1, dt=1e-4, theta=0.5, epsilon_squared=1e-4, FP64 mode. */
+/* Fills *p with G=1, dt=1e-4, theta=0.5, epsilon_squared=1e-4, FP64 mode,
+ * band_theta=0.5, everything else 0. */
 NB_API int nb_params_default(nb_params* p);
 
 /* Replaces BarnesHutCuda::BarnesHutCuda + init_device_resources

@@ -67,6 +67,7 @@ class NbParams(C.Structure):
         ("device", C.c_int32),
         ("flags", C.c_int32),
         ("bmax_ratio", C.c_double),
+        ("band_theta", C.c_double),
     ]
 
 

@@ -209,7 +209,8 @@ __device__ __forceinline__ void walk_group(WarpLists& L, const Tree& t, int root
                                            const bool* act_body, float eps2, float theta2,
                                            int leaf_size, float* ax, float* ay,
                                            unsigned long long& ncell, unsigned long long& npair,
-                                           unsigned* err, int* band, int& nband, int band_cap) {
+                                           unsigned* err, int* band, int& nband, int band_cap,
+                                           float band2) {
     const int lane = threadIdx.x & 31;
     float bx0 = INFINITY, bx1 = -INFINITY, by0 = INFINITY, by1 = -INFINITY;
 #pragma unroll
@@ -243,22 +244,40 @@ __device__ __forceinline__ void walk_group(WarpLists& L, const Tree& t, int root
     if (lane == 0) L.stack[0] = root;
     __syncwarp();
 
-    while (size > 0) {
-        int k = min(32, size);
-        k = min(k, max(1, (kStk - size) / 3));
-        const int ref = lane < k ? L.stack[size - k + lane] : 0;
-        size -= k;
+    // The walk is software-pipelined: the records of the next batch of stack
+    // entries are loaded as soon as the batch is known (after this batch's
+    // children are pushed), so their latency overlaps this batch's body
+    // expansion and list sums.  Batches, and so the interaction lists and
+    // their order, are the same as popping at the top of each iteration.
+    int k = 0, ref = 0;
+    float4 c4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    int2 rg = make_int2(0, -1);
+    float4 cq = make_float4(0.f, 0.f, 0.f, 0.f);
+    auto pop_batch = [&](int& kk, int& rr, float4& c, int2& g, float4& q) {
+        kk = min(32, size);
+        kk = min(kk, max(1, (kStk - size) / 3));
+        rr = lane < kk ? L.stack[size - kk + lane] : 0;
+        size -= kk;
         __syncwarp();
+        if (lane < kk) {
+            // the tree is read-only while the walk runs: non-coherent loads
+            if (rr >= 0) {
+                c = __ldg(t.cell4 + rr);
+                g = __ldg(t.range + rr);
+                if (kQuad) q = __ldg(t.cellq + rr);
+            } else {
+                g = make_int2(~rr, __ldg(t.leaf_last + ~rr));
+            }
+        }
+    };
+    pop_batch(k, ref, c4, rg, cq);
+    while (k > 0) {
         int act = 0;  // 1 accept, 2 bodies, 3 open
         int bfirst = 0, bcnt = 0;
         int4 ch = make_int4(INT_MIN, INT_MIN, INT_MIN, INT_MIN);
-        float4 c4 = make_float4(0.f, 0.f, 0.f, 0.f);
         float band_d2 = 0.f;
         if (lane < k) {
-            // the tree is read-only while the walk runs: non-coherent loads
             if (ref >= 0) {
-                c4 = __ldg(t.cell4 + ref);
-                const int2 rg = __ldg(t.range + ref);
                 const bool overlap = !(rg.y < g0 || rg.x > g1);
                 const float dx = fmaxf(fabsf(c4.x - gcx) - ghx, 0.f);
                 const float dy = fmaxf(fabsf(c4.y - gcy) - ghy, 0.f);
@@ -275,10 +294,9 @@ __device__ __forceinline__ void walk_group(WarpLists& L, const Tree& t, int root
                     ch = __ldg(t.child + ref);
                 }
             } else {
-                const int b = ~ref;
                 act = 2;
-                bfirst = b;
-                bcnt = max(0, min(t.leaf_last[b], n - 1) - b + 1);
+                bfirst = rg.x;
+                bcnt = max(0, min(rg.y, n - 1) - rg.x + 1);
             }
         }
         // accepted cells
@@ -286,14 +304,11 @@ __device__ __forceinline__ void walk_group(WarpLists& L, const Tree& t, int root
         if (act == 1) {
             const int slot = ccount + __popc(acc_mask & below);
             put_entry(L.cxy, L.cm, slot, c4.x, c4.y, c4.z);
-            if (kQuad) {
-                const float4 q = t.cellq[ref];
-                put_entry(L.qa, L.qb, slot, q.x, q.y, q.z);
-            }
+            if (kQuad) put_entry(L.qa, L.qb, slot, cq.x, cq.y, cq.z);
         }
         if (kLearned) {
             // band: accepted here but opened by the plain theta_B walk
-            const bool in_band = act == 1 && c4.w >= kThetaBand * kThetaBand * band_d2;
+            const bool in_band = act == 1 && c4.w >= band2 * band_d2;
             const unsigned bm = __ballot_sync(kFull, in_band);
             if (in_band) {
                 const int slot = nband + __popc(bm & below);
@@ -336,6 +351,9 @@ __device__ __forceinline__ void walk_group(WarpLists& L, const Tree& t, int root
             if (nch > 3) dst[3] = ch.w;
         }
         size += pushed;
+        // the next batch: its loads run while this batch's bodies are summed
+        k = 0;
+        if (size > 0) pop_batch(k, ref, c4, rg, cq);
         // bodies of directly summed cells and leaves, expanded 32 at a time
         int btot;
         const int boff = warp_exclusive_sum(bcnt, btot);
@@ -397,7 +415,8 @@ template <bool kQuad, int kBPL, bool kLearned, bool kZeroSoft>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32)
 force_split(double2* __restrict__ pos, double2* __restrict__ vel, double2* __restrict__ acc_out,
             float2* __restrict__ acc32, int n, Tree t, DeviceScalars* __restrict__ s, Batch bt,
-            float eps2, float theta2, int leaf_size, double G_dt, double dt, int kick) {
+            float eps2, float theta2, int leaf_size, double G_dt, double dt, int kick,
+            float band2) {
     __shared__ WarpLists lists[kWarpsPerBlock];
     const int lane = threadIdx.x & 31;
     WarpLists& L = lists[threadIdx.x >> 5];
@@ -431,7 +450,7 @@ force_split(double2* __restrict__ pos, double2* __restrict__ vel, double2* __res
         int* band = kLearned ? t.band + (int64_t)kBandPerBody * g0 : nullptr;
         walk_group<kQuad, kBPL, kLearned, kZeroSoft>(L, t, root, n, g0, g1, px, py, on, eps2, theta2,
                                           leaf_size, ax, ay, ncell, npair, &s->error, band, nband,
-                                          kBandPerBody * (g1 - g0 + 1));
+                                          kBandPerBody * (g1 - g0 + 1), band2);
         if (kLearned) {
             // the correction kernel adds the learned term, then kicks and drifts
             if (lane == 0) t.band_count[g] = nband;
@@ -483,7 +502,8 @@ void launch_split_soft(nb_ctx* c, const BodyBuffers& b, bool kick, bool store_ac
     const int leaf = c->p.leaf_size > 0 ? c->p.leaf_size : kDefaultLeaf;
     force_split<kQuad, kBPL, kLearned, kZeroSoft><<<grid, 32 * kWarpsPerBlock, 0, c->stream>>>(
         b.pos, b.vel, store_acc ? c->acc : nullptr, c->acc32, (int)c->n, c->tree, c->scal, c->batch,
-        eps2, theta2, leaf, c->p.G * c->p.timestep, c->p.timestep, kick ? 1 : 0);
+        eps2, theta2, leaf, c->p.G * c->p.timestep, c->p.timestep, kick ? 1 : 0,
+        band_theta(c) * band_theta(c));
 }
 
 // eps2 = 0 takes the variant whose terms skip coincident FP32 points
@@ -504,8 +524,12 @@ int split_group_size(const nb_ctx* c) { return 32 * (c->bpl == 1 ? 1 : kBodiesPe
 void launch_force_split(nb_ctx* c, const BodyBuffers& b, bool kick, bool store_acc) {
     c->launches += 1;
     cudaMemsetAsync(&c->scal->group_ticket, 0, sizeof(unsigned), c->stream);
-    if (c->p.flags & NB_FLAG_LEARNED)  // the correction kernel assumes groups of 64
-        launch_split_kernel<false, kBodiesPerLane, true>(c, b, kick, store_acc);
+    if (c->p.flags & NB_FLAG_LEARNED) {  // the correction kernel assumes groups of 64
+        if (c->p.flags & NB_FLAG_QUADRUPOLE)  // the network corrects the quadrupole walk
+            launch_split_kernel<true, kBodiesPerLane, true>(c, b, kick, store_acc);
+        else
+            launch_split_kernel<false, kBodiesPerLane, true>(c, b, kick, store_acc);
+    }
     else if (c->p.flags & NB_FLAG_QUADRUPOLE)
         c->bpl == 1 ? launch_split_kernel<true, 1, false>(c, b, kick, store_acc)
                     : launch_split_kernel<true, kBodiesPerLane, false>(c, b, kick, store_acc);

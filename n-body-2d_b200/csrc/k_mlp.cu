@@ -449,13 +449,15 @@ __device__ __forceinline__ float bf16_hi(uint32_t w) { return __uint_as_float(w 
 // at the group's centre and, as target, the mean over the group's bodies of
 // the exact-minus-monopole pull (FP64 sums over the cell's bodies), in units
 // of M / d_c^2 with d_c the centre's distance.  That mean is the best single
-// correction for the whole group, which is what inference applies.
+// correction for the whole group, which is what inference applies.  When the
+// walk adds quadrupoles (quad != 0) the target is exact minus monopole minus
+// quadrupole, the residual the network then has to supply.
 constexpr int kSampleStack = 128;
 
 __global__ void __launch_bounds__(kWarps * 32)
 mlp_samples_kernel(Tree t, const DeviceScalars* __restrict__ s, const double2* __restrict__ pos,
                    const double* __restrict__ mass, int n, const int* __restrict__ pick, int npick,
-                   float thL2, float thB2, double eps2, float* __restrict__ X,
+                   float thL2, float thB2, double eps2, int quad, float* __restrict__ X,
                    float* __restrict__ Y, unsigned* __restrict__ count, unsigned cap) {
     __shared__ int stacks[kWarps][kSampleStack];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -522,6 +524,13 @@ mlp_samples_kernel(Tree t, const DeviceScalars* __restrict__ s, const double2* _
             // mean over the group's bodies of (exact - monopole), FP64
             const double M = t.mass[ref];
             const double2 c = t.com[ref];
+            double sxx = 0.0, sxy = 0.0, syy = 0.0;
+            if (quad) {
+                const float4 q = t.cellq[ref];
+                sxx = q.x;
+                sxy = q.y;
+                syy = q.z;
+            }
             double rx = 0.0, ry = 0.0;
 #pragma unroll
             for (int b = 0; b < 2; ++b) {
@@ -540,6 +549,15 @@ mlp_samples_kernel(Tree t, const DeviceScalars* __restrict__ s, const double2* _
                 const double am = M / (r2 * sqrt(r2));
                 rx += ax - mx * am;
                 ry += ay - my * am;
+                if (quad) {
+                    // the walk's second-moment term (the softened potential's):
+                    // d [-1.5 tr(S) r^-5 + 7.5 (d.S.d) r^-7] - 3 r^-5 S d
+                    const double ir2 = 1.0 / r2, ir5 = ir2 * ir2 / sqrt(r2), ir7 = ir5 * ir2;
+                    const double sdx = sxx * mx + sxy * my, sdy = sxy * mx + syy * my;
+                    const double radial = -1.5 * (sxx + syy) * ir5 + 7.5 * (mx * sdx + my * sdy) * ir7;
+                    rx -= mx * radial - 3.0 * ir5 * sdx;
+                    ry -= my * radial - 3.0 * ir5 * sdy;
+                }
             }
             for (int o = 16; o > 0; o >>= 1) {
                 rx += __shfl_xor_sync(kFull, rx, o);
@@ -1148,10 +1166,10 @@ void launch_mlp_correct(nb_ctx* c, const BodyBuffers& b, bool kick, bool store_a
 
 void launch_mlp_samples(nb_ctx* c, const BodyBuffers& b, const int* pick, int npick, float* X,
                         float* Y, unsigned* count, unsigned cap) {
-    const float thL = (float)c->p.theta, thB = kThetaBand;
+    const float thL = (float)c->p.theta, thB = band_theta(c);
     mlp_samples_kernel<<<c->sm_count * 8, kWarps * 32, 0, c->stream>>>(
         c->tree, c->scal, b.pos, b.mass, (int)c->n, pick, npick, thL * thL, thB * thB,
-        c->p.epsilon_squared, X, Y, count, cap);
+        c->p.epsilon_squared, (c->p.flags & NB_FLAG_QUADRUPOLE) ? 1 : 0, X, Y, count, cap);
 }
 
 size_t mlp_forward_image_bytes() { return sizeof(UmmaW); }

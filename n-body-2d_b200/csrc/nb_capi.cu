@@ -41,9 +41,11 @@ cudaError_t dalloc(T** p, size_t count) {
 int check_params(const nb_params* p) {
     if (!p) return NB_ERR_INVALID;
     if (!std::isfinite(p->G) || !std::isfinite(p->timestep) || !std::isfinite(p->theta) ||
-        !std::isfinite(p->epsilon_squared) || !std::isfinite(p->bmax_ratio))
+        !std::isfinite(p->epsilon_squared) || !std::isfinite(p->bmax_ratio) ||
+        !std::isfinite(p->band_theta))
         return NB_ERR_INVALID;
-    if (p->theta < 0.0 || p->epsilon_squared < 0.0 || p->bmax_ratio < 0.0) return NB_ERR_INVALID;
+    if (p->theta < 0.0 || p->epsilon_squared < 0.0 || p->bmax_ratio < 0.0 || p->band_theta < 0.0)
+        return NB_ERR_INVALID;
     if (p->mode != NB_MODE_FP64 && p->mode != NB_MODE_SPLIT && p->mode != NB_MODE_ALLPAIRS)
         return NB_ERR_INVALID;
     if (p->leaf_size < 0 ||
@@ -379,6 +381,7 @@ int nb_params_default(nb_params* p) {
     p->theta = 0.5;
     p->epsilon_squared = 1e-4;
     p->mode = NB_MODE_FP64;
+    p->band_theta = 0.5;
     return NB_OK;
 }
 

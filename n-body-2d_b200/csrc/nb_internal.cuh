@@ -18,7 +18,7 @@ constexpr int kSortTileItems = 12; // keys per thread in a radix tile
 constexpr int kSortThreads = 256;
 constexpr int kSortTile = kSortTileItems * kSortThreads;  // 3072 keys
 constexpr int kPhases = 8;        // morton, sort, gather, tree, moments, groups, force, drift
-constexpr float kThetaBand = 0.5f; // learned mode: cells the plain 0.5 walk would open get the MLP
+constexpr float kThetaBand = 0.5f; // learned mode: the default plain walk the MLP stands in for
 constexpr int kBandPerBody = 16;   // learned mode: band-list capacity per body of a group
 
 // Device error flags (bit mask in DeviceScalars::error).
@@ -218,6 +218,12 @@ struct nb_ctx {
 };
 
 namespace nb {
+
+// Learned mode: opening angle of the plain walk whose extra openings the
+// network replaces (band cells: accepted at theta, opened at this angle).
+inline float band_theta(const nb_ctx* c) {
+    return c->p.band_theta > 0.0 ? (float)c->p.band_theta : kThetaBand;
+}
 
 // Centre of the FP32 frame of body slot i, and the squared width of a cell at
 // tree level `level` whose first body is slot i.

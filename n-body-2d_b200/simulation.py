@@ -69,6 +69,7 @@ class SimConfig:
     quadrupole: bool = False
     learned: bool = False
     bmax_ratio: float = 0.0
+    band_theta: float = 0.5  # learned mode: the plain walk's angle the network stands in for
     cpu_law: bool = False   # NB_MODE_ALLPAIRS: the reference CPU backends' pair law
 
     def params(self) -> NbParams:
@@ -82,6 +83,7 @@ class SimConfig:
         p.leaf_size = self.leaf_size
         p.device = self.device
         p.bmax_ratio = self.bmax_ratio
+        p.band_theta = self.band_theta
         p.flags = ((_lib.NB_FLAG_QUADRUPOLE if self.quadrupole else 0)
                    | (_lib.NB_FLAG_LEARNED if self.learned else 0)
                    | (_lib.NB_FLAG_CPU_LAW if self.cpu_law else 0))

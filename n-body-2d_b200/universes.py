@@ -18,6 +18,12 @@ kind of input in code units (G = 1) with every choice pinned here:
   uniform azimuths, isotropic Gaussian velocities of dispersion ``sigma``.
 * ensemble: per-universe seeds, sizes log-uniform in [nmin, nmax], scale
   lengths uniform in [0.5, 2], central-mass ratios log-uniform in [1e3, 1e6].
+* jittered_grid: side x side equal masses 1/n on a square lattice of width
+  ``size``, each moved by up to +-jitter/2 lattice spacings, Gaussian
+  velocities of dispersion ``sigma``.  Its tree is shallow and even, so the
+  reference's GPU walk stays inside its 32-entry stack
+  (src/Simulation/src/BarnesHutCuda.cu:400) at 262,144 bodies, unlike the
+  discs.
 
 Arrays come back as (mass[n], pos[n, 2], vel[n, 2]) float64, C-contiguous,
 matching the Bodies host layout (interleaved x, y).
@@ -83,6 +89,16 @@ def plummer_disc(n: int, seed: int, *, a: float = 1.0, sigma: float = 0.3,
     return mass, np.ascontiguousarray(pos), np.ascontiguousarray(vel)
 
 
+def jittered_grid(side: int, seed: int, *, jitter: float = 0.5, size: float = 10.0,
+                  sigma: float = 0.01) -> Universe:
+    rng = np.random.default_rng(seed)
+    ij = np.stack(np.meshgrid(np.arange(side), np.arange(side), indexing="ij"), -1).reshape(-1, 2)
+    pos = (ij + 0.5 + (rng.random(ij.shape) - 0.5) * jitter) * (size / side)
+    n = pos.shape[0]
+    vel = rng.standard_normal((n, 2)) * sigma
+    return np.full(n, 1.0 / n), np.ascontiguousarray(pos), np.ascontiguousarray(vel)
+
+
 def ensemble_sizes(count: int, seed: int, nmin: int = 1024, nmax: int = 262144) -> np.ndarray:
     rng = np.random.default_rng([seed, 0])
     return np.exp(rng.uniform(np.log(nmin), np.log(nmax), count)).astype(np.int64)
@@ -123,4 +139,9 @@ def make(kind: str, n: int, seed: int = 0) -> Universe:
         return colliding_discs(n, seed)
     if kind == "plummer":
         return plummer_disc(n, seed)
+    if kind == "grid":
+        side = int(round(np.sqrt(n)))
+        if side * side != n:
+            raise ValueError("a jittered grid needs a square body count")
+        return jittered_grid(side, seed)
     raise ValueError(f"unknown universe kind {kind!r}")

@@ -33,6 +33,8 @@ def max_stack(mass, pos, vel, *, theta, steps, eps2, dt, G) -> int:
     worst = 0
     for _ in range(steps):
         worst = max(worst, st.step(theta=theta, eps2=eps2, dt=dt, G=G)["stats"]["max_stack"])
+        if worst > STACK_LIMIT:
+            break  # refused already; later steps cannot lower it
     return worst
 
 
