@@ -549,6 +549,9 @@ def run_ours(args) -> None:
                 "ratio": lv["speedup_vs_plain"], "learned_p50": lv["p50"], "learned_p99": lv["p99"],
                 "plain_p99": accuracy["p99"], "fallback_rule": lv["fallback_rule"],
                 "target_ratio": 2.0}
+    if (rank == 0 and not args.no_learned_comparison and args.workload == "collision4m"
+            and args.mode == "split" and not args.learned and not args.quad and not args.bmax):
+        line["at_accuracy_bar"] = at_accuracy_bar(args, nb, m, p, v, local)
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.n, args.theta, m, p, v)
         line["gpu_baseline"] = gpu_baseline(nb, local)
@@ -580,12 +583,14 @@ def _hbm_rooflines(phases: dict, n: int, fp64: bool, passes: int = 8) -> dict:
 
 
 def _timed_context(nb, cfg, m, p, v, warmup: int, steps: int, counts=None, error_sample=65536,
-                   accuracy=True, autotune=False) -> dict:
+                   accuracy=True, autotune=False, weights=None) -> dict:
     """W + K graph-launched steps of one context, device-timed, with the phase
     times and (optionally) the p50/p99 force error of the state after them."""
     from nbody_b200 import accuracy as acc_mod
 
     with nb.NbContext(cfg, m, p, v, counts=counts) as ctx:
+        if weights is not None:
+            ctx.set_mlp_weights(weights)
         tuned = ctx.autotune(2) if autotune else None
         ctx.step(warmup)
         ctx.step(steps, sync=False)
@@ -822,6 +827,46 @@ def _learned_weights():
     record = weights.with_suffix(".json")
     bmax = json.loads(record.read_text()).get("bmax_ratio", 0.0) if record.exists() else 0.0
     return np.load(weights), bmax
+
+
+# The comparison at the accuracy bar (p99 relative force error <= 1e-3
+# against FP64 all-pairs): neither walk of the literal comparison reaches it
+# on the colliding discs (plain theta = 0.5 has p99 ~2e-2), so the bar is met
+# by the analytic quadrupole walk at a smaller angle.  PLAIN_AT_BAR is the
+# fastest plain walk measured to meet it on this workload; LEARNED_AT_BAR
+# walks at a larger angle and lets the network (trained on the quadrupole
+# walk's residuals, band = cells PLAIN_AT_BAR would open) supply the rest.
+PLAIN_AT_BAR = dict(theta=0.35, quadrupole=True)
+LEARNED_AT_BAR = dict(theta=0.5, quadrupole=True, learned=True, band_theta=0.35)
+LEARNED_AT_BAR_WEIGHTS = "correction_quad_theta0.5"
+ACCURACY_BAR = 1e-3
+
+
+def at_accuracy_bar(args, nb, m, p, v, device) -> dict:
+    """Plain and learned steps at the accuracy bar, timed like the main line
+    (W + K graph-launched steps, CUDA events), each with its p50/p99 against
+    FP64 all-pairs on 65,536 targets; the learned step falls back to the
+    plain one when its p99 misses the bar."""
+    out = {"bar_p99": ACCURACY_BAR}
+    mk = lambda **kw: nb.SimConfig(timestep=1e-4, epsilon_squared=1e-4, G=1.0,
+                                   mode=nb.NB_MODE_SPLIT, device=device, **kw)
+    plain = _timed_context(nb, mk(**PLAIN_AT_BAR), m, p, v, args.warmup, args.steps,
+                           error_sample=args.error_sample)
+    out["plain"] = dict(config=PLAIN_AT_BAR, **plain)
+    wfile = PKG / "weights" / f"{LEARNED_AT_BAR_WEIGHTS}.npy"
+    if not wfile.exists():
+        out["learned"] = {"unavailable": f"no trained weights {wfile.name}"}
+        return out
+    learned = _timed_context(nb, mk(**LEARNED_AT_BAR), m, p, v, args.warmup, args.steps,
+                             error_sample=args.error_sample, weights=np.load(wfile))
+    out["learned"] = dict(config=LEARNED_AT_BAR, weights=wfile.name, **learned)
+    out["ratio"] = learned["value"] / plain["value"]
+    out["plain_meets_bar"] = plain["p99"] <= ACCURACY_BAR
+    out["learned_meets_bar"] = learned["p99"] <= ACCURACY_BAR
+    out["fallback_rule"] = ("kept" if learned["p99"] <= ACCURACY_BAR
+                            else "falls back to the plain step (learned p99 above the bar)")
+    out["target_ratio"] = 2.0
+    return out
 
 
 def run_variants(args, nb, m, p, v, device, plain_value, plain_accuracy, only=None) -> dict:
