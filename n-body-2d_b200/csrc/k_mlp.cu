@@ -1134,6 +1134,340 @@ mlp_forward_tc(const UmmaW* __restrict__ Wg, const float* __restrict__ X, int64_
     }
 }
 
+// ---- training on tcgen05: loss and gradients of a batch -----------------
+// One CTA of 128 threads per SM walks 128-row tiles of the batch; row r of a
+// tile is thread r and TMEM lane r.  Per tile, one thread issues
+//   L1  h1 = tanh(x W1^T + b1)        M 128, N 64, K 16
+//   L2  h2 = tanh(h1 W2^T + b2)       M 128, N 64, K 64
+//   L3  y  = h2 W3^T + b3             M 128, N 16 (2 used), K 64
+//   L4  dh1 = dp2 W2                  M 128, N 64, K 64   (dp2 = dy W3 (1 - h2^2))
+// and, with the batch as K, the weight gradients accumulated in TMEM across
+// the CTA's tiles:
+//   [dp2^T; dp1^T] [h1^T; x^T; 1]     M 128, N 80, K 128: dW2, db2 (rows 0-63),
+//                                     dW1, db1 (rows 64-127)
+//   [dy^T; 0]      [h2^T; 1; 0]       M 128, N 80, K 128: dW3, db3 (rows 0-1)
+// The transposed operands are written K-major by the epilogue threads, each
+// its own column.  BF16 rounding points are those of the mma.sync kernel
+// (inputs, weights, h1, h2, dy, dp2, dp1 enter the products as BF16; the bias
+// sums take the BF16 dp and dy here).
+constexpr uint32_t kGtCols = 256;      // TMEM columns: weight-gradient sums + layer accumulator
+constexpr uint32_t kGtDwg = 0;         // [dW2 | dW1 | db] accumulator, 80 columns
+constexpr uint32_t kGtDw3 = 96;        // [dW3 | db3] accumulator, 80 columns
+constexpr uint32_t kGtLayer = 192;     // L1..L4 accumulators, 64 columns, reused
+
+struct GtW {                            // BF16 K-major images of the weights
+    alignas(128) uint4 w1[kH * 16 / 8];     // n = hidden x k = input (natural order, 12 used)
+    alignas(128) uint4 w2[kH * kH / 8];     // n = out x k = in
+    alignas(128) uint4 w3[16 * kH / 8];     // n = out (2 used) x k = hidden
+    alignas(128) uint4 w2t[kH * kH / 8];    // n = in x k = out
+    float b1[kH], b2[kH], b3[2];
+    float w3f[2][kH];                       // W3 rounded to BF16, for dp2 on the CUDA cores
+};
+
+struct GtSmem {
+    GtW W;
+    alignas(128) uint4 a1[kTcRows * 16 / 8];     // x rows (K = 16), column 12 = 1 on valid rows
+    alignas(128) uint4 a2[kTcRows * kH / 8];     // h1, then h2, then dp2 rows (K = 64)
+    alignas(128) uint4 at[kTcRows * kTcRows / 8];  // [dp2^T; dp1^T] (K = 128 rows of the tile)
+    alignas(128) uint4 bt1[80 * kTcRows / 8];    // [h1^T; x^T with the ones row] (K = 128)
+    alignas(128) uint4 bt3[80 * kTcRows / 8];    // [h2^T; ones row; 0]
+    alignas(128) uint4 a5[kTcRows * kTcRows / 8];  // [dy^T; 0]
+    alignas(8) uint64_t mbar;
+    uint32_t tmem;
+    int fail;
+    float loss;
+};
+
+__global__ void mlp_prepare_train_tc(const float* __restrict__ p, GtW* __restrict__ W) {
+    auto put = [](uint4* img, int off, float v) {
+        reinterpret_cast<__nv_bfloat16*>(img)[off / 2] = __float2bfloat16_rn(v);
+    };
+    for (int e = threadIdx.x; e < kH * 16; e += blockDim.x) {
+        const int n = e / 16, k = e % 16;
+        put(W->w1, umma_off(n, k, 256), k < kNin ? p[kW1 + n * kNin + k] : 0.f);
+    }
+    for (int e = threadIdx.x; e < kH * kH; e += blockDim.x) {
+        const int n = e / kH, k = e % kH;
+        put(W->w2, umma_off(n, k, 1024), p[kW2 + n * kH + k]);
+        put(W->w2t, umma_off(n, k, 1024), p[kW2 + k * kH + n]);
+    }
+    for (int e = threadIdx.x; e < 16 * kH; e += blockDim.x) {
+        const int n = e / kH, k = e % kH;
+        put(W->w3, umma_off(n, k, 1024), n < 2 ? p[kW3 + n * kH + k] : 0.f);
+    }
+    for (int e = threadIdx.x; e < kH; e += blockDim.x) {
+        W->b1[e] = p[kB1 + e];
+        W->b2[e] = p[kB2 + e];
+        W->w3f[0][e] = bf16_round(p[kW3 + e]);
+        W->w3f[1][e] = bf16_round(p[kW3 + kH + e]);
+    }
+    if (threadIdx.x < 2) W->b3[threadIdx.x] = p[kB3 + threadIdx.x];
+}
+
+// element (row, k) of a K-major operand with 128 columns of K
+__device__ __forceinline__ void put_t(uint4* img, int row, int k, float v) {
+    reinterpret_cast<__nv_bfloat16*>(img)[umma_off(row, k, 2048) / 2] = __float2bfloat16_rn(v);
+}
+
+// Issues one MMA group (thread 0) and waits for it (every thread, bounded).
+template <typename F>
+__device__ __forceinline__ void gt_mma(GtSmem& S, uint32_t& phase, F issue) {
+    tc_fence_before();
+    fence_async_smem();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        tc_fence_after();
+        issue();
+        umma_commit(&S.mbar);
+    }
+    if (!mbar_wait(&S.mbar, phase)) S.fail = 1;
+    phase ^= 1u;
+    tc_fence_after();
+}
+
+__global__ void __launch_bounds__(kTcRows, 1)
+mlp_grad_tc(const GtW* __restrict__ Wg, const float* __restrict__ X, const float* __restrict__ Yt,
+            const int64_t* __restrict__ idx, int64_t n, float inv_n, float* __restrict__ grad,
+            float* __restrict__ loss, unsigned* __restrict__ err) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    GtSmem& S = *reinterpret_cast<GtSmem*>(smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u));
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    {
+        const uint4* src = reinterpret_cast<const uint4*>(Wg);
+        uint4* dst = reinterpret_cast<uint4*>(&S.W);
+        for (int k = tid; k < (int)(sizeof(GtW) / 16); k += blockDim.x) dst[k] = src[k];
+        // operands whose other rows stay zero: [dy^T; 0], [h2^T; 1; 0], x^T's padding rows
+        for (int k = tid; k < kTcRows * kTcRows / 8; k += blockDim.x) S.a5[k] = make_uint4(0, 0, 0, 0);
+        for (int k = tid; k < 80 * kTcRows / 8; k += blockDim.x) {
+            S.bt1[k] = make_uint4(0, 0, 0, 0);
+            S.bt3[k] = make_uint4(0, 0, 0, 0);
+        }
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&S.mbar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        S.fail = 0;
+        S.loss = 0.f;
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     :: "r"(smem_u32(&S.tmem)), "r"(kGtCols) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = S.tmem;
+    const uint32_t tlane = tmem + ((uint32_t)(32 * warp) << 16);
+    const uint32_t a1 = smem_u32(S.a1), a2 = smem_u32(S.a2), at = smem_u32(S.at),
+                   bt1 = smem_u32(S.bt1), bt3 = smem_u32(S.bt3), a5 = smem_u32(S.a5);
+    const uint32_t w1 = smem_u32(S.W.w1), w2 = smem_u32(S.W.w2), w3 = smem_u32(S.W.w3),
+                   w2t = smem_u32(S.W.w2t);
+    const int r = tid;
+    uint32_t phase = 0;
+    bool first = true;
+    float my_loss = 0.f;
+    for (int64_t tile = blockIdx.x; tile * kTcRows < n; tile += gridDim.x) {
+        if (S.fail) break;  // uniform: written before the barrier that ended the last wait
+        const int64_t s = tile * kTcRows + r;
+        const bool valid = s < n;
+        const int64_t src = valid ? (idx ? idx[s] : s) : 0;
+        // x: the row (A of L1) and its column of x^T (B of the weight gradients)
+        {
+            float x[16];
+#pragma unroll
+            for (int k = 0; k < 16; ++k)
+                x[k] = valid && k < kNin ? X[src * kNin + k] : (valid && k == kNin ? 1.f : 0.f);
+            uint32_t w[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) w[k] = pack_bf16(x[2 * k], x[2 * k + 1]);
+            uint4* dst = S.a1 + umma_off(r, 0, 256) / 16;
+            dst[0] = make_uint4(w[0], w[1], w[2], w[3]);
+            dst[8] = make_uint4(w[4], w[5], w[6], w[7]);
+#pragma unroll
+            for (int k = 0; k < 13; ++k) put_t(S.bt1, kH + k, r, x[k]);
+        }
+        const float t0 = valid ? Yt[2 * src] : 0.f, t1 = valid ? Yt[2 * src + 1] : 0.f;
+        gt_mma(S, phase, [&] {
+            umma_bf16(tmem + kGtLayer, umma_desc(a1, 128, 256), umma_desc(w1, 128, 256),
+                      umma_idesc(kTcRows, kH), 0u);
+        });
+        // h1 = bf16(tanh(. + b1)): row of L2's A, column of h1^T, kept for dp1
+        uint32_t h1p[32];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            uint32_t v[16];
+            tmem_ld16(tlane + kGtLayer + 16 * c, v);
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const int o = 16 * c + 2 * j;
+                h1p[8 * c + j] = pack_bf16(tanh_fast(__uint_as_float(v[2 * j]) + S.W.b1[o]),
+                                           tanh_fast(__uint_as_float(v[2 * j + 1]) + S.W.b1[o + 1]));
+            }
+            uint4* dst = S.a2 + umma_off(r, 16 * c, 1024) / 16;
+            dst[0] = make_uint4(h1p[8 * c], h1p[8 * c + 1], h1p[8 * c + 2], h1p[8 * c + 3]);
+            dst[8] = make_uint4(h1p[8 * c + 4], h1p[8 * c + 5], h1p[8 * c + 6], h1p[8 * c + 7]);
+        }
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+            put_t(S.bt1, 2 * j, r, bf16_lo(h1p[j]));
+            put_t(S.bt1, 2 * j + 1, r, bf16_hi(h1p[j]));
+        }
+        gt_mma(S, phase, [&] {
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                umma_bf16(tmem + kGtLayer, umma_desc(a2 + 256u * j, 128, 1024),
+                          umma_desc(w2 + 256u * j, 128, 1024), umma_idesc(kTcRows, kH),
+                          j > 0 ? 1u : 0u);
+        });
+        uint32_t h2p[32];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            uint32_t v[16];
+            tmem_ld16(tlane + kGtLayer + 16 * c, v);
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const int o = 16 * c + 2 * j;
+                h2p[8 * c + j] = pack_bf16(tanh_fast(__uint_as_float(v[2 * j]) + S.W.b2[o]),
+                                           tanh_fast(__uint_as_float(v[2 * j + 1]) + S.W.b2[o + 1]));
+            }
+            uint4* dst = S.a2 + umma_off(r, 16 * c, 1024) / 16;
+            dst[0] = make_uint4(h2p[8 * c], h2p[8 * c + 1], h2p[8 * c + 2], h2p[8 * c + 3]);
+            dst[8] = make_uint4(h2p[8 * c + 4], h2p[8 * c + 5], h2p[8 * c + 6], h2p[8 * c + 7]);
+        }
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+            put_t(S.bt3, 2 * j, r, bf16_lo(h2p[j]));
+            put_t(S.bt3, 2 * j + 1, r, bf16_hi(h2p[j]));
+        }
+        put_t(S.bt3, kH, r, valid ? 1.f : 0.f);
+        gt_mma(S, phase, [&] {
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                umma_bf16(tmem + kGtLayer, umma_desc(a2 + 256u * j, 128, 1024),
+                          umma_desc(w3 + 256u * j, 128, 1024), umma_idesc(kTcRows, 16),
+                          j > 0 ? 1u : 0u);
+        });
+        float dy0 = 0.f, dy1 = 0.f;
+        {
+            uint32_t y0, y1;
+            tmem_ld2(tlane + kGtLayer, y0, y1);
+            if (valid) {
+                const float d0 = __uint_as_float(y0) + S.W.b3[0] - t0;
+                const float d1 = __uint_as_float(y1) + S.W.b3[1] - t1;
+                my_loss += d0 * d0 + d1 * d1;
+                dy0 = bf16_round(2.f * d0 * inv_n);
+                dy1 = bf16_round(2.f * d1 * inv_n);
+            }
+        }
+        put_t(S.a5, 0, r, dy0);
+        put_t(S.a5, 1, r, dy1);
+        // dp2 = (dy W3) (1 - h2^2): a row of L4's A and a column of dp2^T
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            uint32_t w[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const int o = 16 * c + 2 * j;
+                const float ha = bf16_lo(h2p[8 * c + j]), hb = bf16_hi(h2p[8 * c + j]);
+                const float pa = fmaf(dy0, S.W.w3f[0][o], dy1 * S.W.w3f[1][o]) * (1.f - ha * ha);
+                const float pb =
+                    fmaf(dy0, S.W.w3f[0][o + 1], dy1 * S.W.w3f[1][o + 1]) * (1.f - hb * hb);
+                w[j] = pack_bf16(pa, pb);
+                put_t(S.at, o, r, pa);
+                put_t(S.at, o + 1, r, pb);
+            }
+            uint4* dst = S.a2 + umma_off(r, 16 * c, 1024) / 16;
+            dst[0] = make_uint4(w[0], w[1], w[2], w[3]);
+            dst[8] = make_uint4(w[4], w[5], w[6], w[7]);
+        }
+        gt_mma(S, phase, [&] {
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                umma_bf16(tmem + kGtLayer, umma_desc(a2 + 256u * j, 128, 1024),
+                          umma_desc(w2t + 256u * j, 128, 1024), umma_idesc(kTcRows, kH),
+                          j > 0 ? 1u : 0u);
+        });
+        // dp1 = dh1 (1 - h1^2): a column of dp1^T
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            uint32_t v[16];
+            tmem_ld16(tlane + kGtLayer + 16 * c, v);
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const int o = 16 * c + 2 * j;
+                const float ha = bf16_lo(h1p[8 * c + j]), hb = bf16_hi(h1p[8 * c + j]);
+                put_t(S.at, kH + o, r, valid ? __uint_as_float(v[2 * j]) * (1.f - ha * ha) : 0.f);
+                put_t(S.at, kH + o + 1, r,
+                      valid ? __uint_as_float(v[2 * j + 1]) * (1.f - hb * hb) : 0.f);
+            }
+        }
+        // weight and bias gradients of the tile, added to the CTA's sums
+        const uint32_t acc = first ? 0u : 1u;
+        gt_mma(S, phase, [&] {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                umma_bf16(tmem + kGtDwg, umma_desc(at + 256u * j, 128, 2048),
+                          umma_desc(bt1 + 256u * j, 128, 2048), umma_idesc(kTcRows, 80),
+                          j > 0 ? 1u : acc);
+                umma_bf16(tmem + kGtDw3, umma_desc(a5 + 256u * j, 128, 2048),
+                          umma_desc(bt3 + 256u * j, 128, 2048), umma_idesc(kTcRows, 80),
+                          j > 0 ? 1u : acc);
+            }
+        });
+        first = false;
+        __syncthreads();  // S.fail is read by every thread at the top of the loop
+    }
+    for (int o = 16; o > 0; o >>= 1) my_loss += __shfl_xor_sync(kFull, my_loss, o);
+    if (lane == 0) atomicAdd(&S.loss, my_loss);
+    if (S.fail) {
+        mbar_wait(&S.mbar, phase ^ 1u);  // let an MMA in flight finish before TMEM is freed
+        if (tid == 0) atomicOr(err, kErrTimeout);
+    } else if (!first) {
+        // row r of the sums: dW2[r] and db2[r] (r < 64) or dW1[r - 64] and db1[r - 64]
+        uint32_t v[16];
+        for (int c = 0; c < 5; ++c) {
+            tmem_ld16(tlane + kGtDwg + 16 * c, v);
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                const int col = 16 * c + j;
+                const float g = __uint_as_float(v[j]);
+                if (r < kH) {
+                    if (col < kH) atomicAdd(grad + kW2 + r * kH + col, g);
+                    else if (col == kH + kNin) atomicAdd(grad + kB2 + r, g);
+                } else {
+                    if (col >= kH && col < kH + kNin)
+                        atomicAdd(grad + kW1 + (r - kH) * kNin + (col - kH), g);
+                    else if (col == kH + kNin)
+                        atomicAdd(grad + kB1 + (r - kH), g);
+                }
+            }
+        }
+        // rows 0 and 1 of the second sum: dW3 and db3
+        for (int c = 0; c < 5; ++c) {
+            tmem_ld16(tlane + kGtDw3 + 16 * c, v);
+            if (r < 2) {
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    const int col = 16 * c + j;
+                    const float g = __uint_as_float(v[j]);
+                    if (col < kH) atomicAdd(grad + kW3 + r * kH + col, g);
+                    else if (col == kH) atomicAdd(grad + kB3 + r, g);
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (tid == 0) atomicAdd(loss, S.loss * inv_n);
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
+                     :: "r"(tmem), "r"(kGtCols) : "memory");
+    }
+}
+
 inline unsigned blocks_for(int64_t n, int per) { return (unsigned)((n + per - 1) / per); }
 
 }  // namespace
@@ -1195,6 +1529,21 @@ int mlp_grad_device(const float* params, const float* X, const float* Yt, const 
     cudaFuncSetAttribute(mlp_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     mlp_grad_kernel<<<blocks, kWarps * 32, smem, st>>>(params, X, Yt, idx, n, 1.f / (float)n, grad,
                                                        loss);
+    return cudaGetLastError() == cudaSuccess ? NB_OK : NB_ERR_CUDA;
+}
+
+size_t mlp_train_image_bytes() { return sizeof(GtW); }
+
+int mlp_grad_tc_device(const float* params, const float* X, const float* Yt, const int64_t* idx,
+                       int64_t n, float* grad, float* loss, void* image, unsigned* err,
+                       int sm_count, cudaStream_t st) {
+    GtW* W = static_cast<GtW*>(image);
+    mlp_prepare_train_tc<<<1, 256, 0, st>>>(params, W);
+    const int smem = (int)(sizeof(GtSmem) + 1024);
+    cudaFuncSetAttribute(mlp_grad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    const int64_t tiles = (n + kTcRows - 1) / kTcRows;
+    const int grid = (int)std::min<int64_t>(tiles, (int64_t)sm_count);
+    mlp_grad_tc<<<grid, kTcRows, smem, st>>>(W, X, Yt, idx, n, 1.f / (float)n, grad, loss, err);
     return cudaGetLastError() == cudaSuccess ? NB_OK : NB_ERR_CUDA;
 }
 

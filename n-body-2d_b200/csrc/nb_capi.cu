@@ -1071,19 +1071,27 @@ int nb_mlp_loss_grad(int32_t device, const float* params, uint64_t n, const floa
     DeviceScope scope(device);
     if (scope.rc != NB_OK) return scope.rc;
     DBuf<float> p(NB_MLP_PARAMS), x(12 * n), y(2 * n), g(NB_MLP_PARAMS), l(1);
-    if (!p.p || !x.p || !y.p || !g.p || !l.p) return NB_ERR_NOMEM;
+    DBuf<unsigned char> image(nb::mlp_train_image_bytes());
+    DBuf<unsigned> err(1);
+    if (!p.p || !x.p || !y.p || !g.p || !l.p || !image.p || !err.p) return NB_ERR_NOMEM;
     cudaMemcpy(p.p, params, sizeof(float) * NB_MLP_PARAMS, cudaMemcpyHostToDevice);
     cudaMemcpy(x.p, features, sizeof(float) * 12 * n, cudaMemcpyHostToDevice);
     cudaMemcpy(y.p, targets, sizeof(float) * 2 * n, cudaMemcpyHostToDevice);
     cudaMemset(g.p, 0, sizeof(float) * NB_MLP_PARAMS);
     cudaMemset(l.p, 0, sizeof(float));
-    const int blocks = (int)std::min<uint64_t>((n + 63) / 64, 592);
-    if (nb::mlp_grad_device(p.p, x.p, y.p, nullptr, (int64_t)n, g.p, l.p, blocks, nullptr) != NB_OK)
+    cudaMemset(err.p, 0, sizeof(unsigned));
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (nb::mlp_grad_tc_device(p.p, x.p, y.p, nullptr, (int64_t)n, g.p, l.p, image.p, err.p,
+                               sms > 0 ? sms : 1, nullptr) != NB_OK)
         return NB_ERR_CUDA;
+    unsigned flags = 0;
     if (cudaMemcpy(grad, g.p, sizeof(float) * NB_MLP_PARAMS, cudaMemcpyDeviceToHost) != cudaSuccess ||
-        cudaMemcpy(loss, l.p, sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess)
+        cudaMemcpy(loss, l.p, sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(&flags, err.p, sizeof(unsigned), cudaMemcpyDeviceToHost) != cudaSuccess)
         return NB_ERR_CUDA;
-    return NB_OK;
+    return flags ? NB_ERR_TIMEOUT : NB_OK;
 }
 
 int nb_mlp_train(int32_t device, uint64_t n, const float* features, const float* residuals,
@@ -1125,7 +1133,12 @@ int nb_mlp_train(int32_t device, uint64_t n, const float* features, const float*
     DBuf<float> p(NB_MLP_PARAMS), x(12 * n), y(2 * n), g(NB_MLP_PARAMS), m(NB_MLP_PARAMS),
         v(NB_MLP_PARAMS), l(1);
     DBuf<int64_t> idx(n);
-    if (!p.p || !x.p || !y.p || !g.p || !m.p || !v.p || !l.p || !idx.p) return NB_ERR_NOMEM;
+    DBuf<unsigned char> image(nb::mlp_train_image_bytes());
+    DBuf<unsigned> err(1);
+    if (!p.p || !x.p || !y.p || !g.p || !m.p || !v.p || !l.p || !idx.p || !image.p || !err.p)
+        return NB_ERR_NOMEM;
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     cudaStream_t st = nullptr;
     if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return NB_ERR_CUDA;
     cudaMemcpyAsync(p.p, P.data(), sizeof(float) * NB_MLP_PARAMS, cudaMemcpyHostToDevice, st);
@@ -1133,6 +1146,7 @@ int nb_mlp_train(int32_t device, uint64_t n, const float* features, const float*
     cudaMemcpyAsync(y.p, T.data(), sizeof(float) * 2 * n, cudaMemcpyHostToDevice, st);
     cudaMemsetAsync(m.p, 0, sizeof(float) * NB_MLP_PARAMS, st);
     cudaMemsetAsync(v.p, 0, sizeof(float) * NB_MLP_PARAMS, st);
+    cudaMemsetAsync(err.p, 0, sizeof(unsigned), st);
     std::vector<int64_t> perm(n);
     for (uint64_t k = 0; k < n; ++k) perm[k] = (int64_t)k;
     int rc = NB_OK;
@@ -1149,9 +1163,8 @@ int nb_mlp_train(int32_t device, uint64_t n, const float* features, const float*
         for (uint64_t b0 = 0; b0 < n; b0 += B, ++nbatches) {
             const uint64_t cnt = std::min<uint64_t>(B, n - b0);
             cudaMemsetAsync(g.p, 0, sizeof(float) * NB_MLP_PARAMS, st);
-            const int blocks = (int)std::min<uint64_t>((cnt + 63) / 64, 592);
-            if (nb::mlp_grad_device(p.p, x.p, y.p, idx.p + b0, (int64_t)cnt, g.p, l.p, blocks, st) !=
-                    NB_OK ||
+            if (nb::mlp_grad_tc_device(p.p, x.p, y.p, idx.p + b0, (int64_t)cnt, g.p, l.p, image.p,
+                                       err.p, sms > 0 ? sms : 1, st) != NB_OK ||
                 nb::mlp_adam_device(p.p, g.p, m.p, v.p, tp->lr, ++step, st) != NB_OK) {
                 rc = NB_ERR_CUDA;
                 break;
@@ -1162,9 +1175,12 @@ int nb_mlp_train(int32_t device, uint64_t n, const float* features, const float*
         if (cudaStreamSynchronize(st) != cudaSuccess) rc = NB_ERR_CUDA;
         if (loss_per_epoch) loss_per_epoch[e] = lsum / (float)nbatches;
     }
+    unsigned flags = 0;
     if (rc == NB_OK) {
         cudaMemcpyAsync(P.data(), p.p, sizeof(float) * (NB_MLP_PARAMS - 1), cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(&flags, err.p, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
         if (cudaStreamSynchronize(st) != cudaSuccess) rc = NB_ERR_CUDA;
+        else if (flags) rc = NB_ERR_TIMEOUT;
         else std::memcpy(params, P.data(), sizeof(float) * NB_MLP_PARAMS);
     }
     cudaStreamDestroy(st);

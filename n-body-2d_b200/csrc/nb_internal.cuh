@@ -278,6 +278,12 @@ int mlp_grad_device(const float* params, const float* X, const float* Yt, const 
                     int64_t n, float* grad, float* loss, int blocks, cudaStream_t st);
 int mlp_adam_device(float* p, const float* g, float* m, float* v, float lr, int step,
                     cudaStream_t st);
+// training loss and gradients on tcgen05 (image = mlp_train_image_bytes() of
+// device scratch for the BF16 weight images; err receives kErrTimeout)
+size_t mlp_train_image_bytes();
+int mlp_grad_tc_device(const float* params, const float* X, const float* Yt, const int64_t* idx,
+                       int64_t n, float* grad, float* loss, void* image, unsigned* err,
+                       int sm_count, cudaStream_t st);
 void launch_groups(nb_ctx* c);
 void launch_force_split(nb_ctx* c, const BodyBuffers& b, bool kick, bool store_acc);
 void launch_force_fp64(nb_ctx* c, const BodyBuffers& b, bool kick, bool store_acc);
