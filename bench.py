@@ -836,8 +836,8 @@ def _learned_weights():
 # fastest plain walk measured to meet it on this workload; LEARNED_AT_BAR
 # walks at a larger angle and lets the network (trained on the quadrupole
 # walk's residuals, band = cells PLAIN_AT_BAR would open) supply the rest.
-PLAIN_AT_BAR = dict(theta=0.35, quadrupole=True)
-LEARNED_AT_BAR = dict(theta=0.5, quadrupole=True, learned=True, band_theta=0.35)
+PLAIN_AT_BAR = dict(theta=0.4, quadrupole=True)
+LEARNED_AT_BAR = dict(theta=0.5, quadrupole=True, learned=True, band_theta=0.4)
 LEARNED_AT_BAR_WEIGHTS = "correction_quad_theta0.5"
 ACCURACY_BAR = 1e-3
 

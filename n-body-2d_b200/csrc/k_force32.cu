@@ -244,40 +244,22 @@ __device__ __forceinline__ void walk_group(WarpLists& L, const Tree& t, int root
     if (lane == 0) L.stack[0] = root;
     __syncwarp();
 
-    // The walk is software-pipelined: the records of the next batch of stack
-    // entries are loaded as soon as the batch is known (after this batch's
-    // children are pushed), so their latency overlaps this batch's body
-    // expansion and list sums.  Batches, and so the interaction lists and
-    // their order, are the same as popping at the top of each iteration.
-    int k = 0, ref = 0;
-    float4 c4 = make_float4(0.f, 0.f, 0.f, 0.f);
-    int2 rg = make_int2(0, -1);
-    float4 cq = make_float4(0.f, 0.f, 0.f, 0.f);
-    auto pop_batch = [&](int& kk, int& rr, float4& c, int2& g, float4& q) {
-        kk = min(32, size);
-        kk = min(kk, max(1, (kStk - size) / 3));
-        rr = lane < kk ? L.stack[size - kk + lane] : 0;
-        size -= kk;
+    while (size > 0) {
+        int k = min(32, size);
+        k = min(k, max(1, (kStk - size) / 3));
+        const int ref = lane < k ? L.stack[size - k + lane] : 0;
+        size -= k;
         __syncwarp();
-        if (lane < kk) {
-            // the tree is read-only while the walk runs: non-coherent loads
-            if (rr >= 0) {
-                c = __ldg(t.cell4 + rr);
-                g = __ldg(t.range + rr);
-                if (kQuad) q = __ldg(t.cellq + rr);
-            } else {
-                g = make_int2(~rr, __ldg(t.leaf_last + ~rr));
-            }
-        }
-    };
-    pop_batch(k, ref, c4, rg, cq);
-    while (k > 0) {
         int act = 0;  // 1 accept, 2 bodies, 3 open
         int bfirst = 0, bcnt = 0;
         int4 ch = make_int4(INT_MIN, INT_MIN, INT_MIN, INT_MIN);
+        float4 c4 = make_float4(0.f, 0.f, 0.f, 0.f);
         float band_d2 = 0.f;
         if (lane < k) {
+            // the tree is read-only while the walk runs: non-coherent loads
             if (ref >= 0) {
+                c4 = __ldg(t.cell4 + ref);
+                const int2 rg = __ldg(t.range + ref);
                 const bool overlap = !(rg.y < g0 || rg.x > g1);
                 const float dx = fmaxf(fabsf(c4.x - gcx) - ghx, 0.f);
                 const float dy = fmaxf(fabsf(c4.y - gcy) - ghy, 0.f);
@@ -294,9 +276,10 @@ __device__ __forceinline__ void walk_group(WarpLists& L, const Tree& t, int root
                     ch = __ldg(t.child + ref);
                 }
             } else {
+                const int b = ~ref;
                 act = 2;
-                bfirst = rg.x;
-                bcnt = max(0, min(rg.y, n - 1) - rg.x + 1);
+                bfirst = b;
+                bcnt = max(0, min(t.leaf_last[b], n - 1) - b + 1);
             }
         }
         // accepted cells
@@ -304,7 +287,10 @@ __device__ __forceinline__ void walk_group(WarpLists& L, const Tree& t, int root
         if (act == 1) {
             const int slot = ccount + __popc(acc_mask & below);
             put_entry(L.cxy, L.cm, slot, c4.x, c4.y, c4.z);
-            if (kQuad) put_entry(L.qa, L.qb, slot, cq.x, cq.y, cq.z);
+            if (kQuad) {
+                const float4 q = t.cellq[ref];
+                put_entry(L.qa, L.qb, slot, q.x, q.y, q.z);
+            }
         }
         if (kLearned) {
             // band: accepted here but opened by the plain theta_B walk
@@ -351,9 +337,6 @@ __device__ __forceinline__ void walk_group(WarpLists& L, const Tree& t, int root
             if (nch > 3) dst[3] = ch.w;
         }
         size += pushed;
-        // the next batch: its loads run while this batch's bodies are summed
-        k = 0;
-        if (size > 0) pop_batch(k, ref, c4, rg, cq);
         // bodies of directly summed cells and leaves, expanded 32 at a time
         int btot;
         const int boff = warp_exclusive_sum(bcnt, btot);

@@ -23,7 +23,6 @@
 // tree therefore keeps only the deepest level of every chain and stores that
 // level, so opening decisions and force terms equal the reference's
 // (cell widths come from the level, never from the body range).
-#include <algorithm>
 #include <climits>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -215,8 +214,7 @@ scan_apply(const int32_t* __restrict__ in, int n, const int32_t* __restrict__ bl
 // the partials in 7-bit bit-reversed order, so a binary-counter pairwise sum
 // over that sequence reproduces it with an 8-entry stack.  Such leaves only
 // hold bodies whose codes agree in 60 bits, so they are rare and small.
-__device__ __noinline__ void bucket_moments(const double2* __restrict__ pos,
-                                            const double* __restrict__ mass,
+__device__ void bucket_moments(const double2* __restrict__ pos, const double* __restrict__ mass,
                                int first, int last, double* out_m, double2* out_c) {
     double sm[8], sx[8], sy[8];
     for (int k = 0; k < 128; ++k) {
@@ -243,219 +241,77 @@ __device__ __noinline__ void bucket_moments(const double2* __restrict__ pos,
     *out_c = make_double2(sx[7] / sm[7], sy[7] / sm[7]);
 }
 
-// Pass 3: every cell writes its range, its children and their parent links.
-//
-// A cell needs up to nine galloping searches over the sorted codes (its end,
-// its children's ends, the first split inside each internal child), of
-// lengths from one probe to ~40 for the top cells.  One thread per cell left
-// most lanes idle behind the longest search of their warp, so the lanes run
-// as small state machines instead: every iteration of one loop, each lane
-// makes one probe of its current search, and a lane whose cell is done takes
-// the next cell from a counter.  All lanes share the probe code, so the warp
-// stays converged while the searches' lengths differ.
-struct Gallop {
-    // last index e in [s, hi] whose code shares `digits` leading digits with
-    // `anchor` (= key[s]); the run of such codes starts at s
-    uint64_t anchor;
-    int s, hi, a, b, step, digits;
-    bool doubling;
-};
-
-__device__ __forceinline__ void gallop_start(Gallop& g, uint64_t anchor, int s, int hi, int digits) {
-    g.anchor = anchor;
-    g.s = s;
-    g.hi = hi;
-    g.a = s;
-    g.b = s;
-    g.step = 1;
-    g.digits = digits;
-    g.doubling = s < hi;
-}
-
-// One probe; true when the search is finished (result in g.a).
-__device__ __forceinline__ bool gallop_probe(Gallop& g, const uint64_t* __restrict__ key) {
-    if (g.doubling) {
-        const int cand = g.s + g.step;
-        if (cand <= g.hi && share(key[cand], g.anchor, g.digits)) {
-            g.a = cand;
-            g.step <<= 1;
-            return false;
-        }
-        g.doubling = false;
-        g.b = min(g.hi, g.s + g.step - 1);
-        return g.a >= g.b;
+// Pass 3: every flagged boundary writes its cell, its children and their
+// parent links.
+__global__ void tree_link(const uint64_t* __restrict__ key, int n,
+                          const double2* __restrict__ pos, const double* __restrict__ mass,
+                          Tree t, DeviceScalars* __restrict__ s) {
+    // one thread per cell, so every lane of a warp builds a cell
+    const int id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= s->cells) return;
+    const int i = t.rep_of[id];
+    const int c = lcp_digits(key[i], key[i + 1]);
+    const int first = t.start_of[i];
+    const int last = c == 0 ? n - 1 : gallop_right(key, i + 1, n - 1, c);
+    int cs[4], ce[4];
+    int nc = 1;
+    cs[0] = first;
+    ce[0] = i;
+    int p = i + 1;
+    while (p <= last && nc < 4) {
+        const int e = gallop_right(key, p, last, c + 1);
+        cs[nc] = p;
+        ce[nc] = e;
+        ++nc;
+        p = e + 1;
     }
-    if (g.a >= g.b) return true;
-    const int mid = (g.a + g.b + 1) >> 1;
-    if (share(key[mid], g.anchor, g.digits)) g.a = mid; else g.b = mid - 1;
-    return g.a >= g.b;
-}
-
-// Element k (0..3) of four scalars, without an indexed local array.
-__device__ __forceinline__ int get4(int a0, int a1, int a2, int a3, int k) {
-    return k == 0 ? a0 : k == 1 ? a1 : k == 2 ? a2 : a3;
-}
-__device__ __forceinline__ void set4(int& a0, int& a1, int& a2, int& a3, int k, int v) {
-    a0 = k == 0 ? v : a0;
-    a1 = k == 1 ? v : a1;
-    a2 = k == 2 ? v : a2;
-    a3 = k == 3 ? v : a3;
-}
-
-__global__ void __launch_bounds__(kThreads, 3)
-tree_link(const uint64_t* __restrict__ key, int n, const double2* __restrict__ pos,
-          const double* __restrict__ mass, Tree t, DeviceScalars* __restrict__ s) {
-    const int lane = threadIdx.x & 31;
-    const unsigned below = (1u << lane) - 1u;
-    const int cells = s->cells;
-    // per-lane cell state
-    int id = -1;          // -1: needs a cell, -2: no cells left
-    int i = 0, c = 0, first = 0, last = 0, p = 0, q = 0, r = 0, nint = 0;
-    int phase = 0;        // 1: the cell's end, 2: children's ends, 3: internal children's splits
-    // child k covers [start_k, start_{k+1} - 1], the last child ends at `last`;
-    // start_0 = first
-    int cs1 = 0, cs2 = 0, cs3 = 0;
-    int rf0 = INT_MIN, rf1 = INT_MIN, rf2 = INT_MIN, rf3 = INT_MIN;
-    Gallop g;
-    g.doubling = false;
-    g.a = g.b = 0;
-    bool searching = false, finished = false;
-    while (true) {
-        // lanes without a cell take the next ones, one atomic per warp
-        const bool need = id == -1;
-        const unsigned needm = __ballot_sync(kFull, need);
-        if (needm) {
-            unsigned base = 0;
-            if (lane == __ffs(needm) - 1) base = atomicAdd(&s->link_ticket, (unsigned)__popc(needm));
-            base = __shfl_sync(kFull, base, __ffs(needm) - 1);
-            if (need) {
-                const unsigned my = base + __popc(needm & below);
-                id = my < (unsigned)cells ? (int)my : -2;
-                if (id >= 0) {
-                    i = t.rep_of[id];
-                    const uint64_t k1 = key[i + 1];
-                    c = lcp_digits(key[i], k1);
-                    first = t.start_of[i];
-                    cs1 = i + 1;
-                    q = 1;
-                    nint = 0;
-                    if (c == 0) {
-                        last = n - 1;
-                        p = i + 1;
-                        phase = 2;
-                        if (p <= last) gallop_start(g, k1, p, last, c + 1);
-                        searching = p <= last;
-                    } else {
-                        phase = 1;
-                        gallop_start(g, k1, i + 1, n - 1, c);
-                        searching = true;
-                    }
-                }
-            }
+    if (p <= last) atomicOr(&s->error, kErrTree);
+    int ref[4] = {INT_MIN, INT_MIN, INT_MIN, INT_MIN};
+    int nint = 0;
+    for (int q = 0; q < nc; ++q) {
+        const int a = cs[q], b = ce[q];
+        if (a == b) {
+            ref[q] = ~a;
+            t.leaf_last[a] = a;
+            t.leaf_plevel[a] = c;
+            continue;
         }
-        if (__all_sync(kFull, id == -2)) break;
-        // one probe of the current search
-        bool found = false;
-        if (searching) {
-            found = gallop_probe(g, key);
-            searching = !found;
+        const int c2 = lcp_digits(key[a], key[b]);
+        if (c2 >= kMaxLevel) {
+            ref[q] = ~a;
+            t.leaf_last[a] = b;
+            t.leaf_plevel[a] = c;
+            bucket_moments(pos, mass, a, b, t.bucket_mass + a, t.bucket_com + a);
+            continue;
         }
-        // advance the cell until it needs another probe or is done
-        if (id >= 0 && !searching) {
-            const int res = g.a;
-            bool have = found;
-            while (!searching && !finished) {
-                if (phase == 1) {  // the cell's end
-                    last = res;
-                    p = i + 1;
-                    phase = 2;
-                    if (p <= last) {
-                        gallop_start(g, key[p], p, last, c + 1);
-                        searching = true;
-                    }
-                    have = false;
-                    continue;
-                }
-                if (phase == 2) {  // a child's end
-                    if (have) {
-                        ++q;  // child q - 1 = [p, res]; the next one starts at res + 1
-                        if (q < 4) set4(first, cs1, cs2, cs3, q, res + 1);
-                        p = res + 1;
-                        have = false;
-                    }
-                    if (p <= last && q < 4) {
-                        gallop_start(g, key[p], p, last, c + 1);
-                        searching = true;
-                        continue;
-                    }
-                    if (p <= last) atomicOr(&s->error, kErrTree);
-                    rf0 = rf1 = rf2 = rf3 = INT_MIN;
-                    r = 0;
-                    phase = 3;
-                }
-                // phase 3: the children in order; an internal child's first
-                // split names its cell
-                if (have) {
-                    const int cid = t.cell_of[res];
-                    set4(rf0, rf1, rf2, rf3, r, cid);
-                    t.parent[cid] = id;
-                    ++nint;
-                    ++r;
-                    have = false;
-                }
-                while (r < q && !searching) {
-                    const int a = get4(first, cs1, cs2, cs3, r);
-                    const int b = r + 1 < q ? get4(first, cs1, cs2, cs3, r + 1) - 1 : last;
-                    if (a == b) {
-                        set4(rf0, rf1, rf2, rf3, r, ~a);
-                        t.leaf_last[a] = a;
-                        t.leaf_plevel[a] = c;
-                        ++r;
-                        continue;
-                    }
-                    const uint64_t ka = key[a];
-                    const int c2 = lcp_digits(ka, key[b]);
-                    if (c2 >= kMaxLevel) {
-                        set4(rf0, rf1, rf2, rf3, r, ~a);
-                        t.leaf_last[a] = b;
-                        t.leaf_plevel[a] = c;
-                        bucket_moments(pos, mass, a, b, t.bucket_mass + a, t.bucket_com + a);
-                        ++r;
-                        continue;
-                    }
-                    gallop_start(g, ka, a, b, c2 + 1);
-                    searching = true;
-                }
-                if (searching) break;
-                // every child resolved: write the cell
-                t.first[id] = first;
-                t.last[id] = last;
-                t.range[id] = make_int2(first, last);
-                t.level[id] = c;
-                t.child[id] = make_int4(rf0, rf1, rf2, rf3);
-                t.nint[id] = nint;
-                t.ready[id] = 0;
-                if (first == 0 && last == n - 1) {
-                    s->root = id;
-                    t.parent[id] = -1;
-                }
-                finished = true;
-            }
-        }
-        // cells whose children are all leaves start the bottom-up climb:
-        // listed with one atomic per warp, where the warp is converged
-        const bool start = finished && nint == 0;
-        const unsigned sm = __ballot_sync(kFull, start);
-        if (sm) {
-            int base = 0;
-            if (lane == __ffs(sm) - 1) base = atomicAdd(&s->nstart, __popc(sm));
-            base = __shfl_sync(kFull, base, __ffs(sm) - 1);
-            if (start) t.start_list[base + __popc(sm & below)] = id;
-        }
-        if (finished) {
-            finished = false;
-            id = -1;
-        }
+        const int rep = gallop_right(key, a, b, c2 + 1);
+        const int cid = t.cell_of[rep];
+        ref[q] = cid;
+        t.parent[cid] = id;
+        ++nint;
+    }
+    t.first[id] = first;
+    t.last[id] = last;
+    t.range[id] = make_int2(first, last);
+    t.level[id] = c;
+    t.child[id] = make_int4(ref[0], ref[1], ref[2], ref[3]);
+    t.nint[id] = nint;
+    t.ready[id] = 0;
+    // cells whose children are all leaves start the bottom-up climb: listed
+    // with one atomic per warp
+    const unsigned active = __activemask();
+    const unsigned starts = __ballot_sync(active, nint == 0);
+    if (nint == 0) {
+        const int leader = __ffs(starts) - 1;
+        const int lane = threadIdx.x & 31;
+        int base = 0;
+        if (lane == leader) base = atomicAdd(&s->nstart, __popc(starts));
+        base = __shfl_sync(starts, base, leader);
+        t.start_list[base + __popc(starts & ((1u << lane) - 1u))] = id;
+    }
+    if (first == 0 && last == n - 1) {
+        s->root = id;
+        t.parent[id] = -1;
     }
 }
 
@@ -1093,18 +949,8 @@ void launch_tree(nb_ctx* c, const BodyBuffers& b) {
     scan_apply<<<sblocks, kThreads, 0, c->stream>>>(c->tree.flag, n, c->scan.block_sums,
                                                      c->tree.cell_of, c->tree.rep_of);
     cudaMemsetAsync(&c->scal->nstart, 0, sizeof(int32_t), c->stream);
-    cudaMemsetAsync(&c->scal->link_ticket, 0, sizeof(unsigned), c->stream);
-    if (c->link_blocks == 0) {
-        int per_sm = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tree_link, kThreads, 0) !=
-                cudaSuccess ||
-            per_sm < 1)
-            per_sm = 3;
-        c->link_blocks = c->sm_count * per_sm;
-    }
-    // persistent lanes: no more blocks than there are bodies for
-    const int link_blocks = (int)std::min<int64_t>(c->link_blocks, blocks_for(n, kThreads));
-    tree_link<<<link_blocks, kThreads, 0, c->stream>>>(key, n, b.pos, b.mass, c->tree, c->scal);
+    tree_link<<<blocks_for(n, kThreads), kThreads, 0, c->stream>>>(key, n, b.pos, b.mass, c->tree,
+                                                                    c->scal);
     tree_trivial_root<<<1, 1, 0, c->stream>>>(b.pos, b.mass, n, c->tree, c->scal);
 }
 

@@ -44,7 +44,6 @@ struct DeviceScalars {
     int32_t stack_pad_;
     int32_t nstart;           // cells whose children are all leaves (climb starts)
     unsigned upload_bad;      // nb_upload's checks: bit 0 non-finite, bit 1 mass <= 0
-    unsigned link_ticket;     // next cell for the persistent tree_link lanes
     // Radix sort over the top sort_passes bytes of the keys only (1..8), chosen
     // per step from the previous tree's histogram of shared leading digits of
     // neighbouring codes; keys that agree in those bytes are then put in order
@@ -180,7 +179,6 @@ struct nb_ctx {
     double* bbox_partials = nullptr;     // [blocks][4]
     int bbox_blocks = 0;
     int split_blocks[16] = {};            // persistent grids of the SPLIT traversal variants
-    int link_blocks = 0;                 // persistent grid of tree_link (0 = not sized yet)
     int corr_blocks_per_sm = 0;          // learned correction kernel occupancy (0 = not set up)
     float* mlp_params = nullptr;         // learned mode: FP32 MLP parameters (device)
     void* mlp_infer = nullptr;           // learned mode: BF16 fragment images for inference
