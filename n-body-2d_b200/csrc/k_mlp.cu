@@ -12,12 +12,13 @@
 // cells (d ~ eps) have residuals that depend on it far more than on any
 // higher moment.
 //
-// Tensor-core layout: mma.sync m16n8k16 BF16 with FP32 accumulators for
-// training and for the step's correction.  A 16-row tile (16 samples, or 16
-// cells of one target group) runs through the three layers in registers; the
-// accumulator fragment of one layer is, element for element, the A fragment of
-// the next, so no shuffles are needed.  Bulk evaluation (nb_mlp_forward) runs
-// on tcgen05 in 128-row tiles (mlp_forward_tc, further down).
+// Tensor-core layout: training (nb_mlp_train, nb_mlp_loss_grad) and bulk
+// evaluation (nb_mlp_forward) run on tcgen05 in 128-row tiles with BF16
+// operands in shared memory and FP32 accumulators in TMEM (mlp_grad_tc,
+// mlp_forward_tc, further down).  The step's correction uses mma.sync
+// m16n8k16: a 16-row tile (16 cells of one target group) runs through the
+// three layers in registers, the accumulator fragment of one layer being,
+// element for element, the A fragment of the next.
 //
 // Inference is per target group: the traversal lists each group's band cells;
 // mlp_correct_kick evaluates the MLP at the group's centre for all of them in
@@ -54,17 +55,6 @@ constexpr int kYS = kB3 + 2;              // output scale
 constexpr int kParams = kYS + 1;
 static_assert(kParams == NB_MLP_PARAMS, "weight layout and header disagree");
 
-// BF16 images of the weights in the layouts the fragments read.
-struct MlpWeights {
-    __nv_bfloat16 w1[kH][16];    // B of layer 1: [n = hidden][k = input, padded]
-    __nv_bfloat16 w2[kH][kH];    // B of layer 2: [n = out][k = in]
-    __nv_bfloat16 w3[8][kH];     // B of layer 3: [n = out, padded][k = hidden]
-    __nv_bfloat16 w2t[kH][kH];   // backward: [n = in][k = out]
-    __nv_bfloat16 w3t[kH][16];   // backward: [n = hidden][k = out, padded]
-    float b1[kH], b2[kH], b3[8];
-    float yscale;
-};
-
 __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
     const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
     return *reinterpret_cast<const uint32_t*>(&v);
@@ -78,16 +68,6 @@ __device__ __forceinline__ void mma16816(float c[4], const uint32_t a[4], uint32
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
-// B fragment of an [n][k] row-major BF16 matrix (leading dimension ld), for
-// the 8 columns starting at nb and the 16 k starting at kb.
-__device__ __forceinline__ void load_b(const __nv_bfloat16* m, int ld, int nb, int kb, uint32_t& b0,
-                                       uint32_t& b1) {
-    const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
-    const __nv_bfloat16* row = m + (nb + g) * ld + kb + 2 * q;
-    b0 = *reinterpret_cast<const uint32_t*>(row);
-    b1 = *reinterpret_cast<const uint32_t*>(row + 8);
-}
-
 // A fragment of a 16 x 16 tile of a row-major BF16 matrix.
 __device__ __forceinline__ void load_a(const __nv_bfloat16* m, int ld, int kb, uint32_t a[4]) {
     const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
@@ -96,22 +76,6 @@ __device__ __forceinline__ void load_a(const __nv_bfloat16* m, int ld, int kb, u
     a[2] = *reinterpret_cast<const uint32_t*>(m + g * ld + kb + 2 * q + 8);
     a[3] = *reinterpret_cast<const uint32_t*>(m + (g + 8) * ld + kb + 2 * q + 8);
 }
-
-// Accumulators of n-tiles 2kt and 2kt+1 -> A fragment of k-tile kt.
-__device__ __forceinline__ void c_to_a(const float c0[4], const float c1[4], uint32_t a[4]) {
-    a[0] = pack_bf16(c0[0], c0[1]);
-    a[1] = pack_bf16(c0[2], c0[3]);
-    a[2] = pack_bf16(c1[0], c1[1]);
-    a[3] = pack_bf16(c1[2], c1[3]);
-}
-
-// Activations kept for the backward pass (the BF16-rounded values the next
-// layer consumed).
-struct Fwd {
-    float h1[8][4];
-    float h2[8][4];
-    float y[4];   // n-tile 0 of the output: columns 2q, 2q+1 of rows g, g+8
-};
 
 __device__ __forceinline__ float bf16_round(float v) {
     return __bfloat162float(__float2bfloat16_rn(v));
@@ -125,275 +89,7 @@ __device__ __forceinline__ float tanh_fast(float x) {
     return y;
 }
 
-// Forward pass of one 16-row tile whose inputs are the A fragment `x`.
-// kKeep stores the BF16-rounded activations the backward pass needs; without
-// it the rounding happens once, in the conversion to the next A fragment.
-template <bool kKeep = true>
-__device__ __forceinline__ void mlp_forward(const MlpWeights& W, const uint32_t x[4], Fwd& f) {
-    const int q = threadIdx.x & 3;
-#pragma unroll
-    for (int nt = 0; nt < 8; ++nt) {
-        const float bl = W.b1[8 * nt + 2 * q], bh = W.b1[8 * nt + 2 * q + 1];
-        float c[4] = {bl, bh, bl, bh};
-        uint32_t b0, b1;
-        load_b(&W.w1[0][0], 16, 8 * nt, 0, b0, b1);
-        mma16816(c, x, b0, b1);
-#pragma unroll
-        for (int e = 0; e < 4; ++e) f.h1[nt][e] = kKeep ? bf16_round(tanh_fast(c[e])) : tanh_fast(c[e]);
-    }
-    uint32_t a1[4][4];
-#pragma unroll
-    for (int kt = 0; kt < 4; ++kt) c_to_a(f.h1[2 * kt], f.h1[2 * kt + 1], a1[kt]);
-#pragma unroll
-    for (int nt = 0; nt < 8; ++nt) {
-        const float bl = W.b2[8 * nt + 2 * q], bh = W.b2[8 * nt + 2 * q + 1];
-        float c[4] = {bl, bh, bl, bh};
-#pragma unroll
-        for (int kt = 0; kt < 4; ++kt) {
-            uint32_t b0, b1;
-            load_b(&W.w2[0][0], kH, 8 * nt, 16 * kt, b0, b1);
-            mma16816(c, a1[kt], b0, b1);
-        }
-#pragma unroll
-        for (int e = 0; e < 4; ++e) f.h2[nt][e] = kKeep ? bf16_round(tanh_fast(c[e])) : tanh_fast(c[e]);
-    }
-    uint32_t a2[4][4];
-#pragma unroll
-    for (int kt = 0; kt < 4; ++kt) c_to_a(f.h2[2 * kt], f.h2[2 * kt + 1], a2[kt]);
-    {
-        const float bl = W.b3[2 * q], bh = W.b3[2 * q + 1];
-        float c[4] = {bl, bh, bl, bh};
-#pragma unroll
-        for (int kt = 0; kt < 4; ++kt) {
-            uint32_t b0, b1;
-            load_b(&W.w3[0][0], kH, 0, 16 * kt, b0, b1);
-            mma16816(c, a2[kt], b0, b1);
-        }
-#pragma unroll
-        for (int e = 0; e < 4; ++e) f.y[e] = c[e];
-    }
-}
-
-// FP32 master parameters -> BF16 fragment images (one block).
-__device__ void fill_weights(const float* __restrict__ p, MlpWeights& W) {
-    for (int k = threadIdx.x; k < kH * 16; k += blockDim.x) {
-        const int o = k / 16, i = k % 16;
-        W.w1[o][i] = __float2bfloat16_rn(i < kNin ? p[kW1 + o * kNin + i] : 0.f);
-        W.w3t[o][i] = __float2bfloat16_rn(i < 2 ? p[kW3 + i * kH + o] : 0.f);
-    }
-    for (int k = threadIdx.x; k < kH * kH; k += blockDim.x) {
-        const int o = k / kH, i = k % kH;
-        W.w2[o][i] = __float2bfloat16_rn(p[kW2 + k]);
-        W.w2t[i][o] = __float2bfloat16_rn(p[kW2 + k]);
-    }
-    for (int k = threadIdx.x; k < 8 * kH; k += blockDim.x) {
-        const int o = k / kH, i = k % kH;
-        W.w3[o][i] = __float2bfloat16_rn(o < 2 ? p[kW3 + o * kH + i] : 0.f);
-    }
-    for (int k = threadIdx.x; k < kH; k += blockDim.x) {
-        W.b1[k] = p[kB1 + k];
-        W.b2[k] = p[kB2 + k];
-    }
-    if (threadIdx.x < 8) W.b3[threadIdx.x] = threadIdx.x < 2 ? p[kB3 + threadIdx.x] : 0.f;
-    if (threadIdx.x == 0) W.yscale = p[kYS];
-}
-
 constexpr int kWarps = 4;
-
-// ---- training: loss and gradients of a batch ---------------------------
-// Loss = mean over the batch of |y - t|^2 (t already divided by yscale).
-// Each warp takes 16-sample tiles; the backward GEMMs run on the tensor cores:
-//   dh2 = dy W3, dh1 = dp2 W2 (A from the accumulators, B = transposed
-//   weights), and the weight gradients dW = dp^T h with the batch as the K
-//   dimension (A and B staged transposed in shared memory).  Gradients sum in
-//   per-block shared memory and then in the global FP32 gradient vector.
-struct TrainSmem {
-    MlpWeights W;
-    float g[kParams];                // block-local gradient sums
-    __nv_bfloat16 xt[kWarps][16][16];    // inputs  [s][k]
-    __nv_bfloat16 p2t[kWarps][kH][16];   // dp2^T   [o][s]
-    __nv_bfloat16 p1t[kWarps][kH][16];   // dp1^T   [o][s]
-    __nv_bfloat16 h1t[kWarps][kH][16];   // h1^T    [i][s]
-    __nv_bfloat16 h2t[kWarps][kH][16];   // h2^T    [i][s]
-    __nv_bfloat16 dyt[kWarps][16][16];   // dy^T    [o][s] (rows >= 2 zero)
-    __nv_bfloat16 xtt[kWarps][16][16];   // x^T     [k][s]
-    float loss;
-};
-
-__device__ __forceinline__ void atomic_tile(float* dst, int ld, int mb, int nb, const float c[4]) {
-    const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
-    atomicAdd(dst + (mb + g) * ld + nb + 2 * q, c[0]);
-    atomicAdd(dst + (mb + g) * ld + nb + 2 * q + 1, c[1]);
-    atomicAdd(dst + (mb + g + 8) * ld + nb + 2 * q, c[2]);
-    atomicAdd(dst + (mb + g + 8) * ld + nb + 2 * q + 1, c[3]);
-}
-
-__global__ void __launch_bounds__(kWarps * 32)
-mlp_grad_kernel(const float* __restrict__ params, const float* __restrict__ X,
-                const float* __restrict__ Yt, const int64_t* __restrict__ idx, int64_t n,
-                float inv_n, float* __restrict__ grad, float* __restrict__ loss) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    TrainSmem& S = *reinterpret_cast<TrainSmem*>(smem_raw);
-    fill_weights(params, S.W);
-    for (int k = threadIdx.x; k < kParams; k += blockDim.x) S.g[k] = 0.f;
-    if (threadIdx.x == 0) S.loss = 0.f;
-    __syncthreads();
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, q = lane & 3;
-    const int64_t ntiles = (n + 15) / 16;
-    for (int64_t tile = blockIdx.x * (int64_t)kWarps + warp; tile < ntiles;
-         tile += (int64_t)gridDim.x * kWarps) {
-        // stage the inputs (row-major for the forward, transposed for dW1)
-        for (int e = lane; e < 256; e += 32) {
-            const int r = e >> 4, k = e & 15;
-            const int64_t s = tile * 16 + r;
-            const int64_t src = s < n ? (idx ? idx[s] : s) : -1;
-            const __nv_bfloat16 v = __float2bfloat16_rn(src >= 0 && k < kNin ? X[src * kNin + k] : 0.f);
-            S.xt[warp][r][k] = v;
-            S.xtt[warp][k][r] = v;
-        }
-        __syncwarp();
-        uint32_t a[4];
-        load_a(&S.xt[warp][0][0], 16, 0, a);
-        Fwd f;
-        mlp_forward(S.W, a, f);
-        // dy = 2 (y - t) / n on valid rows and the two output columns
-        float dy[4];
-        float l = 0.f;
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-            const int row = g + (e >= 2 ? 8 : 0), col = 2 * q + (e & 1);
-            const int64_t s = tile * 16 + row;
-            float d = 0.f;
-            if (s < n && col < 2) {
-                const int64_t src = idx ? idx[s] : s;
-                d = f.y[e] - Yt[2 * src + col];
-                l += d * d;
-            }
-            dy[e] = 2.f * d * inv_n;
-        }
-        for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(kFull, l, o);
-        if (lane == 0) atomicAdd(&S.loss, l * inv_n);
-        // dh2 = dy W3 -> dp2 = dh2 (1 - h2^2)
-        uint32_t ady[4] = {pack_bf16(dy[0], dy[1]), pack_bf16(dy[2], dy[3]), 0u, 0u};
-        float dp2[8][4];
-#pragma unroll
-        for (int nt = 0; nt < 8; ++nt) {
-            float c[4] = {0.f, 0.f, 0.f, 0.f};
-            uint32_t b0, b1;
-            load_b(&S.W.w3t[0][0], 16, 8 * nt, 0, b0, b1);
-            mma16816(c, ady, b0, b1);
-#pragma unroll
-            for (int e = 0; e < 4; ++e) dp2[nt][e] = c[e] * (1.f - f.h2[nt][e] * f.h2[nt][e]);
-        }
-        // dh1 = dp2 W2 -> dp1 = dh1 (1 - h1^2)
-        uint32_t ap2[4][4];
-#pragma unroll
-        for (int kt = 0; kt < 4; ++kt) c_to_a(dp2[2 * kt], dp2[2 * kt + 1], ap2[kt]);
-        float dp1[8][4];
-#pragma unroll
-        for (int nt = 0; nt < 8; ++nt) {
-            float c[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll
-            for (int kt = 0; kt < 4; ++kt) {
-                uint32_t b0, b1;
-                load_b(&S.W.w2t[0][0], kH, 8 * nt, 16 * kt, b0, b1);
-                mma16816(c, ap2[kt], b0, b1);
-            }
-#pragma unroll
-            for (int e = 0; e < 4; ++e) dp1[nt][e] = c[e] * (1.f - f.h1[nt][e] * f.h1[nt][e]);
-        }
-        // stage the transposes: element (row s, col o) -> [o][s]
-#pragma unroll
-        for (int nt = 0; nt < 8; ++nt)
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                const int s = g + (e >= 2 ? 8 : 0), o = 8 * nt + 2 * q + (e & 1);
-                S.p2t[warp][o][s] = __float2bfloat16_rn(dp2[nt][e]);
-                S.p1t[warp][o][s] = __float2bfloat16_rn(dp1[nt][e]);
-                S.h1t[warp][o][s] = __float2bfloat16_rn(f.h1[nt][e]);
-                S.h2t[warp][o][s] = __float2bfloat16_rn(f.h2[nt][e]);
-            }
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-            const int s = g + (e >= 2 ? 8 : 0), o = 2 * q + (e & 1);
-            S.dyt[warp][o][s] = __float2bfloat16_rn(o < 2 ? dy[e] : 0.f);
-            S.dyt[warp][o + 8][s] = __float2bfloat16(0.f);
-        }
-        __syncwarp();
-        // bias gradients: column sums
-#pragma unroll
-        for (int nt = 0; nt < 8; ++nt)
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                const int o = 8 * nt + 2 * q + (e & 1);
-                atomicAdd(&S.g[kB2 + o], dp2[nt][e]);
-                atomicAdd(&S.g[kB1 + o], dp1[nt][e]);
-            }
-#pragma unroll
-        for (int e = 0; e < 4; ++e)
-            if (2 * q + (e & 1) < 2) atomicAdd(&S.g[kB3 + 2 * q + (e & 1)], dy[e]);
-        // dW2[o][i] = sum_s dp2[s][o] h1[s][i]: A = dp2^T (m = o), B = h1 (k = s)
-#pragma unroll
-        for (int mt = 0; mt < 4; ++mt) {
-            uint32_t am[4];
-            load_a(&S.p2t[warp][16 * mt][0], 16, 0, am);
-#pragma unroll
-            for (int nt = 0; nt < 8; ++nt) {
-                float c[4] = {0.f, 0.f, 0.f, 0.f};
-                uint32_t b0, b1;
-                load_b(&S.h1t[warp][0][0], 16, 8 * nt, 0, b0, b1);
-                mma16816(c, am, b0, b1);
-                atomic_tile(S.g + kW2, kH, 16 * mt, 8 * nt, c);
-            }
-        }
-        // dW1[o][k] = sum_s dp1[s][o] x[s][k]
-#pragma unroll
-        for (int mt = 0; mt < 4; ++mt) {
-            uint32_t am[4];
-            load_a(&S.p1t[warp][16 * mt][0], 16, 0, am);
-#pragma unroll
-            for (int nt = 0; nt < 2; ++nt) {
-                float c[4] = {0.f, 0.f, 0.f, 0.f};
-                uint32_t b0, b1;
-                load_b(&S.xtt[warp][0][0], 16, 8 * nt, 0, b0, b1);
-                mma16816(c, am, b0, b1);
-                // columns >= 12 are padding
-                const int o0 = 16 * mt + g, k0 = 8 * nt + 2 * q;
-                if (k0 < kNin) {
-                    atomicAdd(&S.g[kW1 + o0 * kNin + k0], c[0]);
-                    atomicAdd(&S.g[kW1 + (o0 + 8) * kNin + k0], c[2]);
-                }
-                if (k0 + 1 < kNin) {
-                    atomicAdd(&S.g[kW1 + o0 * kNin + k0 + 1], c[1]);
-                    atomicAdd(&S.g[kW1 + (o0 + 8) * kNin + k0 + 1], c[3]);
-                }
-            }
-        }
-        // dW3[o][i] = sum_s dy[s][o] h2[s][i] (rows o >= 2 are padding)
-        {
-            uint32_t am[4];
-            load_a(&S.dyt[warp][0][0], 16, 0, am);
-#pragma unroll
-            for (int nt = 0; nt < 8; ++nt) {
-                float c[4] = {0.f, 0.f, 0.f, 0.f};
-                uint32_t b0, b1;
-                load_b(&S.h2t[warp][0][0], 16, 8 * nt, 0, b0, b1);
-                mma16816(c, am, b0, b1);
-                if (g < 2) {
-                    atomicAdd(&S.g[kW3 + g * kH + 8 * nt + 2 * q], c[0]);
-                    atomicAdd(&S.g[kW3 + g * kH + 8 * nt + 2 * q + 1], c[1]);
-                }
-            }
-        }
-        __syncwarp();
-    }
-    __syncthreads();
-    for (int k = threadIdx.x; k < kYS; k += blockDim.x) {
-        const float v = S.g[k];
-        if (v != 0.f) atomicAdd(grad + k, v);
-    }
-    if (threadIdx.x == 0) atomicAdd(loss, S.loss);
-}
 
 // Adam on the FP32 master parameters (the output scale is not trained).
 __global__ void mlp_adam_kernel(float* __restrict__ p, const float* __restrict__ g,
@@ -410,8 +106,6 @@ __global__ void mlp_adam_kernel(float* __restrict__ p, const float* __restrict__
 }
 
 }  // namespace
-
-int mlp_smem_bytes() { return (int)sizeof(TrainSmem); }
 
 namespace {
 
@@ -1518,17 +1212,6 @@ int mlp_forward_device(const float* params, const float* X, int64_t n, float* Y,
     const int64_t tiles = (n + kTcRows - 1) / kTcRows;
     const int grid = (int)std::min<int64_t>(tiles, (int64_t)sm_count * kTcBlocksPerSm);
     mlp_forward_tc<<<grid, kTcWarps * 32, smem, st>>>(W, X, n, Y, err);
-    return cudaGetLastError() == cudaSuccess ? NB_OK : NB_ERR_CUDA;
-}
-
-int mlp_grad_device(const float* params, const float* X, const float* Yt, const int64_t* idx,
-                    int64_t n, float* grad, float* loss, int blocks, cudaStream_t st) {
-    const int smem = (int)sizeof(TrainSmem);
-    // set on every call: the attribute belongs to the current device, and the
-    // library keeps no process-wide state
-    cudaFuncSetAttribute(mlp_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    mlp_grad_kernel<<<blocks, kWarps * 32, smem, st>>>(params, X, Yt, idx, n, 1.f / (float)n, grad,
-                                                       loss);
     return cudaGetLastError() == cudaSuccess ? NB_OK : NB_ERR_CUDA;
 }
 

@@ -272,8 +272,6 @@ void launch_mlp_samples(nb_ctx* c, const BodyBuffers& b, const int* slots, int n
 size_t mlp_forward_image_bytes();
 int mlp_forward_device(const float* params, const float* X, int64_t n, float* Y, void* image,
                        unsigned* err, int sm_count, cudaStream_t st);
-int mlp_grad_device(const float* params, const float* X, const float* Yt, const int64_t* idx,
-                    int64_t n, float* grad, float* loss, int blocks, cudaStream_t st);
 int mlp_adam_device(float* p, const float* g, float* m, float* v, float lr, int step,
                     cudaStream_t st);
 // training loss and gradients on tcgen05 (image = mlp_train_image_bytes() of

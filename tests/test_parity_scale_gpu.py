@@ -73,6 +73,8 @@ def test_parity_plummer_16m(nbp, orc):
 
 
 def _check_groups(groups, n, gsize, universe_off=None):
+    # groups are stored cell by cell; in body order they must tile [0, n)
+    groups = groups[np.argsort(groups[:, 0], kind="stable")]
     first, last = groups[:, 0], groups[:, 1]
     assert first[0] == 0 and last[-1] == n - 1
     assert np.all(last >= first)
