@@ -86,15 +86,11 @@ __device__ int gallop_right(const uint64_t* __restrict__ key, int i, int hi, int
 
 // Pass 1: flag the boundaries that create a cell.  It also counts, for the
 // next step's sort, how many neighbouring codes share d leading digits
-// (choose_sort_passes reads the histogram), and the cells of each level
-// (tree_link's work order).
+// (choose_sort_passes reads the histogram).
 __global__ void tree_mark(const uint64_t* __restrict__ key, int n, int32_t* __restrict__ flag,
-                          int32_t* __restrict__ start_of, unsigned* __restrict__ lcp_hist,
-                          unsigned* __restrict__ lvl_count) {
+                          int32_t* __restrict__ start_of, unsigned* __restrict__ lcp_hist) {
     __shared__ unsigned hist[33];
-    __shared__ unsigned lhist[32];
     if (threadIdx.x < 33) hist[threadIdx.x] = 0;
-    if (threadIdx.x < 32) lhist[threadIdx.x] = 0;
     __syncthreads();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) {
@@ -107,7 +103,6 @@ __global__ void tree_mark(const uint64_t* __restrict__ key, int n, int32_t* __re
                 s = c == 0 ? 0 : gallop_left(key, 0, i, c);
                 // i opens the cell iff bodies s..i all sit in its first child.
                 f = share(key[s], ki, c + 1) ? 1 : 0;
-                if (f) atomicAdd(&lhist[c], 1u);
             }
         }
         flag[i] = f;
@@ -115,41 +110,6 @@ __global__ void tree_mark(const uint64_t* __restrict__ key, int n, int32_t* __re
     }
     __syncthreads();
     if (threadIdx.x < 33 && hist[threadIdx.x]) atomicAdd(lcp_hist + threadIdx.x, hist[threadIdx.x]);
-    if (threadIdx.x < 32 && lhist[threadIdx.x]) atomicAdd(lvl_count + threadIdx.x, lhist[threadIdx.x]);
-}
-
-// Cell ids grouped by level, shallow levels first.  A cell's linking cost is
-// its galloping searches, whose lengths follow its size, and cells of one
-// level have similar sizes, so warps of tree_link that take consecutive
-// entries of this order finish their lanes at about the same time (in cell-id
-// order a warp waited for its one large cell).
-__global__ void __launch_bounds__(kThreads)
-cells_by_level(const uint64_t* __restrict__ key, Tree t, DeviceScalars* __restrict__ s) {
-    __shared__ unsigned base[32];
-    if (threadIdx.x < 32) {
-        const unsigned v = s->lvl_count[threadIdx.x];
-        unsigned inc = v;
-        for (int o = 1; o < 32; o <<= 1) {
-            const unsigned u = __shfl_up_sync(kFull, inc, o);
-            if ((int)threadIdx.x >= o) inc += u;
-        }
-        base[threadIdx.x] = inc - v;
-    }
-    __syncthreads();
-    const int id = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool on = id < s->cells;
-    int c = 32 + (threadIdx.x & 31);  // unique per lane when off
-    if (on) {
-        const int i = t.rep_of[id];
-        c = lcp_digits(key[i], key[i + 1]);
-    }
-    const unsigned peers = __match_any_sync(kFull, c);
-    const int leader = __ffs(peers) - 1;
-    const int lane = threadIdx.x & 31;
-    unsigned slot = 0;
-    if (on && lane == leader) slot = atomicAdd(&s->lvl_fill[c], (unsigned)__popc(peers));
-    slot = __shfl_sync(kFull, slot, leader) + __popc(peers & ((1u << lane) - 1u));
-    if (on) t.link_order[base[c] + slot] = id;
 }
 
 // ---- exclusive scan of flag[] -> cell_of[], total -> scal->cells ----------
@@ -286,11 +246,9 @@ __device__ void bucket_moments(const double2* __restrict__ pos, const double* __
 __global__ void tree_link(const uint64_t* __restrict__ key, int n,
                           const double2* __restrict__ pos, const double* __restrict__ mass,
                           Tree t, DeviceScalars* __restrict__ s) {
-    // one thread per cell, taken in level order, so every lane of a warp
-    // builds a cell of about the same size
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= s->cells) return;
-    const int id = t.link_order[k];
+    // one thread per cell, so every lane of a warp builds a cell
+    const int id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= s->cells) return;
     const int i = t.rep_of[id];
     const int c = lcp_digits(key[i], key[i + 1]);
     const int first = t.start_of[i];
@@ -981,19 +939,16 @@ void launch_groups(nb_ctx* c) {
 void launch_tree(nb_ctx* c, const BodyBuffers& b) {
     const int n = (int)c->n;
     const uint64_t* key = c->sort.key[0];
-    c->launches += 7;
-    cudaMemsetAsync(c->scal->lvl_count, 0, 2 * 32 * sizeof(unsigned), c->stream);
+    c->launches += 6;
     tree_mark<<<blocks_for(n, kThreads), kThreads, 0, c->stream>>>(key, n, c->tree.flag,
                                                                     c->tree.start_of,
-                                                                    c->scal->lcp_hist,
-                                                                    c->scal->lvl_count);
+                                                                    c->scal->lcp_hist);
     const int sblocks = (int)blocks_for(n, kScanTile);
     scan_reduce<<<sblocks, kThreads, 0, c->stream>>>(c->tree.flag, n, c->scan.block_sums);
     scan_block_sums<<<1, kThreads, 0, c->stream>>>(c->scan.block_sums, sblocks, &c->scal->cells);
     scan_apply<<<sblocks, kThreads, 0, c->stream>>>(c->tree.flag, n, c->scan.block_sums,
                                                      c->tree.cell_of, c->tree.rep_of);
     cudaMemsetAsync(&c->scal->nstart, 0, sizeof(int32_t), c->stream);
-    cells_by_level<<<blocks_for(n, kThreads), kThreads, 0, c->stream>>>(key, c->tree, c->scal);
     tree_link<<<blocks_for(n, kThreads), kThreads, 0, c->stream>>>(key, n, b.pos, b.mass, c->tree,
                                                                     c->scal);
     tree_trivial_root<<<1, 1, 0, c->stream>>>(b.pos, b.mass, n, c->tree, c->scal);

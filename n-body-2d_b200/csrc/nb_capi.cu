@@ -118,7 +118,6 @@ int alloc_all(nb_ctx* c) {
     NB_CUDA(c, dalloc(&t.flag, n));
     NB_CUDA(c, dalloc(&t.cell_of, n));
     NB_CUDA(c, dalloc(&t.rep_of, n));
-    NB_CUDA(c, dalloc(&t.link_order, n));
     NB_CUDA(c, dalloc(&t.start_of, n));
     NB_CUDA(c, dalloc(&c->scal, 1));
     NB_CUDA(c, cudaMemset(c->scal, 0, sizeof(nb::DeviceScalars)));
@@ -152,7 +151,7 @@ void free_all(nb_ctx* c) {
                          t.nint,      t.ready,       t.mass,        t.com,        t.leaf_last,
                          t.leaf_plevel, t.bucket_mass, t.bucket_com, t.flag,      t.cell_of,
                          t.start_of,  t.range,       t.s64,         t.cell4,      t.cellq,
-                         t.body4,     t.gcount,      t.gbase,       t.groups,     t.rep_of,     t.link_order,
+                         t.body4,     t.gcount,      t.gbase,       t.groups,     t.rep_of,
                          t.t32,       t.cellh,       t.band,        t.band_count,
                          t.start_list, t.prefix, t.prefix_tiles};
     for (void* q : tree_ptrs) cudaFree(q);

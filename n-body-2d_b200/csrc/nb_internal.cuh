@@ -53,8 +53,6 @@ struct DeviceScalars {
     int32_t sort_passes_forced;
     unsigned lcp_hist[33];    // neighbouring codes sharing d leading 2-bit digits (d = 32: equal)
     unsigned tie_count[2];    // tie groups of <= 32 keys / of more keys, this step
-    unsigned lvl_count[32];   // cells of the tree being built, per level
-    unsigned lvl_fill[32];    // cells placed in link_order so far, per level
 };
 
 // Batched universes (nb_batch_create): bodies of universe u occupy the fixed
@@ -134,7 +132,6 @@ struct Tree {
     int32_t* flag = nullptr;
     int32_t* cell_of = nullptr;     // exclusive scan of flag
     int32_t* rep_of = nullptr;      // cell id -> the boundary that creates it
-    int32_t* link_order = nullptr;  // cell ids by level: tree_link's work order
     int32_t* start_of = nullptr;    // first body of the cell owning boundary i
 };
 
