@@ -220,10 +220,10 @@ mlp_samples_kernel(Tree t, const DeviceScalars* __restrict__ s, const double2* _
             const double2 c = t.com[ref];
             double sxx = 0.0, sxy = 0.0, syy = 0.0;
             if (quad) {
-                const float4 q = t.cellq[ref];
-                sxx = q.x;
-                sxy = q.y;
-                syy = q.z;
+                const float4 q = t.cellq[ref];  // 7.5 S
+                sxx = q.x / 7.5;
+                sxy = q.y / 7.5;
+                syy = q.z / 7.5;
             }
             double rx = 0.0, ry = 0.0;
 #pragma unroll

@@ -461,7 +461,8 @@ __device__ __forceinline__ void cell_moments(int id, const DeviceScalars* __rest
         const double2 fc = frame_center(s, bt, first);
         t.cell4[id] = make_float4((float)(com.x - fc.x), (float)(com.y - fc.y), (float)M,
                                   accept_size2(s, bt, pos, first, t.level[id], com, accept_scale));
-        t.cellq[id] = make_float4((float)sxx, (float)sxy, (float)syy, 0.f);
+        // the walk's record carries 7.5 S, the factor of its (d.S.d) r^-7 term
+        t.cellq[id] = make_float4((float)(7.5 * sxx), (float)(7.5 * sxy), (float)(7.5 * syy), 0.f);
     }
 }
 
@@ -719,7 +720,7 @@ __device__ void write_features(const Tree& t, const DeviceScalars* __restrict__ 
     const int first = t.range[id].x;
     const double w2 = cell_width2(s, bt, first, t.level[id]), w = sqrt(w2);
     const float im2 = (float)(1.0 / (M * w2)), im3 = (float)(1.0 / (M * w2 * w));
-    __stcg(t.cellq + id, make_float4(S[0], S[1], S[2], 0.f));
+    __stcg(t.s32 + id, make_float4(S[0], S[1], S[2], 0.f));
     __stcg(t.t32 + id, make_float4(T[0], T[1], T[2], T[3]));
     const float4 c4 = t.cell4[id];
     t.cellh[2 * id] = make_uint4(bf16_pair((float)(mmax / M), S[0] * im2),
@@ -785,7 +786,7 @@ learned_features(DeviceScalars* __restrict__ s, const double2* __restrict__ pos,
             float4 cs = zero, ct = zero;
             if (r >= 0) {
                 cc = t.com[r];
-                cs = __ldcg(t.cellq + r);
+                cs = __ldcg(t.s32 + r);
                 ct = __ldcg(t.t32 + r);
             } else {
                 const int b = ~r;

@@ -95,6 +95,7 @@ int alloc_all(nb_ctx* c) {
         NB_CUDA(c, dalloc(&t.s64, n));
         NB_CUDA(c, dalloc(&t.cell4, n));
         NB_CUDA(c, dalloc(&t.cellq, n));
+        NB_CUDA(c, dalloc(&t.s32, n));
         NB_CUDA(c, dalloc(&t.body4, n));
         NB_CUDA(c, dalloc(&t.gcount, n));
         NB_CUDA(c, dalloc(&t.gbase, n));
@@ -150,7 +151,7 @@ void free_all(nb_ctx* c) {
     void* tree_ptrs[] = {t.first,     t.last,        t.level,       t.child,      t.parent,
                          t.nint,      t.ready,       t.mass,        t.com,        t.leaf_last,
                          t.leaf_plevel, t.bucket_mass, t.bucket_com, t.flag,      t.cell_of,
-                         t.start_of,  t.range,       t.s64,         t.cell4,      t.cellq,
+                         t.start_of,  t.range,       t.s64,         t.cell4,      t.cellq,      t.s32,
                          t.body4,     t.gcount,      t.gbase,       t.groups,     t.rep_of,
                          t.t32,       t.cellh,       t.band,        t.band_count,
                          t.start_list, t.prefix, t.prefix_tiles};

@@ -100,12 +100,14 @@ struct Tree {
     // the packed FP32 records the traversal reads
     double4* s64 = nullptr;      // {Sxx, Sxy, Syy, 0}
     float4* cell4 = nullptr;     // {com_x - cx, com_y - cy, mass, width^2}
-    float4* cellq = nullptr;     // {Sxx, Sxy, Syy, 0}
+    float4* cellq = nullptr;     // the walk's quadrupole record {7.5 Sxx, 7.5 Sxy, 7.5 Syy, 0}
     float4* body4 = nullptr;     // per body {x - cx, y - cy, mass, index bits}
     // learned correction: third moments (FP64, bottom-up) and the per-cell
     // MLP features (see k_mlp.cu): the eight moment features as BF16 and the
     // cell width
     float4* t32 = nullptr;       // {Txxx, Txxy, Txyy, Tyyy} (FP32: they only feed BF16 features)
+    float4* s32 = nullptr;       // {Sxx, Sxy, Syy, 0} of the feature pass (FP32, its own copy:
+                                 // it runs beside the walk, which reads cellq)
     // two uint4 per cell (one 32-byte sector for the correction's gathers):
     // BF16 pairs {f3 f4, f5 f6, f7 f8, f9 f10}, then the float bits of
     // {com_x - cx, com_y - cy, mass, width}
