@@ -87,6 +87,9 @@ typedef struct nb_params {
     double band_theta;      /* learned mode: the opening angle of the plain walk the
                                correction stands in for; cells accepted at theta that
                                this angle would open get the network's term (0 = 0.5) */
+    int32_t bodies_per_lane;/* SPLIT: target group size 32 x this, 1, 2 or 4 (0 = 2; learned
+                               contexts always use 2); nb_autotune may change it */
+    int32_t reserved;       /* must be 0 */
 } nb_params;
 
 typedef struct nb_stats {
@@ -163,8 +166,8 @@ NB_API int nb_batch_create(const nb_params* p, uint32_t nuniverses, const uint64
                            const double* mass, const double* pos_xy, const double* vel_xy,
                            nb_ctx** out);
 
-/* Picks the SPLIT traversal's bodies per lane (1 or 2: target groups of 32
- * or 64) and leaf size (4, 8, 16, 32) by timing `steps` steps of each on a
+/* Picks the SPLIT traversal's bodies per lane (1, 2 or 4: target groups of
+ * 32, 64 or 128) and leaf size (4, 8, 16, 32) by timing `steps` steps of each on a
  * copy of the bodies, which are restored afterwards; the choice stays set.
  * Either output pointer may be NULL. */
 NB_API int nb_autotune(nb_ctx* ctx, uint32_t steps, int32_t* leaf_out, int32_t* bpl_out);

@@ -68,6 +68,8 @@ class NbParams(C.Structure):
         ("flags", C.c_int32),
         ("bmax_ratio", C.c_double),
         ("band_theta", C.c_double),
+        ("bodies_per_lane", C.c_int32),
+        ("reserved", C.c_int32),
     ]
 
 

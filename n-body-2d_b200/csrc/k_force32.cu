@@ -472,6 +472,7 @@ force_split(double2* __restrict__ pos, double2* __restrict__ vel, double2* __res
 template <bool kQuad, int kBPL, bool kLearned, bool kZeroSoft>
 void launch_split_soft(nb_ctx* c, const BodyBuffers& b, bool kick, bool store_acc, float eps2) {
     int& grid = c->split_blocks[(kQuad ? 1 : 0) + (kLearned ? 2 : 0) + (kBPL == 1 ? 4 : 0) +
+                                (kBPL == 4 ? 16 : 0) +
                                 (kZeroSoft ? 8 : 0)];
     if (grid == 0) {
         int blocks = 0;
@@ -503,7 +504,11 @@ void launch_split_kernel(nb_ctx* c, const BodyBuffers& b, bool kick, bool store_
 
 }  // namespace
 
-int split_group_size(const nb_ctx* c) { return 32 * (c->bpl == 1 ? 1 : kBodiesPerLane); }
+int split_group_size(const nb_ctx* c) {
+    // learned contexts keep groups of 64 (the correction kernel's layout)
+    if (c->p.flags & NB_FLAG_LEARNED) return 32 * kBodiesPerLane;
+    return 32 * (c->bpl == 1 ? 1 : c->bpl == 4 ? 4 : kBodiesPerLane);
+}
 
 void launch_force_split(nb_ctx* c, const BodyBuffers& b, bool kick, bool store_acc) {
     c->launches += 1;
@@ -515,11 +520,13 @@ void launch_force_split(nb_ctx* c, const BodyBuffers& b, bool kick, bool store_a
             launch_split_kernel<false, kBodiesPerLane, true>(c, b, kick, store_acc);
     }
     else if (c->p.flags & NB_FLAG_QUADRUPOLE)
-        c->bpl == 1 ? launch_split_kernel<true, 1, false>(c, b, kick, store_acc)
-                    : launch_split_kernel<true, kBodiesPerLane, false>(c, b, kick, store_acc);
+        c->bpl == 1   ? launch_split_kernel<true, 1, false>(c, b, kick, store_acc)
+        : c->bpl == 4 ? launch_split_kernel<true, 4, false>(c, b, kick, store_acc)
+                      : launch_split_kernel<true, kBodiesPerLane, false>(c, b, kick, store_acc);
     else
-        c->bpl == 1 ? launch_split_kernel<false, 1, false>(c, b, kick, store_acc)
-                    : launch_split_kernel<false, kBodiesPerLane, false>(c, b, kick, store_acc);
+        c->bpl == 1   ? launch_split_kernel<false, 1, false>(c, b, kick, store_acc)
+        : c->bpl == 4 ? launch_split_kernel<false, 4, false>(c, b, kick, store_acc)
+                      : launch_split_kernel<false, kBodiesPerLane, false>(c, b, kick, store_acc);
 }
 
 }  // namespace nb

@@ -48,6 +48,10 @@ int check_params(const nb_params* p) {
         return NB_ERR_INVALID;
     if (p->mode != NB_MODE_FP64 && p->mode != NB_MODE_SPLIT && p->mode != NB_MODE_ALLPAIRS)
         return NB_ERR_INVALID;
+    if (p->bodies_per_lane != 0 && p->bodies_per_lane != 1 && p->bodies_per_lane != 2 &&
+        p->bodies_per_lane != 4)
+        return NB_ERR_INVALID;
+    if (p->reserved != 0) return NB_ERR_INVALID;
     if (p->leaf_size < 0 ||
         (p->flags & ~(int32_t)(NB_FLAG_QUADRUPOLE | NB_FLAG_LEARNED | NB_FLAG_CPU_LAW)) != 0)
         return NB_ERR_INVALID;
@@ -418,6 +422,7 @@ int create_context(const nb_params* p, uint64_t n, const double* mass, const dou
     nb_ctx* c = new (std::nothrow) nb_ctx();
     if (!c) return NB_ERR_NOMEM;
     c->p = *p;
+    c->bpl = p->bodies_per_lane > 0 ? p->bodies_per_lane : 2;
     c->n = (int64_t)n;
     c->device = p->device;
     DeviceGuard guard(c->device);
@@ -920,12 +925,12 @@ int nb_autotune(nb_ctx* c, uint32_t steps, int32_t* leaf_out, int32_t* bpl_out) 
     cudaMemcpyAsync(save.mass, A.mass, n * 8, cudaMemcpyDeviceToDevice, c->stream);
     cudaMemcpyAsync(save.orig, A.orig, n * 4, cudaMemcpyDeviceToDevice, c->stream);
     const bool learned = (c->p.flags & NB_FLAG_LEARNED) != 0;
-    const int bpls[2] = {2, 1};
+    const int bpls[3] = {2, 1, 4};
     const int leaves[4] = {4, 8, 16, 32};
     double best = 1e300;
     int best_leaf = c->p.leaf_size, best_bpl = c->bpl;
     int rc = NB_OK;
-    for (int bi = 0; bi < (learned ? 1 : 2) && rc == NB_OK; ++bi)
+    for (int bi = 0; bi < (learned ? 1 : 3) && rc == NB_OK; ++bi)
         for (int li = 0; li < 4 && rc == NB_OK; ++li) {
             c->bpl = bpls[bi];
             c->p.leaf_size = leaves[li];

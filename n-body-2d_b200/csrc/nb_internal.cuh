@@ -180,7 +180,7 @@ struct nb_ctx {
     nb::DeviceScalars* scal = nullptr;   // device
     double* bbox_partials = nullptr;     // [blocks][4]
     int bbox_blocks = 0;
-    int split_blocks[16] = {};            // persistent grids of the SPLIT traversal variants
+    int split_blocks[32] = {};            // persistent grids of the SPLIT traversal variants
     int corr_blocks_per_sm = 0;          // learned correction kernel occupancy (0 = not set up)
     float* mlp_params = nullptr;         // learned mode: FP32 MLP parameters (device)
     void* mlp_infer = nullptr;           // learned mode: BF16 fragment images for inference
@@ -192,7 +192,7 @@ struct nb_ctx {
     bool mlp_ready = false;
     float2* acc32 = nullptr;             // learned mode: traversal accelerations
     nb::Batch batch;                     // batched universes (nuni > 0)
-    int bpl = 2;                         // SPLIT: bodies per lane (group of 32 x bpl)
+    int bpl = 2;                         // SPLIT: bodies per lane, 1, 2 or 4 (groups of 32 x bpl)
     double2* acc = nullptr;              // optional FP64 accelerations (sorted order)
     uint2* dbg_terms = nullptr;          // nb_debug_interactions: per-body {cell, body} terms
     bool want_terms = false;             // the force pass writes dbg_terms

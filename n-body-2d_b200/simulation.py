@@ -70,6 +70,7 @@ class SimConfig:
     learned: bool = False
     bmax_ratio: float = 0.0
     band_theta: float = 0.5  # learned mode: the plain walk's angle the network stands in for
+    bodies_per_lane: int = 0  # SPLIT target groups of 32 x this (1, 2, 4; 0 = 2)
     cpu_law: bool = False   # NB_MODE_ALLPAIRS: the reference CPU backends' pair law
 
     def params(self) -> NbParams:
@@ -84,6 +85,7 @@ class SimConfig:
         p.device = self.device
         p.bmax_ratio = self.bmax_ratio
         p.band_theta = self.band_theta
+        p.bodies_per_lane = self.bodies_per_lane
         p.flags = ((_lib.NB_FLAG_QUADRUPOLE if self.quadrupole else 0)
                    | (_lib.NB_FLAG_LEARNED if self.learned else 0)
                    | (_lib.NB_FLAG_CPU_LAW if self.cpu_law else 0))

@@ -129,7 +129,7 @@ def test_autotune_restores_bodies(nbp):
         p0, v0 = ctx.download()
         a0 = ctx.accelerations()
         leaf, bpl = ctx.autotune(2)
-        assert leaf in (4, 8, 16, 32) and bpl in (1, 2)
+        assert leaf in (4, 8, 16, 32) and bpl in (1, 2, 4)
         p1, v1 = ctx.download()
         assert np.array_equal(p0, p1) and np.array_equal(v0, v1)
         assert ctx.stats().steps == 1
@@ -147,5 +147,5 @@ def test_batch_autotune(nbp):
         leaf, bpl = ctx.autotune(2)
         ctx.step(2)
         pb, _ = ctx.download()
-    assert leaf in (4, 8, 16, 32) and bpl in (1, 2)
+    assert leaf in (4, 8, 16, 32) and bpl in (1, 2, 4)
     assert np.isfinite(pb).all()

@@ -128,3 +128,33 @@ def test_bmax_guard_tightens_the_walk(nbp, quad):
         out[ratio] = (np.percentile(rel_err(a[tgt], exact), 99), st.cell_interactions)
     assert out[0.75][1] >= out[0.0][1]  # only ever opens more cells
     assert out[0.75][0] < 0.7 * out[0.0][0]
+
+
+@pytest.mark.parametrize("bpl", [1, 2, 4])
+def test_group_sizes_theta_zero_and_errors(nbp, orc, bpl):
+    # target groups of 32, 64 and 128 bodies: at theta = 0 every group sums
+    # every body (the FP32 bound of the all-pairs sum holds), and at theta =
+    # 0.5 (monopole and quadrupole) the error stays that of the default groups
+    m, p, v = nbp.universes.colliding_discs(20000, 6)
+    cfg = nbp.SimConfig(theta=0.0, epsilon_squared=EPS2, mode=nbp.NB_MODE_SPLIT, leaf_size=1,
+                        bodies_per_lane=bpl)
+    with nbp.NbContext(cfg, m, p, v) as ctx:
+        a0 = ctx.accelerations()
+    tgt = np.arange(0, 20000, 7)
+    box = orc.bbox_squared(p)
+    center = (0.5 * (box[0] + box[1]), 0.5 * (box[2] + box[3]))
+    bound = orc.allpairs_fp32_bound(m, p, center, targets=tgt, eps2=EPS2)
+    exact = orc.allpairs_plummer(m, p, tgt, eps2=EPS2)
+    assert (np.linalg.norm(a0[tgt] - exact, axis=1) <= bound).all()
+    for quad in (False, True):
+        errs = {}
+        for b in (2, bpl):
+            cfg = nbp.SimConfig(theta=0.5, epsilon_squared=EPS2, mode=nbp.NB_MODE_SPLIT,
+                                quadrupole=quad, bodies_per_lane=b)
+            with nbp.NbContext(cfg, m, p, v) as ctx:
+                ctx.step(1)  # a step first: groups are built by the step's graph too
+                errs[b] = np.percentile(rel_err(ctx.accelerations()[tgt],
+                                                nbp.allpairs_accelerations(
+                                                    m, ctx.download()[0], tgt, EPS2)), 99)
+        # larger groups accept fewer cells (a looser box), smaller ones more
+        assert errs[bpl] <= errs[2] * (1.3 if bpl == 1 else 1.02), (quad, errs)
