@@ -34,6 +34,7 @@ constexpr int kStkAlloc = kStk + 96;   // + one depth-first descent (<= 3 x 30 +
 constexpr int kList = 64;
 constexpr int kBodiesPerLane = 2;      // group of 64 bodies per warp
 constexpr int kDefaultLeaf = 8;        // cells this small are summed body by body
+constexpr int kMaxBPL = 4;             // largest group: 128 bodies per warp
 
 // Interaction lists hold entries in pairs, so that one lane evaluates two
 // entries with the packed FP32x2 instructions of sm_100 (FADD2/FMUL2/FFMA2):
@@ -47,6 +48,7 @@ struct WarpLists {
     float2 qb[kList / 2];
     float4 bxy[kList / 2];
     float2 bm[kList / 2];
+    float2 tot[2 * kMaxBPL][32];   // running {x, y} sums of each lane's bodies (halves kept apart)
 };
 
 // An entry that adds nothing: zero mass far away, so that d2 stays finite
@@ -163,9 +165,27 @@ __device__ __forceinline__ void quad_pair(const float4 xy, const float2 m, const
     }
 }
 
+// Each flush of a list is summed into the lane's register sums, which start
+// every flush at zero and are then added to the body's running totals, kept
+// in the warp's shared lists (blocked summation): the FP32 rounding of a
+// body's total then grows with the flush length plus the number of flushes,
+// not with the number of terms (a body's terms mostly share their sign, so a
+// running sum's rounding adds up).  The totals live in shared memory so that
+// the blocking costs no registers.
+template <int kBPL>
+__device__ __forceinline__ void fold_block(WarpLists& L, float2* ax, float2* ay) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int b = 0; b < kBPL; ++b) {
+        L.tot[2 * b][lane] = __fadd2_rn(L.tot[2 * b][lane], ax[b]);
+        L.tot[2 * b + 1][lane] = __fadd2_rn(L.tot[2 * b + 1][lane], ay[b]);
+        ax[b] = ay[b] = make_float2(0.f, 0.f);
+    }
+}
+
 // Sum the first npairs pairs of the cell list.
 template <bool kQuad, bool kZeroSoft, int kBPL>
-__device__ __forceinline__ void sum_cells(const WarpLists& L, int npairs, const float2* nx,
+__device__ __forceinline__ void sum_cells(WarpLists& L, int npairs, const float2* nx,
                                           const float2* ny, const float2 e2, float2* ax,
                                           float2* ay) {
     if (npairs == 16) {
@@ -186,10 +206,11 @@ __device__ __forceinline__ void sum_cells(const WarpLists& L, int npairs, const 
                 mono_pair<kZeroSoft, kBPL>(L.cxy[k], L.cm[k], nx, ny, e2, ax, ay);
         }
     }
+    fold_block<kBPL>(L, ax, ay);
 }
 
 template <bool kZeroSoft, int kBPL>
-__device__ __forceinline__ void sum_bodies(const WarpLists& L, int npairs, const float2* nx,
+__device__ __forceinline__ void sum_bodies(WarpLists& L, int npairs, const float2* nx,
                                            const float2* ny, const float2 e2, float2* ax,
                                            float2* ay) {
     if (npairs == 16) {
@@ -200,6 +221,7 @@ __device__ __forceinline__ void sum_bodies(const WarpLists& L, int npairs, const
         for (int k = 0; k < npairs; ++k)
             mono_pair<kZeroSoft, kBPL>(L.bxy[k], L.bm[k], nx, ny, e2, ax, ay);
     }
+    fold_block<kBPL>(L, ax, ay);
 }
 
 // Walk the tree for one group [g0, g1] of <= 32 kBPL bodies (lane l owns
@@ -241,6 +263,8 @@ __device__ __forceinline__ void walk_group(WarpLists& L, const Tree& t, int root
     const float2 e2 = make_float2(eps2, eps2);
     ncell = 0;
     npair = 0;
+#pragma unroll
+    for (int b = 0; b < kBPL; ++b) L.tot[2 * b][lane] = L.tot[2 * b + 1][lane] = make_float2(0.f, 0.f);
     int ccount = 0, bcount = 0, size = 1;
     if (lane == 0) L.stack[0] = root;
     __syncwarp();
@@ -387,8 +411,9 @@ __device__ __forceinline__ void walk_group(WarpLists& L, const Tree& t, int root
     npair += bcount;
 #pragma unroll
     for (int b = 0; b < kBPL; ++b) {
-        ax[b] = ax2[b].x + ax2[b].y;
-        ay[b] = ay2[b].x + ay2[b].y;
+        const float2 tx = L.tot[2 * b][lane], ty = L.tot[2 * b + 1][lane];
+        ax[b] = tx.x + tx.y;
+        ay[b] = ty.x + ty.y;
     }
     __syncwarp();
 }
