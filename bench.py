@@ -250,10 +250,8 @@ def gpu_baseline(nb, device: int) -> dict:
     events (FP64 parity walk and SPLIT)."""
     if str(ROOT) not in sys.path:
         sys.path.insert(0, str(ROOT))
-    from oracle import refgpu
-
     m, p, v = nb.universes.make("grid", 262144, 0)
-    ref = _ref_gpu_record(refgpu.time_steps(m, p, v, theta=0.5, steps=5), 262144)
+    ref = _ref_gpu_record(_ref_gpu_timed(m, p, v, 0.5, 5), 262144)
     mk = lambda mode: nb.SimConfig(timestep=1e-4, theta=0.5, epsilon_squared=1e-4, G=1.0,
                                    mode=mode, device=device)
     fp64 = _timed_context(nb, mk(nb.NB_MODE_FP64), m, p, v, 3, 20, accuracy=False)
@@ -326,6 +324,16 @@ GRID_CASE = ("jittered grid, 512 x 512 = 262,144 bodies, seed 0, theta 0.5: the 
              "replay finds at most 28 of the reference kernel's 32 traversal-stack entries in use")
 
 
+def _ref_gpu_timed(m, p, v, theta: float, steps: int) -> dict:
+    """refgpu.time_steps, with any failure of the harness reported, not raised."""
+    from oracle import refgpu
+
+    try:
+        return refgpu.time_steps(m, p, v, theta=theta, steps=steps)
+    except Exception as e:  # the record says why; the arm's own line still prints
+        return {"unavailable": f"reference GPU harness failed: {type(e).__name__}: {e}"[:300]}
+
+
 def _ref_gpu_record(r: dict, n: int) -> dict:
     if "seconds_per_step" not in r:
         return r
@@ -339,16 +347,13 @@ def reference_gpu_records(args, m, p, v) -> dict:
     the benchmark workload when the oracle's replay certifies it (else the
     refusal, with the stack depth the replay found), and always the jittered
     262,144-body grid, which it certifies."""
-    from oracle import refgpu
-
     out = {}
     steps = max(1, min(args.steps, 5))
     if args.kind != "grid":
-        out[args.workload] = _ref_gpu_record(
-            refgpu.time_steps(m, p, v, theta=args.theta, steps=steps), args.n)
+        out[args.workload] = _ref_gpu_record(_ref_gpu_timed(m, p, v, args.theta, steps), args.n)
     nb = _package()
     gm, gp, gv = nb.universes.make("grid", 262144, 0)
-    rec = _ref_gpu_record(refgpu.time_steps(gm, gp, gv, theta=0.5, steps=steps), 262144)
+    rec = _ref_gpu_record(_ref_gpu_timed(gm, gp, gv, 0.5, steps), 262144)
     rec["case"] = GRID_CASE
     out["grid256k"] = rec
     return out
