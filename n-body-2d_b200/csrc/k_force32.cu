@@ -165,13 +165,15 @@ __device__ __forceinline__ void quad_pair(const float4 xy, const float2 m, const
     }
 }
 
-// Each flush of a list is summed into the lane's register sums, which start
-// every flush at zero and are then added to the body's running totals, kept
-// in the warp's shared lists (blocked summation): the FP32 rounding of a
-// body's total then grows with the flush length plus the number of flushes,
-// not with the number of terms (a body's terms mostly share their sign, so a
-// running sum's rounding adds up).  The totals live in shared memory so that
-// the blocking costs no registers.
+// Every kFoldFlushes list flushes, the lane's register sums are added to the
+// body's running totals, kept in the warp's shared lists, and restart from
+// zero (blocked summation): the FP32 rounding of a body's total then grows
+// with the block length plus the number of blocks, not with the number of
+// terms (a body's terms mostly share their sign, so a running sum's rounding
+// adds up).  The totals live in shared memory so that the blocking costs no
+// registers, and a block spans four flushes so that it costs few
+// instructions.
+constexpr int kFoldFlushes = 4;
 template <int kBPL>
 __device__ __forceinline__ void fold_block(WarpLists& L, float2* ax, float2* ay) {
     const int lane = threadIdx.x & 31;
@@ -187,7 +189,7 @@ __device__ __forceinline__ void fold_block(WarpLists& L, float2* ax, float2* ay)
 template <bool kQuad, bool kZeroSoft, int kBPL>
 __device__ __forceinline__ void sum_cells(WarpLists& L, int npairs, const float2* nx,
                                           const float2* ny, const float2 e2, float2* ax,
-                                          float2* ay) {
+                                          float2* ay, bool fold) {
     if (npairs == 16) {
 #pragma unroll 4
         for (int k = 0; k < 16; ++k) {
@@ -206,13 +208,13 @@ __device__ __forceinline__ void sum_cells(WarpLists& L, int npairs, const float2
                 mono_pair<kZeroSoft, kBPL>(L.cxy[k], L.cm[k], nx, ny, e2, ax, ay);
         }
     }
-    fold_block<kBPL>(L, ax, ay);
+    if (fold) fold_block<kBPL>(L, ax, ay);
 }
 
 template <bool kZeroSoft, int kBPL>
 __device__ __forceinline__ void sum_bodies(WarpLists& L, int npairs, const float2* nx,
                                            const float2* ny, const float2 e2, float2* ax,
-                                           float2* ay) {
+                                           float2* ay, bool fold) {
     if (npairs == 16) {
 #pragma unroll 4
         for (int k = 0; k < 16; ++k)
@@ -221,7 +223,7 @@ __device__ __forceinline__ void sum_bodies(WarpLists& L, int npairs, const float
         for (int k = 0; k < npairs; ++k)
             mono_pair<kZeroSoft, kBPL>(L.bxy[k], L.bm[k], nx, ny, e2, ax, ay);
     }
-    fold_block<kBPL>(L, ax, ay);
+    if (fold) fold_block<kBPL>(L, ax, ay);
 }
 
 // Walk the tree for one group [g0, g1] of <= 32 kBPL bodies (lane l owns
@@ -266,6 +268,7 @@ __device__ __forceinline__ void walk_group(WarpLists& L, const Tree& t, int root
 #pragma unroll
     for (int b = 0; b < kBPL; ++b) L.tot[2 * b][lane] = L.tot[2 * b + 1][lane] = make_float2(0.f, 0.f);
     int ccount = 0, bcount = 0, size = 1;
+    int flushes = 0;  // warp-uniform: every lane takes part in every flush
     if (lane == 0) L.stack[0] = root;
     __syncwarp();
 
@@ -330,7 +333,8 @@ __device__ __forceinline__ void walk_group(WarpLists& L, const Tree& t, int root
         ccount += __popc(acc_mask);
         __syncwarp();
         if (ccount >= 32) {
-            sum_cells<kQuad, kZeroSoft, kBPL>(L, 16, nx, ny, e2, ax2, ay2);
+            sum_cells<kQuad, kZeroSoft, kBPL>(L, 16, nx, ny, e2, ax2, ay2,
+                                              ++flushes % kFoldFlushes == 0);
             ncell += 32;
             __syncwarp();
             // pairs 16.. move down; source and destination never overlap
@@ -384,7 +388,8 @@ __device__ __forceinline__ void walk_group(WarpLists& L, const Tree& t, int root
             bcount += added;
             __syncwarp();
             if (bcount >= 32) {
-                sum_bodies<kZeroSoft, kBPL>(L, 16, nx, ny, e2, ax2, ay2);
+                sum_bodies<kZeroSoft, kBPL>(L, 16, nx, ny, e2, ax2, ay2,
+                                            ++flushes % kFoldFlushes == 0);
                 npair += 32;
                 __syncwarp();
                 if (lane < (bcount - 31) / 2) {
@@ -405,8 +410,8 @@ __device__ __forceinline__ void walk_group(WarpLists& L, const Tree& t, int root
         if (bcount & 1) put_entry(L.bxy, L.bm, bcount, kPadCoord, kPadCoord, 0.f);
     }
     __syncwarp();
-    sum_cells<kQuad, kZeroSoft, kBPL>(L, (ccount + 1) >> 1, nx, ny, e2, ax2, ay2);
-    sum_bodies<kZeroSoft, kBPL>(L, (bcount + 1) >> 1, nx, ny, e2, ax2, ay2);
+    sum_cells<kQuad, kZeroSoft, kBPL>(L, (ccount + 1) >> 1, nx, ny, e2, ax2, ay2, false);
+    sum_bodies<kZeroSoft, kBPL>(L, (bcount + 1) >> 1, nx, ny, e2, ax2, ay2, true);
     ncell += ccount;
     npair += bcount;
 #pragma unroll
