@@ -554,13 +554,16 @@ def run_ours(args) -> None:
                 "ratio": lv["speedup_vs_plain"], "learned_p50": lv["p50"], "learned_p99": lv["p99"],
                 "plain_p99": accuracy["p99"], "fallback_rule": lv["fallback_rule"],
                 "target_ratio": 2.0}
-    if (rank == 0 and not args.no_learned_comparison and args.workload == "collision4m"
+    # the extra records run on one GPU only: under torchrun the other ranks
+    # would wait at the closing barrier longer than the process group allows
+    if (world == 1 and not args.no_learned_comparison and args.workload == "collision4m"
             and args.mode == "split" and not args.learned and not args.quad and not args.bmax):
         line["at_accuracy_bar"] = at_accuracy_bar(args, nb, m, p, v, local)
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.n, args.theta, m, p, v)
-        line["gpu_baseline"] = gpu_baseline(nb, local)
-    if rank == 0 and args.workload == "collision4m" and not args.no_sub_configs:
+        if world == 1:
+            line["gpu_baseline"] = gpu_baseline(nb, local)
+    if world == 1 and args.workload == "collision4m" and not args.no_sub_configs:
         line["configs"] = sub_configs(args, nb, local)
     if world > 1:
         import torch.distributed as dist
