@@ -246,9 +246,36 @@ __device__ void bucket_moments(const double2* __restrict__ pos, const double* __
 __global__ void tree_link(const uint64_t* __restrict__ key, int n,
                           const double2* __restrict__ pos, const double* __restrict__ mass,
                           Tree t, DeviceScalars* __restrict__ s) {
-    // one thread per cell, so every lane of a warp builds a cell
-    const int id = blockIdx.x * blockDim.x + threadIdx.x;
-    if (id >= s->cells) return;
+    // one thread per cell; the block's 256 consecutive cells are re-dealt by
+    // level (a counting sort in shared memory), so a warp's lanes build cells
+    // of similar size while the block keeps to one stretch of the codes
+    __shared__ int lvl_cnt[32];
+    __shared__ int dealt[kThreads];
+    const int cells = s->cells;
+    const int id0 = blockIdx.x * blockDim.x + threadIdx.x;
+    if (threadIdx.x < 32) lvl_cnt[threadIdx.x] = 0;
+    __syncthreads();
+    int c0 = 31;  // past every level: empty slots go last
+    if (id0 < cells) {
+        const int i0 = t.rep_of[id0];
+        c0 = lcp_digits(key[i0], key[i0 + 1]);
+    }
+    const int rank = atomicAdd(&lvl_cnt[c0], 1);
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        const int v = lvl_cnt[threadIdx.x];
+        int inc = v;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int u = __shfl_up_sync(kFull, inc, o);
+            if ((int)threadIdx.x >= o) inc += u;
+        }
+        lvl_cnt[threadIdx.x] = inc - v;
+    }
+    __syncthreads();
+    dealt[lvl_cnt[c0] + rank] = id0;
+    __syncthreads();
+    const int id = dealt[threadIdx.x];
+    if (id >= cells) return;
     const int i = t.rep_of[id];
     const int c = lcp_digits(key[i], key[i + 1]);
     const int first = t.start_of[i];
