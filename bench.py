@@ -527,7 +527,11 @@ def run_ours(args) -> None:
                                     f"median SM clock {sm_mhz} MHz",
                      "interactions_per_s": interactions / (force_ms * 1e-3),
                      "interactions_per_body": interactions / args.n,
-                     "flops_per_interaction": FLOPS_PER_INTERACTION},
+                     "flops_per_interaction": FLOPS_PER_INTERACTION,
+                     # one 1/sqrt per interaction on the SFU: 16 per clock per SM
+                     "sfu_frac": round(interactions / (force_ms * 1e-3)
+                                       / (148 * 16 * sm_mhz * 1e6), 4),
+                     "sfu_peak_source": f"nominal 16 MUFU ops/clk/SM x 148 SMs at {sm_mhz} MHz"},
         "rooflines_hbm": rooflines, "hbm_peak_source": f"{peak_kind} MEASURED_PEAKS.json hbm_gbs"
         if peak_kind == "measured" else "fallback 6.65 TB/s",
         "phases_ms": {k: round(v, 4) for k, v in phases.items()},
