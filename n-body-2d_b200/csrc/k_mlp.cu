@@ -557,7 +557,7 @@ mlp_correct_kick(const InferW* __restrict__ Wg, Tree t, const DeviceScalars* __r
 constexpr int kTcRows = 128;
 constexpr int kTcWarps = kTcRows / 32;  // one warp per 32 rows (TMEM lanes)
 constexpr uint32_t kTcCols = 64;    // TMEM columns a CTA allocates; the three layers share them
-constexpr int kTcBlocksPerSm = 6;   // shared memory allows six CTAs per SM, TMEM eight
+constexpr int kTcBlocksPerSm = 5;   // shared memory allows five CTAs per SM, TMEM eight
 constexpr int kTcSpin = 1 << 20;    // bound on each wait for an MMA to complete
 
 struct UmmaW {
@@ -603,7 +603,9 @@ struct TcSmem {
     UmmaW W;
     alignas(128) uint4 a1[kTcRows * 16 / 8];   // layer-1 input rows (K = 16)
     alignas(128) uint4 a2[kTcRows * kH / 8];   // hidden rows (K = 64), both layers
+    alignas(16) float xs[kTcRows * kNin];      // the next tile's FP32 features (bulk copy)
     alignas(8) uint64_t mbar;                  // MMA completion
+    alignas(8) uint64_t xbar;                  // feature tile arrived
     uint32_t tmem;                             // TMEM base address from tcgen05.alloc
     int fail;                                  // a wait for an MMA ran out
 };
@@ -725,7 +727,9 @@ mlp_forward_tc(const UmmaW* __restrict__ Wg, const float* __restrict__ X, int64_
     }
     if (tid == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&S.mbar)) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&S.xbar)) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         S.fail = 0;
     }
     if (warp == 0) {
@@ -744,16 +748,45 @@ mlp_forward_tc(const UmmaW* __restrict__ Wg, const float* __restrict__ X, int64_
                    w3_addr = smem_u32(S.W.w3);
     const int row = tid;  // this thread's tile row and TMEM lane
     uint32_t phase = 0;
+    // the features of the CTA's first tile; each later tile's are copied in
+    // while the tile before it runs through the network
+    auto fetch = [&](int64_t tile) {
+        const int64_t rows = std::min<int64_t>(kTcRows, n - tile * kTcRows);
+        const unsigned bytes = (unsigned)(rows * kNin * sizeof(float));  // 48 B a row
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(
+                         smem_u32(&S.xbar)),
+                     "r"(bytes)
+                     : "memory");
+        asm volatile(
+            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
+            "[%3];" ::"r"(smem_u32(S.xs)),
+            "l"(X + tile * kTcRows * kNin), "r"(bytes), "r"(smem_u32(&S.xbar))
+            : "memory");
+    };
+    if (tid == 0 && (int64_t)blockIdx.x * kTcRows < n) fetch(blockIdx.x);
+    uint32_t xphase = 0;
     for (int64_t tile = blockIdx.x; tile * kTcRows < n; tile += gridDim.x) {
         if (S.fail) break;  // uniform: set before the barrier that ended the last tile
         const int64_t sr = tile * kTcRows + row;
+        if (!mbar_wait(&S.xbar, xphase)) S.fail = 1;
+        xphase ^= 1u;
         uint32_t x[8];
+        {
+            float v[kNin];
+            const float4* src = reinterpret_cast<const float4*>(S.xs + row * kNin);
 #pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            const int f0 = infer_feature(2 * k), f1 = infer_feature(2 * k + 1);
-            const float v0 = sr < n && f0 >= 0 ? X[sr * kNin + f0] : 0.f;
-            const float v1 = sr < n && f1 >= 0 ? X[sr * kNin + f1] : 0.f;
-            x[k] = pack_bf16(v0, v1);
+            for (int q = 0; q < kNin / 4; ++q) {
+                const float4 f = sr < n ? src[q] : make_float4(0.f, 0.f, 0.f, 0.f);
+                v[4 * q] = f.x;
+                v[4 * q + 1] = f.y;
+                v[4 * q + 2] = f.z;
+                v[4 * q + 3] = f.w;
+            }
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const int f0 = infer_feature(2 * k), f1 = infer_feature(2 * k + 1);
+                x[k] = pack_bf16(f0 >= 0 ? v[f0] : 0.f, f1 >= 0 ? v[f1] : 0.f);
+            }
         }
         {
             uint4* dst = S.a1 + umma_off(row, 0, 256) / 16;
@@ -761,8 +794,9 @@ mlp_forward_tc(const UmmaW* __restrict__ Wg, const float* __restrict__ X, int64_
             dst[8] = make_uint4(x[4], x[5], x[6], x[7]);
         }
         fence_async_smem();
-        __syncthreads();
+        __syncthreads();  // every row of xs has been read: the next tile may land there
         if (tid == 0) {
+            if ((tile + gridDim.x) * kTcRows < n) fetch(tile + gridDim.x);
             tc_fence_after();
             umma_bf16(tmem, umma_desc(a1_addr, 128, 256), umma_desc(w1_addr, 128, 256),
                       umma_idesc(kTcRows, kH), 0u);
@@ -815,8 +849,10 @@ mlp_forward_tc(const UmmaW* __restrict__ Wg, const float* __restrict__ X, int64_
         __syncthreads();  // TMEM columns and operand rows are free for the next tile
     }
     if (S.fail) {
-        // the last MMAs may still run: wait for them (bounded) before freeing TMEM
+        // the last MMAs may still run, and the feature tile fetched for the
+        // tile not taken: wait for both (bounded) before TMEM and the CTA go
         mbar_wait(&S.mbar, phase ^ 1u);
+        mbar_wait(&S.xbar, xphase);
         if (tid == 0) atomicOr(err, kErrTimeout);
     }
     tc_fence_before();
