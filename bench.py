@@ -69,11 +69,11 @@ def _package():
 
 # DRAM bytes one launch of the SPLIT monopole force kernel moves per body:
 # ncu dram__bytes_read.sum + dram__bytes_write.sum of one force_split launch
-# on the 1,048,576-body collision (77.5 MB + 7.1 MB = 84.6 MB, --clock-control
+# on the 1,048,576-body collision (77.5 MB + 6.6 MB = 84.1 MB, --clock-control
 # none).  Bodies and cells both grow linearly with N, so the figure scales by
 # N; it is a property of the kernel's access pattern, re-measured when the
 # kernel changes.
-FORCE_TRAFFIC_BYTES_PER_BODY = 84.6e6 / 1048576
+FORCE_TRAFFIC_BYTES_PER_BODY = 84.1e6 / 1048576
 
 
 def _peaks() -> tuple[dict, str]:
