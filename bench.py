@@ -84,27 +84,75 @@ def _peaks() -> tuple[dict, str]:
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons, sampled every 20 ms from before
-    the timed region to after it; samples are kept when their timestamp falls
-    inside the region widened by one interval (a region of a few tens of ms
-    would otherwise see none)."""
+    """SM clock and clock-event reasons of the benchmarked GPU, sampled from
+    before the timed region to after it; samples are kept when their timestamp
+    falls inside the region widened by one interval.  NVML (read-only queries,
+    the device found by its UUID) is polled every 2 ms from a thread, so even a
+    region of a few tens of ms gets a dozen samples; nvidia-smi at 20 ms is the
+    fallback when NVML cannot be loaded."""
 
     FIELDS = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
-    INTERVAL_MS = 20
+    REASON_BITS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40),
+                   ("sw_thermal_slowdown", 0x20), ("sw_power_cap", 0x4))
+    NVML_INTERVAL_MS = 2
+    SMI_INTERVAL_MS = 20
 
     def __init__(self, device: int):
         self.device = device
         self.proc = None
+        self.nvml = None
+        self.thread = None
+        self.stop = None
         self.t0 = self.t1 = None
-        self.lines: list[str] = []
+        self.samples: list[tuple] = []   # (time, sm MHz, max sm MHz, reason names)
+        self.interval_ms = self.SMI_INTERVAL_MS
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+
+        pynvml.nvmlInit()
+        try:
+            uuid = str(torch.cuda.get_device_properties(self.device).uuid)
+            return pynvml, pynvml.nvmlDeviceGetHandleByUUID(
+                uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.device)
+
+    def _poll(self, pynvml, h):
+        reasons_of = getattr(pynvml, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            pynvml.nvmlDeviceGetCurrentClocksThrottleReasons
+        smax = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+        while not self.stop.is_set():
+            try:
+                clk = pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
+                bits = reasons_of(h)
+            except Exception:
+                break
+            self.samples.append((time.time(), float(clk), float(smax),
+                                 [name for name, bit in self.REASON_BITS if bits & bit]))
+            self.stop.wait(self.NVML_INTERVAL_MS / 1000.0)
 
     def __enter__(self):
+        import threading
+
+        try:
+            pynvml, h = self._nvml_handle()
+            self.nvml = pynvml
+            self.interval_ms = self.NVML_INTERVAL_MS
+            self.stop = threading.Event()
+            self.thread = threading.Thread(target=self._poll, args=(pynvml, h), daemon=True)
+            self.thread.start()
+            time.sleep(0.05)
+            return self
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", str(self.INTERVAL_MS), "-i", str(self.device)],
+                 "-lms", str(self.SMI_INTERVAL_MS), "-i", str(self.device)],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             time.sleep(0.5)  # let the sampler start before the region opens
         except OSError:
@@ -116,9 +164,16 @@ class ClockSampler:
 
     def mark_end(self):
         self.t1 = time.time()
-        time.sleep(2.5 * self.INTERVAL_MS / 1000.0)
+        time.sleep(2.5 * self.interval_ms / 1000.0)
 
     def __exit__(self, *exc):
+        if self.thread is not None:
+            self.stop.set()
+            self.thread.join(timeout=5)
+            try:
+                self.nvml.nvmlShutdown()
+            except Exception:
+                pass
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -126,9 +181,10 @@ class ClockSampler:
             except subprocess.TimeoutExpired:
                 self.proc.kill()
                 out, _ = self.proc.communicate()
-            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+            self.samples = self._parse_smi([ln for ln in out.splitlines() if ln.strip()])
 
-    def summary(self) -> dict:
+    @staticmethod
+    def _parse_smi(lines):
         import datetime
 
         def stamp(text):
@@ -139,30 +195,37 @@ class ClockSampler:
                     pass
             return None
 
-        sm, smax, reasons = [], [], set()
-        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
-        pad = self.INTERVAL_MS / 1000.0
-        parsed = [[x.strip() for x in ln.split(",")] for ln in self.lines]
-        parsed = [p for p in parsed if len(p) >= 10]
-        stamps = [stamp(p[0]) for p in parsed]
-        windowed = self.t0 is not None and any(t is not None for t in stamps)
-        for parts, ts in zip(parsed, stamps):
+        names = [name for name, _ in ClockSampler.REASON_BITS]
+        out = []
+        for ln in lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 10:
+                continue
             try:
                 clk, clk_max = float(parts[2]), float(parts[3])
             except ValueError:
                 continue
+            out.append((stamp(parts[0]), clk, clk_max,
+                        [n for n, val in zip(names, parts[6:10]) if val.lower() == "active"]))
+        return out
+
+    def summary(self) -> dict:
+        pad = self.interval_ms / 1000.0
+        windowed = self.t0 is not None and any(ts is not None for ts, *_ in self.samples)
+        sm, smax, reasons = [], [], set()
+        for ts, clk, clk_max, names in self.samples:
             if windowed and (ts is None or not (self.t0 - pad <= ts <= self.t1 + pad)):
                 continue
             sm.append(clk)
             smax.append(clk_max)
-            for name, val in zip(names, parts[6:10]):
-                if val.lower() == "active":
-                    reasons.add(name)
+            reasons.update(names)
         if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0,
+                    "source": "nvml" if self.nvml else "nvidia-smi"}
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax),
                 "reasons": sorted(reasons), "samples": len(sm),
-                "interval_ms": self.INTERVAL_MS, "windowed": windowed}
+                "interval_ms": self.interval_ms, "windowed": windowed,
+                "source": "nvml" if self.nvml else "nvidia-smi"}
 
 
 def _dist():

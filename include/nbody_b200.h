@@ -87,8 +87,9 @@ typedef struct nb_params {
     double band_theta;      /* learned mode: the opening angle of the plain walk the
                                correction stands in for; cells accepted at theta that
                                this angle would open get the network's term (0 = 0.5) */
-    int32_t bodies_per_lane;/* SPLIT: target group size 32 x this, 1, 2 or 4 (0 = 2; learned
-                               contexts always use 2); nb_autotune may change it */
+    int32_t bodies_per_lane;/* SPLIT: target group size 32 x this, 1, 2 or 4 (0 = 1 below
+                               131,072 bodies, else 2; learned contexts always use 2);
+                               nb_autotune may change it */
     int32_t reserved;       /* must be 0 */
 } nb_params;
 

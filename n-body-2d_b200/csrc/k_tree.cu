@@ -835,9 +835,17 @@ learned_features(DeviceScalars* __restrict__ s, const double2* __restrict__ pos,
 // exactly gsize bodies and the child's rest starts the next group.  Multi-body
 // leaves larger than a group are cut into chunks of gsize.  kWrite = false
 // counts the groups of each cell, kWrite = true writes them at gbase[cell].
+//
+// Children in key order are quadrants 0..3; 0,1 and 2,3 are the two halves of
+// the cell, while a run that takes quadrants from both halves has the whole
+// cell as its bounding box.  When one child is large (it emits its own
+// groups), such a box would cover that dense quadrant and the group's walk
+// would open it down to its bodies: in a sparse disc tail, a group of outer
+// bodies then walked the whole core on one warp (2.3 ms of a 65,536-body
+// step).  So with a large child present, runs also end at the half boundary.
 template <bool kWrite>
 __global__ void tree_groups(int n, int gsize, int fill, Tree t, const DeviceScalars* __restrict__ s,
-                            Batch bt) {
+                            Batch bt, const uint64_t* __restrict__ key) {
     const int id = blockIdx.x * blockDim.x + threadIdx.x;
     const int cells = s->cells;
     if (id >= n) return;
@@ -869,20 +877,32 @@ __global__ void tree_groups(int n, int gsize, int fill, Tree t, const DeviceScal
     } else {
         const int4 ch = t.child[id];
         const int refs[4] = {ch.x, ch.y, ch.z, ch.w};
-        int run_a = -1, run_b = -1;
+        int ca[4], cb[4];
+        bool large = false;  // some child emits its own groups
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int r = refs[q];
+            ca[q] = cb[q] = -1;
+            if (r == INT_MIN) continue;
+            if (r >= 0) {
+                const int2 cr = t.range[r];
+                ca[q] = cr.x;
+                cb[q] = cr.y;
+            } else {
+                ca[q] = ~r;
+                cb[q] = t.leaf_last[ca[q]];
+            }
+            large |= cb[q] - ca[q] + 1 > gsize || (bt.nuni && bt.uid[ca[q]] != bt.uid[cb[q]]);
+        }
+        // the children differ in digit `level` of their codes; its high bit is
+        // the half (read only when a large child makes it matter)
+        const int level = large ? min(lcp_digits(key[rg.x], key[rg.y]), 31) : 0;
+        int run_a = -1, run_b = -1, run_half = 0;
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             const int r = refs[q];
             if (r == INT_MIN) break;
-            int a, b;
-            if (r >= 0) {
-                const int2 cr = t.range[r];
-                a = cr.x;
-                b = cr.y;
-            } else {
-                a = ~r;
-                b = t.leaf_last[a];
-            }
+            const int a = ca[q], b = cb[q];
             const int cnt = b - a + 1;
             if (cnt > gsize || (bt.nuni && bt.uid[a] != bt.uid[b])) {  // the child emits
                 if (run_a >= 0) emit(run_a, run_b);
@@ -891,8 +911,11 @@ __global__ void tree_groups(int n, int gsize, int fill, Tree t, const DeviceScal
                     for (int k = a; k <= b; k += gsize) emit(k, min(b, k + gsize - 1));
                 continue;
             }
-            // a group never spans two universes (a forest cell's children may)
-            if (run_a >= 0 && bt.nuni && bt.uid[a] != bt.uid[run_a]) {
+            const int half = large ? (int)(key[a] >> (63 - 2 * level)) & 1 : 0;
+            // a group never spans two universes (a forest cell's children may),
+            // nor both halves of a cell that has a large child
+            if (run_a >= 0 && ((bt.nuni && bt.uid[a] != bt.uid[run_a]) ||
+                               (large && half != run_half))) {
                 emit(run_a, run_b);
                 run_a = -1;
             } else if (run_a >= 0 && b - run_a + 1 > gsize) {
@@ -906,7 +929,10 @@ __global__ void tree_groups(int n, int gsize, int fill, Tree t, const DeviceScal
                 emit(run_a, run_b);
                 run_a = -1;
             }
-            if (run_a < 0) run_a = a;
+            if (run_a < 0) {
+                run_a = a;
+                run_half = half;
+            }
             run_b = b;
         }
         if (run_a >= 0) emit(run_a, run_b);
@@ -954,14 +980,15 @@ void launch_groups(nb_ctx* c) {
     // warps, measured 2.6% off the walk at 4M with slightly lower errors); the
     // learned correction keeps groups of whole cells, whose residuals it fits
     const int fill = (c->p.flags & NB_FLAG_LEARNED) ? 0 : 1;
+    const uint64_t* key = c->sort.key[0];
     tree_groups<false><<<blocks_for(n, kThreads), kThreads, 0, c->stream>>>(n, gsize, fill, c->tree,
-                                                                            c->scal, c->batch);
+                                                                            c->scal, c->batch, key);
     scan_reduce<<<sblocks, kThreads, 0, c->stream>>>(c->tree.gcount, n, c->scan.block_sums);
     scan_block_sums<<<1, kThreads, 0, c->stream>>>(c->scan.block_sums, sblocks, &c->scal->groups);
     scan_apply<<<sblocks, kThreads, 0, c->stream>>>(c->tree.gcount, n, c->scan.block_sums,
                                                      c->tree.gbase, nullptr);
     tree_groups<true><<<blocks_for(n, kThreads), kThreads, 0, c->stream>>>(n, gsize, fill, c->tree,
-                                                                           c->scal, c->batch);
+                                                                           c->scal, c->batch, key);
 }
 
 void launch_tree(nb_ctx* c, const BodyBuffers& b) {

@@ -422,7 +422,9 @@ int create_context(const nb_params* p, uint64_t n, const double* mass, const dou
     nb_ctx* c = new (std::nothrow) nb_ctx();
     if (!c) return NB_ERR_NOMEM;
     c->p = *p;
-    c->bpl = p->bodies_per_lane > 0 ? p->bodies_per_lane : 2;
+    // default group size: 32 bodies below 131,072 bodies (too few groups of 64
+    // to fill the GPU; 16,384- and 65,536-body discs step 7-8% faster), else 64
+    c->bpl = p->bodies_per_lane > 0 ? p->bodies_per_lane : (n < 131072 ? 1 : 2);
     c->n = (int64_t)n;
     c->device = p->device;
     DeviceGuard guard(c->device);

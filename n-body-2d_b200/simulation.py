@@ -70,7 +70,7 @@ class SimConfig:
     learned: bool = False
     bmax_ratio: float = 0.0
     band_theta: float = 0.5  # learned mode: the plain walk's angle the network stands in for
-    bodies_per_lane: int = 0  # SPLIT target groups of 32 x this (1, 2, 4; 0 = 2)
+    bodies_per_lane: int = 0  # SPLIT target groups of 32 x this (1, 2, 4; 0 = 1 below 131,072 bodies, else 2)
     cpu_law: bool = False   # NB_MODE_ALLPAIRS: the reference CPU backends' pair law
 
     def params(self) -> NbParams:

@@ -3,6 +3,8 @@
 SPLIT decides acceptance once per 32-body group, so its cell set differs from
 the reference's per-body walk; it is judged against the FP64 all-pairs sum and
 against the FP64 parity mode's own error."""
+import pathlib
+
 import numpy as np
 import pytest
 
@@ -158,3 +160,44 @@ def test_group_sizes_theta_zero_and_errors(nbp, orc, bpl):
                                                     m, ctx.download()[0], tgt, EPS2)), 99)
         # larger groups accept fewer cells (a looser box), smaller ones more
         assert errs[bpl] <= errs[2] * (1.3 if bpl == 1 else 1.02), (quad, errs)
+
+
+def _bodies_in_group_boxes(pos, groups, chunk=64):
+    """For each group [first, last] (device order), how many bodies of pos lie
+    inside the bounding box of the group's own bodies."""
+    lo = np.array([pos[a:b + 1].min(axis=0) for a, b in groups])
+    hi = np.array([pos[a:b + 1].max(axis=0) for a, b in groups])
+    out = np.empty(len(groups), dtype=np.int64)
+    for s in range(0, len(groups), chunk):
+        l, h = lo[s:s + chunk, None, :], hi[s:s + chunk, None, :]
+        inside = ((pos[None] >= l) & (pos[None] <= h)).all(axis=2)
+        out[s:s + chunk] = inside.sum(axis=1)
+    return out
+
+
+@pytest.mark.parametrize("kind", ["disc", "plummer"])
+@pytest.mark.parametrize("bpl", [1, 2, 4])
+@pytest.mark.parametrize("learned", [False, True])
+def test_group_boxes_hold_few_foreign_bodies(nbp, kind, bpl, learned):
+    # A group's walk opens every cell inside its bounding box down to the
+    # bodies, so the box must not cover a dense region.  Runs of sibling
+    # children stay inside one half of their parent when a sibling is large,
+    # which bounds the bodies inside any group's box by 4 group sizes (the
+    # parent of a run without large siblings holds at most 4).  Merged runs
+    # across both halves once put the core of a sparse 65,536-body universe
+    # inside one group's box (a 2-5 ms step instead of 0.3 ms).
+    n = 65536
+    m, p, v = nbp.universes.make(kind, n, 0)
+    cfg = nbp.SimConfig(theta=0.5, epsilon_squared=EPS2, mode=nbp.NB_MODE_SPLIT,
+                        bodies_per_lane=bpl, learned=learned)
+    with nbp.NbContext(cfg, m, p, v) as ctx:
+        if learned:
+            wdir = pathlib.Path(nbp.__file__).resolve().parent / "weights"
+            ctx.set_mlp_weights(np.load(wdir / "correction_theta1.npy"))
+        ctx.accelerations()
+        g = ctx.debug_groups()
+        _, pos, _, _ = ctx.debug_state()
+    gsize = 64 if learned else 32 * bpl      # the learned correction keeps groups of 64
+    assert (g[:, 1] - g[:, 0] + 1).max() <= gsize
+    inside = _bodies_in_group_boxes(pos, g)
+    assert inside.max() <= 4 * gsize, (inside.max(), int((inside > 4 * gsize).sum()))
