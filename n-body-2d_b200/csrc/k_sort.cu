@@ -454,45 +454,54 @@ constexpr uint32_t kFlagPrefix = 2u << 30;
 constexpr uint32_t kCountMask = (1u << 30) - 1;
 constexpr int kSpinLimit = 1 << 22;
 
-// Histograms of all eight digits.  Each thread counts a run of kHistRun
-// consecutive keys and flushes a digit's count to shared memory only when the
-// digit changes: the keys arrive nearly sorted (the bodies keep last step's
-// order), so the high digits change rarely and the low ones hit random bins.
-constexpr int kHistRun = 16;
+// Histograms of the digits the radix passes sort (the top sort_passes bytes;
+// the passes below return at once and need none).  A warp reads rows of 32
+// consecutive keys (one coalesced load) and, per digit, finds the runs of
+// equal digits in the row with one ballot: each run's first lane adds the
+// run's length to the digit's bin.  The keys arrive nearly sorted (the bodies
+// keep last step's order), so the high digits form long runs and most rows
+// cost one shared-memory atomic per digit.
+constexpr int kHistRows = 4;
 
 __global__ void __launch_bounds__(kSortThreads)
 onesweep_histogram(const uint64_t* __restrict__ key0, const uint64_t* __restrict__ key1, int64_t n,
                    const DeviceScalars* __restrict__ s, uint32_t* __restrict__ hist) {
     // the Morton pass wrote the codes where the first radix pass reads them
     const uint64_t* __restrict__ key = (s->sort_passes & 1) ? key1 : key0;
+    const int dmin = 8 - s->sort_passes;  // digits below are not sorted by a pass
     __shared__ uint32_t h[8][256];
     for (int k = threadIdx.x; k < 8 * 256; k += kSortThreads) (&h[0][0])[k] = 0;
     __syncthreads();
-    const int64_t stride = (int64_t)gridDim.x * kSortThreads * kHistRun;
-    for (int64_t first = ((int64_t)blockIdx.x * kSortThreads + threadIdx.x) * kHistRun; first < n;
-         first += stride) {
-        const int cnt = (int)min((int64_t)kHistRun, n - first);
-        uint64_t prev = __ldg(key + first);
-        uint32_t run[8];
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (kSortThreads / 32);
+    const int64_t w = (int64_t)blockIdx.x * (kSortThreads / 32) + (threadIdx.x >> 5);
+    const unsigned after_me = ~((2u << lane) - 1u);  // lanes above this one (none for lane 31)
+    // kHistRows rows per warp and iteration: their loads are in flight together
+    for (int64_t row0 = w * 32 * kHistRows; row0 < n; row0 += warps * 32 * kHistRows) {
+        uint64_t k[kHistRows];
 #pragma unroll
-        for (int d = 0; d < 8; ++d) run[d] = 1;
-        for (int j = 1; j < cnt; ++j) {
-            const uint64_t k = __ldg(key + first + j);
-#pragma unroll
-            for (int d = 0; d < 8; ++d) {
-                const uint32_t a = (uint32_t)(prev >> (8 * d)) & 0xFF;
-                const uint32_t b = (uint32_t)(k >> (8 * d)) & 0xFF;
-                if (a != b) {
-                    atomicAdd(&h[d][a], run[d]);
-                    run[d] = 1;
-                } else {
-                    ++run[d];
-                }
-            }
-            prev = k;
+        for (int r = 0; r < kHistRows; ++r) {
+            const int64_t i = row0 + 32 * r + lane;
+            k[r] = i < n ? __ldg(key + i) : 0ull;
         }
 #pragma unroll
-        for (int d = 0; d < 8; ++d) atomicAdd(&h[d][(uint32_t)(prev >> (8 * d)) & 0xFF], run[d]);
+        for (int r = 0; r < kHistRows; ++r) {
+            const int64_t left = n - (row0 + 32 * r);  // valid lanes of the row are a prefix
+            if (left <= 0) break;
+            const int end = left < 32 ? (int)left : 32;
+            const bool valid = lane < end;
+            const uint64_t kp = __shfl_up_sync(kFull, k[r], 1);
+            const uint64_t diff = k[r] ^ kp;
+#pragma unroll
+            for (int d = 0; d < 8; ++d) {
+                if (d < dmin) continue;
+                const bool head = valid && (lane == 0 || ((diff >> (8 * d)) & 0xFF) != 0);
+                const unsigned later = __ballot_sync(kFull, head) & after_me;
+                if (head)
+                    atomicAdd(&h[d][(uint32_t)(k[r] >> (8 * d)) & 0xFF],
+                              (uint32_t)((later ? __ffs(later) - 1 : end) - lane));
+            }
+        }
     }
     __syncthreads();
     for (int k = threadIdx.x; k < 8 * 256; k += kSortThreads) {
@@ -973,7 +982,7 @@ void launch_sort(nb_ctx* c) {
     cudaMemsetAsync(c->sort.hist, 0, sizeof(uint32_t) * 8 * 256, c->stream);
     cudaMemsetAsync(c->sort.status, 0, sizeof(uint32_t) * 8 * 256 * (size_t)tiles, c->stream);
     cudaMemsetAsync(c->sort.tile_counter, 0, sizeof(unsigned) * 8, c->stream);
-    onesweep_histogram<<<2 * c->sm_count, kSortThreads, 0, c->stream>>>(
+    onesweep_histogram<<<4 * c->sm_count, kSortThreads, 0, c->stream>>>(
         c->sort.key[0], c->sort.key[1], c->n, c->scal, c->sort.hist);
     onesweep_bins<<<8, kSortThreads, 0, c->stream>>>(c->sort.hist);
     for (int pass = 0; pass < 8; ++pass) {

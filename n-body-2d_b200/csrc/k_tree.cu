@@ -84,32 +84,263 @@ __device__ int gallop_right(const uint64_t* __restrict__ key, int i, int hi, int
     return a;
 }
 
-// Pass 1: flag the boundaries that create a cell.  It also counts, for the
-// next step's sort, how many neighbouring codes share d leading digits
-// (choose_sort_passes reads the histogram).
-__global__ void tree_mark(const uint64_t* __restrict__ key, int n, int32_t* __restrict__ flag,
-                          int32_t* __restrict__ start_of, unsigned* __restrict__ lcp_hist) {
+// ---- cell structure from the boundary levels ---------------------------
+// Boundary i lies between bodies i and i + 1; its level c_i is the number of
+// leading digits codes i and i + 1 share (capped at kMaxLevel: codes sharing
+// 30 or more digits sit in one leaf).  The cell whose children boundary i
+// separates spans the bodies between the nearest boundaries on either side
+// with a smaller level, and the boundaries of equal level between those are
+// its other child separators.  So the whole build reduces to nearest smaller
+// values over c (ANSV), which three passes find without a search:
+//   tree_lcp         c_i per boundary, and per tile and level v the first
+//                    and last boundary with a level below v;
+//   tree_ansv_tiles  those tables scanned over the tiles (prefix maximum of
+//                    the last, suffix minimum of the first);
+//   tree_ansv        per boundary the nearest smaller (and smaller-or-equal)
+//                    level on each side: inside its warp row from the row's
+//                    ballot for that level, inside its tile from the rows'
+//                    summaries, beyond the tile from the scanned tables.
+// A tile is kAnsvTile boundaries; warp w holds rows 8w..8w+7 of 32.  Lane v
+// of a row needs the row's mask "level < v": each lane writes its level as a
+// thermometer word (bit v set for every v above its level) and a 32 x 32 bit
+// transpose across the warp (five butterfly shuffles) hands lane v bit v of
+// every lane, which is that mask.
+constexpr int kAnsvItems = kAnsvTile / kThreads;  // rows per warp
+constexpr int kAnsvRows = kAnsvTile / 32;           // 64 rows
+constexpr int kNoLevel = kMaxLevel + 1;             // past the last body: never below a level
+static_assert(kAnsvItems == 8 && kAnsvLevels == 32, "one lane per level, 8 rows per warp");
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// Lane v receives bit v of every lane's word x (bit l from lane l): the 32 x
+// 32 bit matrix of the warp's words transposed by swapping off-diagonal
+// blocks of 16, 8, 4, 2 and 1 between lane pairs.
+__device__ __forceinline__ unsigned warp_transpose_bits(unsigned x) {
+    const int lane = threadIdx.x & 31;
+    constexpr unsigned keep[5] = {0x0000FFFFu, 0x00FF00FFu, 0x0F0F0F0Fu, 0x33333333u, 0x55555555u};
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        const int j = 16 >> k;
+        const unsigned p = __shfl_xor_sync(kFull, x, j);
+        x = (lane & j) ? (x & ~keep[k]) | ((p >> j) & keep[k])
+                       : (x & keep[k]) | ((p << j) & ~keep[k]);
+    }
+    return x;
+}
+
+// Bit v set for every v above level c (v = 0..31).
+__device__ __forceinline__ unsigned thermometer(int c) {
+    return c >= 31 ? 0u : (0xFFFFFFFFu << (c + 1));
+}
+
+// Tables are level-major: tab[v * tiles + t].
+__global__ void __launch_bounds__(kThreads)
+tree_lcp(const uint64_t* __restrict__ key, int n, int tiles, uint8_t* __restrict__ lcp8,
+         int32_t* __restrict__ tile_first, int32_t* __restrict__ tile_last,
+         unsigned* __restrict__ lcp_hist) {
     __shared__ unsigned hist[33];
+    __shared__ int sfirst[kAnsvLevels], slast[kAnsvLevels];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (threadIdx.x < 33) hist[threadIdx.x] = 0;
-    __syncthreads();
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) {
-        int f = 0, s = 0;
-        if (i < n - 1) {
-            const uint64_t ki = key[i];
-            const int c = lcp_digits(ki, key[i + 1]);
-            atomicAdd(&hist[c], 1u);
-            if (c < kMaxLevel) {
-                s = c == 0 ? 0 : gallop_left(key, 0, i, c);
-                // i opens the cell iff bodies s..i all sit in its first child.
-                f = share(key[s], ki, c + 1) ? 1 : 0;
-            }
-        }
-        flag[i] = f;
-        start_of[i] = s;
+    if (threadIdx.x < kAnsvLevels) {
+        sfirst[threadIdx.x] = INT_MAX;
+        slast[threadIdx.x] = -1;
     }
     __syncthreads();
+    const int base = blockIdx.x * kAnsvTile + warp * (32 * kAnsvItems);
+    // lane v (1..30): first and last boundary of the warp's rows with level < v;
+    // lane v (1..31) and lane 0 (for 32): how many have a level < v
+    int myfirst = INT_MAX, mylast = -1;
+    unsigned mycnt = 0, nbound = 0;
+#pragma unroll 1
+    for (int r = 0; r < kAnsvItems; ++r) {
+        const int row0 = base + 32 * r;
+        const int i = row0 + lane;
+        int c = 64;  // not a boundary
+        if (i < n - 1) c = lcp_digits(key[i], key[i + 1]);
+        if (i < n) lcp8[i] = (uint8_t)(i < n - 1 ? min(c, kMaxLevel) : kNoLevel);
+        // lane v (1..31): the row's mask of levels below v; lane 0: below 32
+        unsigned mine = warp_transpose_bits(thermometer(c));
+        const unsigned below32 = __ballot_sync(kFull, c < 32);
+        if (lane == 0) mine = below32;
+        nbound += __popc(__ballot_sync(kFull, i < n - 1));
+        mycnt += __popc(mine);
+        if (mine && lane >= 1 && lane <= kMaxLevel) {
+            if (myfirst == INT_MAX) myfirst = row0 + __ffs(mine) - 1;
+            mylast = row0 + 31 - __clz(mine);
+        }
+    }
+    if (myfirst != INT_MAX) atomicMin(&sfirst[lane], myfirst);
+    if (mylast >= 0) atomicMax(&slast[lane], mylast);
+    {   // histogram of levels 0..32 from the counts below each level
+        const unsigned c32 = __shfl_sync(kFull, mycnt, 0);
+        const unsigned x = lane == 0 ? 0u : mycnt;         // count below level `lane`
+        const unsigned up = __shfl_down_sync(kFull, x, 1);  // count below level lane + 1
+        const unsigned h = lane < 31 ? up - x : c32 - x;
+        if (h) atomicAdd(&hist[lane], h);
+        if (lane == 0 && nbound > c32) atomicAdd(&hist[32], nbound - c32);
+    }
+    __syncthreads();
+    if (threadIdx.x < kAnsvLevels) {
+        tile_first[threadIdx.x * tiles + blockIdx.x] = sfirst[threadIdx.x];
+        tile_last[threadIdx.x * tiles + blockIdx.x] = slast[threadIdx.x];
+    }
+    // the next step's sort reads how many neighbouring codes share d digits
     if (threadIdx.x < 33 && hist[threadIdx.x]) atomicAdd(lcp_hist + threadIdx.x, hist[threadIdx.x]);
+}
+
+// One block per level v: tile_last becomes the last boundary of tiles 0..t
+// with a level below v, tile_first the first of tiles t..tiles-1.
+constexpr int kTileScanThreads = 1024;
+__global__ void __launch_bounds__(kTileScanThreads)
+tree_ansv_tiles(int tiles, int32_t* __restrict__ tile_first, int32_t* __restrict__ tile_last) {
+    __shared__ int wagg[kTileScanThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int32_t* last = tile_last + blockIdx.x * tiles;
+    int32_t* first = tile_first + blockIdx.x * tiles;
+    int carry = -1;
+    for (int b = 0; b < tiles; b += kTileScanThreads) {
+        const int t = b + threadIdx.x;
+        int x = t < tiles ? last[t] : -1;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(kFull, x, o);
+            if (lane >= o) x = max(x, y);
+        }
+        if (lane == 31) wagg[warp] = x;
+        __syncthreads();
+        int pre = carry, tot = carry;
+        for (int w = 0; w < kTileScanThreads / 32; ++w) {
+            if (w < warp) pre = max(pre, wagg[w]);
+            tot = max(tot, wagg[w]);
+        }
+        if (t < tiles) last[t] = max(x, pre);
+        carry = tot;
+        __syncthreads();
+    }
+    carry = INT_MAX;
+    for (int b = tiles - 1; b >= 0; b -= kTileScanThreads) {
+        const int t = b - (int)threadIdx.x;  // descending: a prefix over the threads is a suffix over tiles
+        int x = t >= 0 ? first[t] : INT_MAX;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(kFull, x, o);
+            if (lane >= o) x = min(x, y);
+        }
+        if (lane == 31) wagg[warp] = x;
+        __syncthreads();
+        int pre = carry, tot = carry;
+        for (int w = 0; w < kTileScanThreads / 32; ++w) {
+            if (w < warp) pre = min(pre, wagg[w]);
+            tot = min(tot, wagg[w]);
+        }
+        if (t >= 0) first[t] = min(x, pre);
+        carry = tot;
+        __syncthreads();
+    }
+}
+
+// Per boundary i below kMaxLevel: flag = 1 iff i is its cell's first
+// separator (no equal level between it and the cell's start), which numbers
+// the cells; bnd[i] = {first body of the cell, last body of the cell,
+// previous separator of the cell or -1, next separator or -1}, the first two
+// written for flagged boundaries only.  The cell's first body follows the
+// nearest smaller level on the left, its last body is the nearest smaller on
+// the right (or n - 1); a separator's neighbours are the nearest levels <= c_i
+// when those equal c_i.
+__global__ void __launch_bounds__(kThreads)
+tree_ansv(const uint8_t* __restrict__ lcp8, int n, int tiles,
+          const int32_t* __restrict__ tile_first, const int32_t* __restrict__ tile_last,
+          int32_t* __restrict__ flag, int4* __restrict__ bnd) {
+    // masks[r][v]: row r's ballot of "level < v" (v = 1..30; 0 elsewhere).
+    // rlast[r][v]: after the scan, the last boundary with a level below v in
+    // rows 8p..r of r's part p (-1 if none), rfirst[r][v] the first in rows
+    // r..8p+7 (kAnsvTile if none); tile-local positions
+    __shared__ unsigned masks[kAnsvRows][32];
+    __shared__ int16_t rlast[kAnsvRows][kAnsvLevels];
+    __shared__ int16_t rfirst[kAnsvRows][kAnsvLevels];
+    __shared__ int16_t before[kThreads / 32][kAnsvLevels];  // last in the parts before p
+    __shared__ int16_t after[kThreads / 32][kAnsvLevels];   // first in the parts after p
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int tile = blockIdx.x, tbase = tile * kAnsvTile;
+#pragma unroll 1
+    for (int r = 0; r < kAnsvItems; ++r) {
+        const int row = warp * kAnsvItems + r;
+        const int i = tbase + 32 * row + lane;
+        const int cap = i < n ? lcp8[i] : kNoLevel;
+        // lane v: the row's mask of levels below v (lanes 0 and 31 unused: 0)
+        unsigned mine = warp_transpose_bits(thermometer(cap));
+        if (lane == 0 || lane > kMaxLevel) mine = 0u;
+        masks[row][lane] = mine;
+        rfirst[row][lane] = (int16_t)(mine ? 32 * row + __ffs(mine) - 1 : kAnsvTile);
+        rlast[row][lane] = (int16_t)(mine ? 32 * row + 31 - __clz(mine) : -1);
+    }
+    __syncwarp();
+    {   // scan the warp's own 8 rows, lane = level
+        int run = -1;
+        for (int r = 0; r < kAnsvItems; ++r) {
+            const int row = warp * kAnsvItems + r;
+            run = max(run, (int)rlast[row][lane]);
+            rlast[row][lane] = (int16_t)run;
+        }
+        int runf = kAnsvTile;
+        for (int r = kAnsvItems - 1; r >= 0; --r) {
+            const int row = warp * kAnsvItems + r;
+            runf = min(runf, (int)rfirst[row][lane]);
+            rfirst[row][lane] = (int16_t)runf;
+        }
+    }
+    __syncthreads();
+    {
+        int b = -1, a = kAnsvTile;
+        for (int p = 0; p < kThreads / 32; ++p) {
+            if (p < warp) b = max(b, (int)rlast[p * kAnsvItems + kAnsvItems - 1][lane]);
+            if (p > warp) a = min(a, (int)rfirst[p * kAnsvItems][lane]);
+        }
+        before[warp][lane] = (int16_t)b;
+        after[warp][lane] = (int16_t)a;
+    }
+    __syncthreads();
+    const unsigned lt = lanemask_lt(), gt = ~lt & ~(1u << lane);
+#pragma unroll 1
+    for (int r = 0; r < kAnsvItems; ++r) {
+        const int row = warp * kAnsvItems + r;
+        const int i = tbase + 32 * row + lane;
+        if (i >= n) continue;
+        const int v = lcp8[i];
+        if (i == n - 1 || v >= kMaxLevel) {
+            flag[i] = 0;
+            continue;
+        }
+        // nearest boundary on the left / right with a level below u
+        auto left = [&](int u) {
+            const unsigned m = masks[row][u] & lt;
+            if (m) return tbase + 32 * row + 31 - __clz(m);
+            int j = r > 0 ? (int)rlast[row - 1][u] : -1;
+            if (j < 0) j = before[warp][u];
+            if (j >= 0) return tbase + j;
+            return tile > 0 ? tile_last[u * tiles + tile - 1] : -1;
+        };
+        auto right = [&](int u) {
+            const unsigned m = masks[row][u] & gt;
+            if (m) return tbase + 32 * row + __ffs(m) - 1;
+            int j = r < kAnsvItems - 1 ? (int)rfirst[row + 1][u] : kAnsvTile;
+            if (j >= kAnsvTile) j = after[warp][u];
+            if (j < kAnsvTile) return tbase + j;
+            const int g = tile + 1 < tiles ? tile_first[u * tiles + tile + 1] : INT_MAX;
+            return g == INT_MAX ? n - 1 : g;
+        };
+        const int l_lt = left(v), l_le = left(v + 1);
+        const int r_lt = right(v), r_le = right(v + 1);
+        const bool first_sep = l_le == l_lt;
+        flag[i] = first_sep ? 1 : 0;
+        bnd[i] = make_int4(first_sep ? l_lt + 1 : -1, first_sep ? r_lt : -1,
+                           first_sep ? -1 : l_le, r_le == r_lt ? -1 : r_le);
+    }
 }
 
 // ---- exclusive scan of flag[] -> cell_of[], total -> scal->cells ----------
@@ -241,87 +472,53 @@ __device__ void bucket_moments(const double2* __restrict__ pos, const double* __
     *out_c = make_double2(sx[7] / sm[7], sy[7] / sm[7]);
 }
 
-// Pass 3: every flagged boundary writes its cell, its children and their
-// parent links.
-__global__ void tree_link(const uint64_t* __restrict__ key, int n,
-                          const double2* __restrict__ pos, const double* __restrict__ mass,
+// Every cell (one thread each) writes its own record and its leaf children,
+// and enters itself in its parent's child list: the parent is the cell of the
+// deeper of the two boundaries around this cell's bodies (their levels are
+// below the cell's; ties are two separators of the same parent), and the
+// slot is the child's position among the parent's children in code order.
+__global__ void tree_link(const uint64_t* __restrict__ key, const uint8_t* __restrict__ lcp8,
+                          int n, const double2* __restrict__ pos, const double* __restrict__ mass,
                           Tree t, DeviceScalars* __restrict__ s) {
-    // one thread per cell; the block's 256 consecutive cells are re-dealt by
-    // level (a counting sort in shared memory), so a warp's lanes build cells
-    // of similar size while the block keeps to one stretch of the codes
-    __shared__ int lvl_cnt[32];
-    __shared__ int dealt[kThreads];
+    const int id = blockIdx.x * blockDim.x + threadIdx.x;
     const int cells = s->cells;
-    const int id0 = blockIdx.x * blockDim.x + threadIdx.x;
-    if (threadIdx.x < 32) lvl_cnt[threadIdx.x] = 0;
-    __syncthreads();
-    int c0 = 31;  // past every level: empty slots go last
-    if (id0 < cells) {
-        const int i0 = t.rep_of[id0];
-        c0 = lcp_digits(key[i0], key[i0 + 1]);
-    }
-    const int rank = atomicAdd(&lvl_cnt[c0], 1);
-    __syncthreads();
-    if (threadIdx.x < 32) {
-        const int v = lvl_cnt[threadIdx.x];
-        int inc = v;
-        for (int o = 1; o < 32; o <<= 1) {
-            const int u = __shfl_up_sync(kFull, inc, o);
-            if ((int)threadIdx.x >= o) inc += u;
-        }
-        lvl_cnt[threadIdx.x] = inc - v;
-    }
-    __syncthreads();
-    dealt[lvl_cnt[c0] + rank] = id0;
-    __syncthreads();
-    const int id = dealt[threadIdx.x];
     if (id >= cells) return;
     const int i = t.rep_of[id];
-    const int c = lcp_digits(key[i], key[i + 1]);
-    const int first = t.start_of[i];
-    const int last = c == 0 ? n - 1 : gallop_right(key, i + 1, n - 1, c);
-    int cs[4], ce[4];
-    int nc = 1;
-    cs[0] = first;
-    ce[0] = i;
-    int p = i + 1;
-    while (p <= last && nc < 4) {
-        const int e = gallop_right(key, p, last, c + 1);
-        cs[nc] = p;
-        ce[nc] = e;
-        ++nc;
-        p = e + 1;
+    const int4 bi = t.bnd[i];
+    const int c = lcp8[i];
+    const int first = bi.x, last = bi.y;
+    // the cell's separators: i, then the chain of next separators
+    int sep[3] = {i, n - 1, n - 1};
+    int ns = 1;
+    for (int j = bi.w; j >= 0; j = t.bnd[j].w) {
+        if (ns == 3) {  // a fifth child: the codes are inconsistent
+            atomicOr(&s->error, kErrTree);
+            break;
+        }
+        sep[ns++] = j;
     }
-    if (p <= last) atomicOr(&s->error, kErrTree);
-    int ref[4] = {INT_MIN, INT_MIN, INT_MIN, INT_MIN};
+    int* child = reinterpret_cast<int*>(t.child + id);
     int nint = 0;
-    for (int q = 0; q < nc; ++q) {
-        const int a = cs[q], b = ce[q];
+    for (int q = 0; q <= ns; ++q) {
+        const int a = q == 0 ? first : sep[q - 1] + 1;
+        const int b = q == ns ? last : sep[q];
         if (a == b) {
-            ref[q] = ~a;
+            child[q] = ~a;
             t.leaf_last[a] = a;
             t.leaf_plevel[a] = c;
-            continue;
-        }
-        const int c2 = lcp_digits(key[a], key[b]);
-        if (c2 >= kMaxLevel) {
-            ref[q] = ~a;
+        } else if (lcp8[a] == kMaxLevel && lcp_digits(key[a], key[b]) >= kMaxLevel) {
+            // (a boundary below level 30 right after a makes the child a cell)
+            child[q] = ~a;
             t.leaf_last[a] = b;
             t.leaf_plevel[a] = c;
             bucket_moments(pos, mass, a, b, t.bucket_mass + a, t.bucket_com + a);
-            continue;
+        } else {
+            ++nint;  // a cell: it enters itself below
         }
-        const int rep = gallop_right(key, a, b, c2 + 1);
-        const int cid = t.cell_of[rep];
-        ref[q] = cid;
-        t.parent[cid] = id;
-        ++nint;
     }
-    t.first[id] = first;
-    t.last[id] = last;
+    for (int q = ns + 1; q < 4; ++q) child[q] = INT_MIN;
     t.range[id] = make_int2(first, last);
     t.level[id] = c;
-    t.child[id] = make_int4(ref[0], ref[1], ref[2], ref[3]);
     t.nint[id] = nint;
     t.ready[id] = 0;
     // cells whose children are all leaves start the bottom-up climb: listed
@@ -339,7 +536,25 @@ __global__ void tree_link(const uint64_t* __restrict__ key, int n,
     if (first == 0 && last == n - 1) {
         s->root = id;
         t.parent[id] = -1;
+        return;
     }
+    const int cl = first > 0 ? lcp8[first - 1] : -1;
+    const int cr = last < n - 1 ? lcp8[last] : -1;
+    const bool from_left = cl >= cr;
+    int k = from_left ? first - 1 : last;  // a separator of the parent
+    int rank = 0;  // its rank among the parent's separators; k ends at the first
+    for (int p = t.bnd[k].z; p >= 0 && rank < 3; p = t.bnd[k].z) {
+        k = p;
+        ++rank;
+    }
+    const int slot = from_left ? rank + 1 : rank;
+    if (slot > 3) {  // more than four children: the codes are inconsistent
+        atomicOr(&s->error, kErrTree);
+        return;
+    }
+    const int pid = t.cell_of[k];
+    reinterpret_cast<int*>(t.child + pid)[slot] = id;
+    t.parent[id] = pid;
 }
 
 // A tree without internal cells: one body, or all bodies in one level-30 leaf.
@@ -994,19 +1209,24 @@ void launch_groups(nb_ctx* c) {
 void launch_tree(nb_ctx* c, const BodyBuffers& b) {
     const int n = (int)c->n;
     const uint64_t* key = c->sort.key[0];
-    c->launches += 6;
-    tree_mark<<<blocks_for(n, kThreads), kThreads, 0, c->stream>>>(key, n, c->tree.flag,
-                                                                    c->tree.start_of,
-                                                                    c->scal->lcp_hist);
+    Tree& t = c->tree;
+    const int tiles = (int)blocks_for(n, kAnsvTile);
+    c->launches += 8;
+    tree_lcp<<<tiles, kThreads, 0, c->stream>>>(key, n, tiles, t.lcp8, t.ansv_first, t.ansv_last,
+                                                c->scal->lcp_hist);
+    tree_ansv_tiles<<<kAnsvLevels, kTileScanThreads, 0, c->stream>>>(tiles, t.ansv_first,
+                                                                     t.ansv_last);
+    tree_ansv<<<tiles, kThreads, 0, c->stream>>>(t.lcp8, n, tiles, t.ansv_first, t.ansv_last,
+                                                 t.flag, t.bnd);
     const int sblocks = (int)blocks_for(n, kScanTile);
-    scan_reduce<<<sblocks, kThreads, 0, c->stream>>>(c->tree.flag, n, c->scan.block_sums);
+    scan_reduce<<<sblocks, kThreads, 0, c->stream>>>(t.flag, n, c->scan.block_sums);
     scan_block_sums<<<1, kThreads, 0, c->stream>>>(c->scan.block_sums, sblocks, &c->scal->cells);
-    scan_apply<<<sblocks, kThreads, 0, c->stream>>>(c->tree.flag, n, c->scan.block_sums,
-                                                     c->tree.cell_of, c->tree.rep_of);
+    scan_apply<<<sblocks, kThreads, 0, c->stream>>>(t.flag, n, c->scan.block_sums, t.cell_of,
+                                                     t.rep_of);
     cudaMemsetAsync(&c->scal->nstart, 0, sizeof(int32_t), c->stream);
-    tree_link<<<blocks_for(n, kThreads), kThreads, 0, c->stream>>>(key, n, b.pos, b.mass, c->tree,
+    tree_link<<<blocks_for(n, kThreads), kThreads, 0, c->stream>>>(key, t.lcp8, n, b.pos, b.mass, t,
                                                                     c->scal);
-    tree_trivial_root<<<1, 1, 0, c->stream>>>(b.pos, b.mass, n, c->tree, c->scal);
+    tree_trivial_root<<<1, 1, 0, c->stream>>>(b.pos, b.mass, n, t, c->scal);
 }
 
 void launch_features(nb_ctx* c, const BodyBuffers& b) {

@@ -82,8 +82,6 @@ int alloc_all(nb_ctx* c) {
     c->scan.blocks = (int)((n + 2047) / 2048);
     NB_CUDA(c, dalloc(&c->scan.block_sums, (size_t)c->scan.blocks));
     nb::Tree& t = c->tree;
-    NB_CUDA(c, dalloc(&t.first, n));
-    NB_CUDA(c, dalloc(&t.last, n));
     NB_CUDA(c, dalloc(&t.level, n));
     NB_CUDA(c, dalloc(&t.child, n));
     NB_CUDA(c, dalloc(&t.parent, n));
@@ -123,7 +121,13 @@ int alloc_all(nb_ctx* c) {
     NB_CUDA(c, dalloc(&t.flag, n));
     NB_CUDA(c, dalloc(&t.cell_of, n));
     NB_CUDA(c, dalloc(&t.rep_of, n));
-    NB_CUDA(c, dalloc(&t.start_of, n));
+    NB_CUDA(c, dalloc(&t.bnd, n));
+    NB_CUDA(c, dalloc(&t.lcp8, n));
+    {
+        const size_t tiles = (n + nb::kAnsvTile - 1) / nb::kAnsvTile;
+        NB_CUDA(c, dalloc(&t.ansv_first, tiles * nb::kAnsvLevels));
+        NB_CUDA(c, dalloc(&t.ansv_last, tiles * nb::kAnsvLevels));
+    }
     NB_CUDA(c, dalloc(&c->scal, 1));
     NB_CUDA(c, cudaMemset(c->scal, 0, sizeof(nb::DeviceScalars)));
     c->bbox_blocks = 2 * c->sm_count;
@@ -152,13 +156,14 @@ void free_all(nb_ctx* c) {
     cudaFree(c->sort.ties_big);
     cudaFree(c->scan.block_sums);
     nb::Tree& t = c->tree;
-    void* tree_ptrs[] = {t.first,     t.last,        t.level,       t.child,      t.parent,
+    void* tree_ptrs[] = {t.level,       t.child,      t.parent,
                          t.nint,      t.ready,       t.mass,        t.com,        t.leaf_last,
                          t.leaf_plevel, t.bucket_mass, t.bucket_com, t.flag,      t.cell_of,
-                         t.start_of,  t.range,       t.s64,         t.cell4,      t.cellq,      t.s32,
+                         t.bnd,       t.range,       t.s64,         t.cell4,      t.cellq,      t.s32,
                          t.body4,     t.gcount,      t.gbase,       t.groups,     t.rep_of,
                          t.t32,       t.cellh,       t.band,        t.band_count,
-                         t.start_list, t.prefix, t.prefix_tiles};
+                         t.start_list, t.prefix, t.prefix_tiles, t.lcp8, t.ansv_first,
+                         t.ansv_last};
     for (void* q : tree_ptrs) cudaFree(q);
     cudaFree(c->scal);
     cudaFree(c->bbox_partials);
@@ -824,8 +829,12 @@ int nb_debug_tree(nb_ctx* c, double* cell_mass, double* cell_com_xy, int32_t* le
     if (cell_mass && m) NB_CUDA(c, cudaMemcpy(cell_mass, t.mass, m * 8, cudaMemcpyDeviceToHost));
     if (cell_com_xy && m) NB_CUDA(c, cudaMemcpy(cell_com_xy, t.com, m * 16, cudaMemcpyDeviceToHost));
     if (level && m) NB_CUDA(c, cudaMemcpy(level, t.level, m * 4, cudaMemcpyDeviceToHost));
-    if (first_body && m) NB_CUDA(c, cudaMemcpy(first_body, t.first, m * 4, cudaMemcpyDeviceToHost));
-    if (last_body && m) NB_CUDA(c, cudaMemcpy(last_body, t.last, m * 4, cudaMemcpyDeviceToHost));
+    // the body ranges are {first, last} pairs: copy each half with a pitch of 8 bytes
+    if (first_body && m)
+        NB_CUDA(c, cudaMemcpy2D(first_body, 4, t.range, 8, 4, m, cudaMemcpyDeviceToHost));
+    if (last_body && m)
+        NB_CUDA(c, cudaMemcpy2D(last_body, 4, reinterpret_cast<const char*>(t.range) + 4, 8, 4, m,
+                                cudaMemcpyDeviceToHost));
     if (root_ref) *root_ref = s.root;
     return NB_OK;
 }

@@ -17,6 +17,8 @@ constexpr int kStackDepth = 96;   // >= 1 + 3 * 30 pending cells of a DFS
 constexpr int kSortTileItems = 12; // keys per thread in a radix tile
 constexpr int kSortThreads = 256;
 constexpr int kSortTile = kSortTileItems * kSortThreads;  // 3072 keys
+constexpr int kAnsvTile = 2048;   // boundaries per tile of the tree build's level scans
+constexpr int kAnsvLevels = 32;   // table width per tile: levels 0..30 and one spare
 constexpr int kPhases = 8;        // morton, sort, gather, tree, moments, groups, force, drift
 constexpr float kThetaBand = 0.5f; // learned mode: the default plain walk the MLP stands in for
 constexpr int kBandPerBody = 16;   // learned mode: band-list capacity per body of a group
@@ -86,8 +88,6 @@ struct BodyBuffers {
 
 // Compressed quadtree, one entry per internal cell (capacity n).
 struct Tree {
-    int32_t* first = nullptr;    // first body of the cell
-    int32_t* last = nullptr;     // last body of the cell
     int32_t* level = nullptr;    // depth in the reference's uncompressed tree
     int4* child = nullptr;       // child refs: >= 0 cell, < 0 leaf ~first_body, INT_MIN none
     int32_t* parent = nullptr;   // parent cell, -1 at the root
@@ -131,10 +131,15 @@ struct Tree {
     double* bucket_mass = nullptr;  // moments of multi-body leaves
     double2* bucket_com = nullptr;
     // build scratch (per boundary i between bodies i and i+1)
+    uint8_t* lcp8 = nullptr;        // level of boundary i: shared leading digits, capped at 30
     int32_t* flag = nullptr;
     int32_t* cell_of = nullptr;     // exclusive scan of flag
     int32_t* rep_of = nullptr;      // cell id -> the boundary that creates it
-    int32_t* start_of = nullptr;    // first body of the cell owning boundary i
+    int4* bnd = nullptr;            // per boundary: {first body, last body} of the cell it
+                                    // creates (flagged boundaries only), {previous, next}
+                                    // separator of its cell or -1
+    int32_t* ansv_first = nullptr;  // [kAnsvLevels][tiles] per level v and tile: first /
+    int32_t* ansv_last = nullptr;   //   last boundary with a level below v (then scanned)
 };
 
 struct SortBuffers {
