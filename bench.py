@@ -325,7 +325,36 @@ def gpu_baseline(nb, device: int) -> dict:
     if "value" in ref:
         rec["ratio_fp64_vs_reference"] = fp64["value"] / ref["value"]
         rec["ratio_split_vs_reference"] = split["value"] / ref["value"]
+    # the reference's own step ends with a download of every body (CU:632-646):
+    # both sides again with that copy in every step, on the host clock
+    ref_dl = _ref_gpu_record(_ref_gpu_timed(m, p, v, 0.5, 5, download=True), 262144)
+    dl = {"reference": ref_dl,
+          "ours_fp64": _stepped_with_download(nb, mk(nb.NB_MODE_FP64), m, p, v, 3, 20),
+          "ours_split": _stepped_with_download(nb, mk(nb.NB_MODE_SPLIT), m, p, v, 3, 20)}
+    if "value" in ref_dl:
+        dl["ratio_fp64_vs_reference"] = dl["ours_fp64"]["value"] / ref_dl["value"]
+        dl["ratio_split_vs_reference"] = dl["ours_split"]["value"] / ref_dl["value"]
+    rec["with_download_every_step"] = dl
     return rec
+
+
+def _stepped_with_download(nb, cfg, m, p, v, warmup: int, steps: int) -> dict:
+    """Steps of one context each followed by nb_download of every body into
+    host arrays (the reference's per-step copy), host clock over K steps."""
+    hp, hv = np.empty((m.shape[0], 2)), np.empty((m.shape[0], 2))
+    with nb.NbContext(cfg, m, p, v) as ctx:
+        # the download is stream-ordered after the step and waits for its copies
+        for _ in range(warmup):
+            ctx.step(1, sync=False)
+            ctx.download(hp, hv)
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            ctx.step(1, sync=False)
+            ctx.download(hp, hv)
+        dt = (time.perf_counter() - t0) / steps
+    return {"value": m.shape[0] / dt, "unit": "body-steps/s", "ms_per_step": dt * 1e3,
+            "how": "nb_step(1) then nb_download of all positions and velocities into host "
+                   "arrays, each step; host clock"}
 
 
 def run_reference(args) -> None:
@@ -387,12 +416,12 @@ GRID_CASE = ("jittered grid, 512 x 512 = 262,144 bodies, seed 0, theta 0.5: the 
              "replay finds at most 28 of the reference kernel's 32 traversal-stack entries in use")
 
 
-def _ref_gpu_timed(m, p, v, theta: float, steps: int) -> dict:
+def _ref_gpu_timed(m, p, v, theta: float, steps: int, download: bool = False) -> dict:
     """refgpu.time_steps, with any failure of the harness reported, not raised."""
     from oracle import refgpu
 
     try:
-        return refgpu.time_steps(m, p, v, theta=theta, steps=steps)
+        return refgpu.time_steps(m, p, v, theta=theta, steps=steps, download=download)
     except Exception as e:  # the record says why; the arm's own line still prints
         return {"unavailable": f"reference GPU harness failed: {type(e).__name__}: {e}"[:300]}
 

@@ -160,6 +160,10 @@ int main(int argc, char** argv) {
     if (std::fread(hdr, 8, 4, in) != 4 || std::fread(par, 8, 4, in) != 4) return 4;
     const int32_t n = (int32_t)hdr[0];
     const int64_t steps = hdr[1];
+    // header word 2, bit 0: end every step as BarnesHutCuda::simulate does,
+    // with the scatter to original order and the download of positions and
+    // velocities into host memory (CU:498-506, 632-646)
+    const bool download = (hdr[2] & 1) != 0;
     const double theta = par[0], eps2 = par[1], dt = par[2], G = par[3];
     std::vector<double> m(n), p(2 * n), v(2 * n);
     if (std::fread(m.data(), 8, n, in) != (size_t)n || std::fread(p.data(), 8, 2 * n, in) != (size_t)(2 * n) ||
@@ -224,6 +228,12 @@ int main(int argc, char** argv) {
         }
         force(s, s.vel, eps2, G * dt, theta * theta);
         Kernel::update_positions<<<(n + BLOCK_SIZE - 1) / BLOCK_SIZE, BLOCK_SIZE>>>(s.pos, s.vel, n, dt);
+        if (download) {
+            Kernel::scatter_to_original_order<<<(n + BLOCK_SIZE - 1) / BLOCK_SIZE, BLOCK_SIZE>>>(
+                s.pos, s.vel, s.idx, s.pos_alt, s.vel_alt, n);
+            CUDA_CHECK(cudaMemcpy(p.data(), s.pos_alt, 16 * n, cudaMemcpyDeviceToHost));
+            CUDA_CHECK(cudaMemcpy(v.data(), s.vel_alt, 16 * n, cudaMemcpyDeviceToHost));
+        }
         CUDA_CHECK(cudaDeviceSynchronize());
     }
     const double timed = steps > 1 ? std::chrono::duration<double>(

@@ -3,9 +3,10 @@
 oracle/_ref/ref_gpu_harness runs src/Simulation/src/BarnesHutCuda.cu's kernels
 unmodified under its own host driver (see oracle/ref/ref_gpu_harness.cu) and
 reports the host-clock time per step of steps 1.., which is the reference's
-step cost: its driver synchronises with the host at every tree level.  The
-per-step download of all bodies that BarnesHutCuda::simulate adds is not
-included.  The reference kernel keeps a 32-entry traversal stack (CU:400), so
+step cost: its driver synchronises with the host at every tree level.  With
+download=True every step also ends as BarnesHutCuda::simulate's does, with the
+scatter to original order and the copy of all positions and velocities to the
+host (CU:498-506, 632-646); without it that per-step download is left out.  The reference kernel keeps a 32-entry traversal stack (CU:400), so
 a case runs only after the CPU oracle has replayed every step and found at
 most 28 entries in use; deeper cases are refused, not run.
 """
@@ -38,7 +39,8 @@ def max_stack(mass, pos, vel, *, theta, steps, eps2, dt, G) -> int:
     return worst
 
 
-def time_steps(mass, pos, vel, *, theta, steps, eps2=1e-4, dt=1e-4, G=1.0) -> dict:
+def time_steps(mass, pos, vel, *, theta, steps, eps2=1e-4, dt=1e-4, G=1.0,
+               download: bool = False) -> dict:
     """Seconds per step of the reference GPU path over `steps` timed steps
     (one more, untimed, runs first), or the reason it was not run."""
     if not available():
@@ -50,7 +52,7 @@ def time_steps(mass, pos, vel, *, theta, steps, eps2=1e-4, dt=1e-4, G=1.0) -> di
     with tempfile.TemporaryDirectory() as td:
         fin, fout = pathlib.Path(td) / "in.bin", pathlib.Path(td) / "out.bin"
         with open(fin, "wb") as f:
-            np.array([n, steps + 1, 0, 0], dtype=np.int64).tofile(f)
+            np.array([n, steps + 1, 1 if download else 0, 0], dtype=np.int64).tofile(f)
             np.array([theta, eps2, dt, G], dtype=np.float64).tofile(f)
             for a in (mass, pos, vel):
                 np.ascontiguousarray(a, dtype=np.float64).tofile(f)
