@@ -458,11 +458,24 @@ __device__ void bucket_moments(const double2* __restrict__ pos, const double* __
 // deeper of the two boundaries around this cell's bodies (their levels are
 // below the cell's; ties are two separators of the same parent), and the
 // slot is the child's position among the parent's children in code order.
+// Mass, COM and the packed FP32 record of cell id from two prefix sums
+// (SPLIT monopoles; defined with the prefix kernels below, which run before
+// the tree build).
+__device__ void cell_from_prefix(const double4* __restrict__ prefix, const Tree& t,
+                                 const DeviceScalars* __restrict__ s, const Batch& bt,
+                                 const double2* __restrict__ pos, int id, int2 r, int level,
+                                 float accept_scale);
+
 // Five blocks per SM (48 registers): more dependent load chains in flight
 // than the 56-register build's four (tree phase 0.196 -> 0.192 ms at 4M).
-__global__ void __launch_bounds__(kThreads, 5) tree_link(const uint64_t* __restrict__ key, const uint8_t* __restrict__ lcp8,
-                          int n, const double2* __restrict__ pos, const double* __restrict__ mass,
-                          Tree t, DeviceScalars* __restrict__ s) {
+// kMono (SPLIT monopoles): the prefix sums are ready, and each cell also
+// writes its monopole record, which saves a pass over the cells.
+template <bool kMono>
+__global__ void __launch_bounds__(kThreads, 5)
+tree_link(const uint64_t* __restrict__ key, const uint8_t* __restrict__ lcp8, int n,
+          const double2* __restrict__ pos, const double* __restrict__ mass, Tree t,
+          DeviceScalars* __restrict__ s, const double4* __restrict__ prefix, Batch bt,
+          float accept_scale) {
     const int id = blockIdx.x * blockDim.x + threadIdx.x;
     const int cells = s->cells;
     if (id >= cells) return;
@@ -504,6 +517,7 @@ __global__ void __launch_bounds__(kThreads, 5) tree_link(const uint64_t* __restr
     t.level[id] = c;
     t.nint[id] = nint;
     t.ready[id] = 0;
+    if (kMono) cell_from_prefix(prefix, t, s, bt, pos, id, make_int2(first, last), c, accept_scale);
     // cells whose children are all leaves start the bottom-up climb: listed
     // with one atomic per warp
     const unsigned active = __activemask();
@@ -887,13 +901,10 @@ prefix_apply(const double2* __restrict__ pos, const double* __restrict__ mass, i
     if (blockIdx.x == ntiles - 1 && threadIdx.x == 0) prefix[n] = tiles[ntiles];
 }
 
-// Phase 4: every cell from two prefix entries.
-__global__ void __launch_bounds__(kThreads)
-cells_from_prefix(const double4* __restrict__ prefix, Tree t, const DeviceScalars* __restrict__ s,
-                  Batch bt, const double2* __restrict__ pos, float accept_scale) {
-    const int id = blockIdx.x * blockDim.x + threadIdx.x;
-    if (id >= s->cells) return;
-    const int2 r = t.range[id];
+__device__ void cell_from_prefix(const double4* __restrict__ prefix, const Tree& t,
+                                 const DeviceScalars* __restrict__ s, const Batch& bt,
+                                 const double2* __restrict__ pos, int id, int2 r, int level,
+                                 float accept_scale) {
     const double4 a = prefix[r.x], b = prefix[r.y + 1];
     const double M = b.x - a.x;
     const double rx = (b.y - a.y) / M, ry = (b.z - a.z) / M;
@@ -902,8 +913,9 @@ cells_from_prefix(const double4* __restrict__ prefix, Tree t, const DeviceScalar
     t.mass[id] = M;
     t.com[id] = com;
     t.cell4[id] = make_float4((float)rx, (float)ry, (float)M,
-                              accept_size2(s, bt, pos, r.x, t.level[id], com, accept_scale));
+                              accept_size2(s, bt, pos, r.x, level, com, accept_scale));
 }
+
 
 // ---- learned features: second and third moments -------------------------
 // The features need S and T about each cell's centre of mass, which the
@@ -1189,8 +1201,33 @@ void launch_groups(nb_ctx* c) {
                                                                            c->scal, c->batch, key);
 }
 
+// SPLIT without quadrupoles takes its monopoles from prefix sums over the
+// sorted bodies, which the linking pass turns into cell records.
+static bool mono_prefix(const nb_ctx* c) {
+    return c->p.mode == NB_MODE_SPLIT && !(c->p.flags & NB_FLAG_QUADRUPOLE);
+}
+
+// The acceptance-size factor of the b_max test (0 = plain width test).
+static float split_accept_scale(const nb_ctx* c) {
+    const double ratio = c->p.bmax_ratio;
+    return c->p.mode == NB_MODE_SPLIT && ratio > 0.0
+               ? (float)(c->p.theta * c->p.theta / (ratio * ratio))
+               : 0.f;
+}
+
 void launch_tree(nb_ctx* c, const BodyBuffers& b) {
     const int n = (int)c->n;
+    const bool mono = mono_prefix(c);
+    if (mono) {  // the prefix sums need only the sorted bodies
+        const int ptiles = (int)blocks_for(n, kScanTile);
+        c->launches += 3;
+        prefix_reduce<<<ptiles, kThreads, 0, c->stream>>>(b.pos, b.mass, n, c->scal, c->batch,
+                                                          c->tree.prefix_tiles);
+        prefix_tiles_scan<<<1, kThreads, 0, c->stream>>>(c->tree.prefix_tiles, ptiles);
+        prefix_apply<<<ptiles, kThreads, 0, c->stream>>>(b.pos, b.mass, n, c->scal, c->batch,
+                                                         c->tree.prefix_tiles, ptiles,
+                                                         c->tree.prefix);
+    }
     const uint64_t* key = c->sort.key[0];
     Tree& t = c->tree;
     const int tiles = (int)blocks_for(n, kAnsvTile);
@@ -1207,8 +1244,12 @@ void launch_tree(nb_ctx* c, const BodyBuffers& b) {
     scan_apply<<<sblocks, kThreads, 0, c->stream>>>(t.flag, n, c->scan.block_sums, t.cell_of,
                                                      t.rep_of);
     cudaMemsetAsync(&c->scal->nstart, 0, sizeof(int32_t), c->stream);
-    tree_link<<<blocks_for(n, kThreads), kThreads, 0, c->stream>>>(key, t.lcp8, n, b.pos, b.mass, t,
-                                                                    c->scal);
+    if (mono)
+        tree_link<true><<<blocks_for(n, kThreads), kThreads, 0, c->stream>>>(
+            key, t.lcp8, n, b.pos, b.mass, t, c->scal, t.prefix, c->batch, split_accept_scale(c));
+    else
+        tree_link<false><<<blocks_for(n, kThreads), kThreads, 0, c->stream>>>(
+            key, t.lcp8, n, b.pos, b.mass, t, c->scal, nullptr, c->batch, 0.f);
     tree_trivial_root<<<1, 1, 0, c->stream>>>(b.pos, b.mass, n, t, c->scal);
 }
 
@@ -1232,17 +1273,8 @@ void launch_moments(nb_ctx* c, const BodyBuffers& b, bool split) {
         tree_moments<true, true><<<blocks, kThreads, 0, c->stream>>>(c->scal, b.pos, b.mass, c->tree,
                                                                      c->batch, accept_scale);
     } else if (split) {
-        // monopoles from the prefix sums
-        const int n = (int)c->n;
-        const int tiles = (int)blocks_for(n, kScanTile);
-        c->launches += 4;
-        prefix_reduce<<<tiles, kThreads, 0, c->stream>>>(b.pos, b.mass, n, c->scal, c->batch,
-                                                         c->tree.prefix_tiles);
-        prefix_tiles_scan<<<1, kThreads, 0, c->stream>>>(c->tree.prefix_tiles, tiles);
-        prefix_apply<<<tiles, kThreads, 0, c->stream>>>(b.pos, b.mass, n, c->scal, c->batch,
-                                                        c->tree.prefix_tiles, tiles, c->tree.prefix);
-        cells_from_prefix<<<blocks, kThreads, 0, c->stream>>>(c->tree.prefix, c->tree, c->scal,
-                                                              c->batch, b.pos, accept_scale);
+        // monopoles: the prefix sums ran before the tree, and the linking
+        // pass wrote every cell's record from them
     } else {
         c->launches += 1;
         tree_moments<false, false><<<blocks, kThreads, 0, c->stream>>>(c->scal, b.pos, b.mass,
