@@ -50,6 +50,17 @@ PHASE_BYTES_PER_BODY = {"bbox+morton": 16 + 28, "sort": 8 + 8 * 24, "gather": 88
                         "moments": 65, "drift": 48}
 
 
+def phase_bytes(passes: int, mono_prefix: bool) -> dict:
+    """Algorithmic bytes per body of each HBM phase.  SPLIT monopoles take the
+    prefix sums before the tree and the cell records in the linking pass, so
+    their moments bytes belong to the tree phase and the moments phase is
+    empty."""
+    out = dict(PHASE_BYTES_PER_BODY, sort=sort_bytes(passes))
+    if mono_prefix:
+        out["tree"] += out.pop("moments")
+    return out
+
+
 def sort_bytes(passes: int) -> int:
     """Bytes per body of a sort over the top `passes` key bytes: histogram read,
     the passes, and the tie pass's read of the sorted keys when passes < 8."""
@@ -591,7 +602,8 @@ def run_ours(args) -> None:
     achieved = FLOPS_PER_INTERACTION * interactions / (force_ms * 1e-3) / 1e12
     hbm = peaks.get("hbm_gbs", FALLBACK_PEAKS["hbm_gbs"])
     rooflines = {}
-    for name, bpb in dict(PHASE_BYTES_PER_BODY, sort=sort_bytes(passes or 8)).items():
+    mono = args.mode == "split" and not args.quad
+    for name, bpb in phase_bytes(passes or 8, mono).items():
         if name == "drift" and args.mode != "fp64":
             continue
         if args.mode == "allpairs" and name != "force":
@@ -670,11 +682,12 @@ def run_ours(args) -> None:
         print(json.dumps(line), flush=True)
 
 
-def _hbm_rooflines(phases: dict, n: int, fp64: bool, passes: int = 8) -> dict:
+def _hbm_rooflines(phases: dict, n: int, fp64: bool, passes: int = 8,
+                   mono_prefix: bool = False) -> dict:
     peaks, kind = _peaks()
     hbm = peaks.get("hbm_gbs", FALLBACK_PEAKS["hbm_gbs"])
     out = {}
-    for name, bpb in dict(PHASE_BYTES_PER_BODY, sort=sort_bytes(passes)).items():
+    for name, bpb in phase_bytes(passes, mono_prefix).items():
         if name == "drift" and not fp64:
             continue
         if phases.get(name, 0) > 0:
@@ -720,7 +733,8 @@ def _timed_context(nb, cfg, m, p, v, warmup: int, steps: int, counts=None, error
                                                     cfg.epsilon_squared, k=error_sample,
                                                     device=cfg.device)
             rec["p50"], rec["p99"] = err["p50"], err["p99"]
-    rec["rooflines_hbm"] = _hbm_rooflines(phases, m.shape[0], cfg.mode == nb.NB_MODE_FP64, passes)
+    rec["rooflines_hbm"] = _hbm_rooflines(phases, m.shape[0], cfg.mode == nb.NB_MODE_FP64, passes,
+                                          cfg.mode == nb.NB_MODE_SPLIT and not cfg.quadrupole)
     return rec
 
 
