@@ -466,19 +466,29 @@ __device__ void cell_from_prefix(const double4* __restrict__ prefix, const Tree&
                                  const double2* __restrict__ pos, int id, int2 r, int level,
                                  float accept_scale);
 
+// The SPLIT target groups of one cell (defined with tree_groups_write below).
+template <bool kWrite>
+__device__ int cell_groups(int2 rg, bool is_root, int nc, const int* ca, const int* cb,
+                           const bool* leaf, int gsize, int fill, const Batch& bt,
+                           const uint64_t* __restrict__ key, int2* __restrict__ out);
+
 // Five blocks per SM (48 registers): more dependent load chains in flight
 // than the 56-register build's four (tree phase 0.196 -> 0.192 ms at 4M).
 // kMono (SPLIT monopoles): the prefix sums are ready, and each cell also
-// writes its monopole record, which saves a pass over the cells.
+// writes its monopole record, which saves a pass over the cells.  gsize > 0
+// (SPLIT): each cell also counts its target groups into gcount.
 template <bool kMono>
 __global__ void __launch_bounds__(kThreads, 5)
 tree_link(const uint64_t* __restrict__ key, const uint8_t* __restrict__ lcp8, int n,
           const double2* __restrict__ pos, const double* __restrict__ mass, Tree t,
           DeviceScalars* __restrict__ s, const double4* __restrict__ prefix, Batch bt,
-          float accept_scale) {
+          float accept_scale, int gsize, int fill) {
     const int id = blockIdx.x * blockDim.x + threadIdx.x;
     const int cells = s->cells;
-    if (id >= cells) return;
+    if (id >= cells) {
+        if (gsize > 0 && id < n) t.gcount[id] = 0;  // the group scan runs over n entries
+        return;
+    }
     const int i = t.rep_of[id];
     const int4 bi = t.bnd[i];
     const int c = lcp8[i];
@@ -495,9 +505,14 @@ tree_link(const uint64_t* __restrict__ key, const uint8_t* __restrict__ lcp8, in
     }
     int* child = reinterpret_cast<int*>(t.child + id);
     int nint = 0;
+    int ca[4], cb[4];
+    bool leaf[4];
     for (int q = 0; q <= ns; ++q) {
         const int a = q == 0 ? first : sep[q - 1] + 1;
         const int b = q == ns ? last : sep[q];
+        ca[q] = a;
+        cb[q] = b;
+        leaf[q] = true;
         if (a == b) {
             child[q] = ~a;
             t.leaf_last[a] = a;
@@ -509,9 +524,13 @@ tree_link(const uint64_t* __restrict__ key, const uint8_t* __restrict__ lcp8, in
             t.leaf_plevel[a] = c;
             bucket_moments(pos, mass, a, b, t.bucket_mass + a, t.bucket_com + a);
         } else {
+            leaf[q] = false;
             ++nint;  // a cell: it enters itself below
         }
     }
+    if (gsize > 0)
+        t.gcount[id] = cell_groups<false>(make_int2(first, last), first == 0 && last == n - 1,
+                                          ns + 1, ca, cb, leaf, gsize, fill, bt, key, nullptr);
     for (int q = ns + 1; q < 4; ++q) child[q] = INT_MIN;
     t.range[id] = make_int2(first, last);
     t.level[id] = c;
@@ -556,8 +575,9 @@ tree_link(const uint64_t* __restrict__ key, const uint8_t* __restrict__ lcp8, in
 
 // A tree without internal cells: one body, or all bodies in one level-30 leaf.
 __global__ void tree_trivial_root(const double2* __restrict__ pos, const double* __restrict__ mass,
-                                  int n, Tree t, DeviceScalars* __restrict__ s) {
+                                  int n, Tree t, DeviceScalars* __restrict__ s, int gsize) {
     if (s->cells != 0) return;
+    if (gsize > 0) t.gcount[0] = (n + gsize - 1) / gsize;  // groups of the root leaf
     s->root = ~0;
     t.leaf_last[0] = n - 1;
     t.leaf_plevel[0] = -1;
@@ -1053,101 +1073,107 @@ learned_features(DeviceScalars* __restrict__ s, const double2* __restrict__ pos,
 // would open it down to its bodies: in a sparse disc tail, a group of outer
 // bodies then walked the whole core on one warp (2.3 ms of a 65,536-body
 // step).  So with a large child present, runs also end at the half boundary.
+// The groups of one cell with body range rg and nc children in code order
+// ([ca, cb], leaf marks the leaf children); returns their number and, with
+// kWrite, writes them from out on.
 template <bool kWrite>
-__global__ void tree_groups(int n, int gsize, int fill, Tree t, const DeviceScalars* __restrict__ s,
-                            Batch bt, const uint64_t* __restrict__ key) {
-    const int id = blockIdx.x * blockDim.x + threadIdx.x;
-    const int cells = s->cells;
-    if (id >= n) return;
-    if (id >= cells) {
-        if (!kWrite) t.gcount[id] = 0;
-        if (cells == 0 && id == 0) {  // no cell: the root leaf holds all bodies
-            const int ng = (n + gsize - 1) / gsize;
-            if (!kWrite) {
-                t.gcount[0] = ng;
-            } else {
-                for (int k = 0; k < ng; ++k)
-                    t.groups[k] = make_int2(k * gsize, min(n, (k + 1) * gsize) - 1);
-            }
-        }
-        return;
-    }
-    const int2 rg = t.range[id];
-    int out = kWrite ? t.gbase[id] : 0;
+__device__ int cell_groups(int2 rg, bool is_root, int nc, const int* ca, const int* cb,
+                           const bool* leaf, int gsize, int fill, const Batch& bt,
+                           const uint64_t* __restrict__ key, int2* __restrict__ out) {
     int emitted = 0;
     auto emit = [&](int a, int b) {
-        if (kWrite) t.groups[out + emitted] = make_int2(a, b);
+        if (kWrite) out[emitted] = make_int2(a, b);
         ++emitted;
     };
     // batched universes: a forest cell above the universe roots may hold few
     // bodies but never becomes a group; it hands its children on instead
     const bool spans = bt.nuni && bt.uid[rg.x] != bt.uid[rg.y];
     if (rg.y - rg.x + 1 <= gsize && !spans) {
-        if (id == s->root) emit(rg.x, rg.y);  // the whole (small) tree is one group
-    } else {
-        const int4 ch = t.child[id];
-        const int refs[4] = {ch.x, ch.y, ch.z, ch.w};
-        int ca[4], cb[4];
-        bool large = false;  // some child emits its own groups
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int r = refs[q];
-            ca[q] = cb[q] = -1;
-            if (r == INT_MIN) continue;
-            if (r >= 0) {
-                const int2 cr = t.range[r];
-                ca[q] = cr.x;
-                cb[q] = cr.y;
-            } else {
-                ca[q] = ~r;
-                cb[q] = t.leaf_last[ca[q]];
-            }
-            large |= cb[q] - ca[q] + 1 > gsize || (bt.nuni && bt.uid[ca[q]] != bt.uid[cb[q]]);
+        if (is_root) emit(rg.x, rg.y);  // the whole (small) tree is one group
+        return emitted;
+    }
+    bool large = false;  // some child emits its own groups
+    for (int q = 0; q < nc; ++q)
+        large |= cb[q] - ca[q] + 1 > gsize || (bt.nuni && bt.uid[ca[q]] != bt.uid[cb[q]]);
+    // the children differ in digit `level` of their codes; its high bit is
+    // the half (read only when a large child makes it matter)
+    const int level = large ? min(lcp_digits(key[rg.x], key[rg.y]), 31) : 0;
+    int run_a = -1, run_b = -1, run_half = 0;
+    for (int q = 0; q < nc; ++q) {
+        const int a = ca[q], b = cb[q];
+        const int cnt = b - a + 1;
+        if (cnt > gsize || (bt.nuni && bt.uid[a] != bt.uid[b])) {  // the child emits
+            if (run_a >= 0) emit(run_a, run_b);
+            run_a = -1;
+            if (leaf[q])  // oversized multi-body leaf: chunks of one group each
+                for (int k = a; k <= b; k += gsize) emit(k, min(b, k + gsize - 1));
+            continue;
         }
-        // the children differ in digit `level` of their codes; its high bit is
-        // the half (read only when a large child makes it matter)
-        const int level = large ? min(lcp_digits(key[rg.x], key[rg.y]), 31) : 0;
-        int run_a = -1, run_b = -1, run_half = 0;
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int r = refs[q];
-            if (r == INT_MIN) break;
-            const int a = ca[q], b = cb[q];
-            const int cnt = b - a + 1;
-            if (cnt > gsize || (bt.nuni && bt.uid[a] != bt.uid[b])) {  // the child emits
-                if (run_a >= 0) emit(run_a, run_b);
-                run_a = -1;
-                if (r < 0)  // oversized multi-body leaf: chunks of one group each
-                    for (int k = a; k <= b; k += gsize) emit(k, min(b, k + gsize - 1));
+        const int half = large ? (int)(key[a] >> (63 - 2 * level)) & 1 : 0;
+        // a group never spans two universes (a forest cell's children may),
+        // nor both halves of a cell that has a large child
+        if (run_a >= 0 && ((bt.nuni && bt.uid[a] != bt.uid[run_a]) ||
+                           (large && half != run_half))) {
+            emit(run_a, run_b);
+            run_a = -1;
+        } else if (run_a >= 0 && b - run_a + 1 > gsize) {
+            if (fill) {
+                // fill the group; the rest of this child starts the next one
+                emit(run_a, run_a + gsize - 1);
+                run_a += gsize;
+                run_b = b;
                 continue;
             }
-            const int half = large ? (int)(key[a] >> (63 - 2 * level)) & 1 : 0;
-            // a group never spans two universes (a forest cell's children may),
-            // nor both halves of a cell that has a large child
-            if (run_a >= 0 && ((bt.nuni && bt.uid[a] != bt.uid[run_a]) ||
-                               (large && half != run_half))) {
-                emit(run_a, run_b);
-                run_a = -1;
-            } else if (run_a >= 0 && b - run_a + 1 > gsize) {
-                if (fill) {
-                    // fill the group; the rest of this child starts the next one
-                    emit(run_a, run_a + gsize - 1);
-                    run_a += gsize;
-                    run_b = b;
-                    continue;
-                }
-                emit(run_a, run_b);
-                run_a = -1;
-            }
-            if (run_a < 0) {
-                run_a = a;
-                run_half = half;
-            }
-            run_b = b;
+            emit(run_a, run_b);
+            run_a = -1;
         }
-        if (run_a >= 0) emit(run_a, run_b);
+        if (run_a < 0) {
+            run_a = a;
+            run_half = half;
+        }
+        run_b = b;
     }
-    if (!kWrite) t.gcount[id] = emitted;
+    if (run_a >= 0) emit(run_a, run_b);
+    return emitted;
+}
+
+// Writes every cell's groups at gbase[cell] (the linking pass counted them).
+__global__ void tree_groups_write(int n, int gsize, int fill, Tree t,
+                                  const DeviceScalars* __restrict__ s, Batch bt,
+                                  const uint64_t* __restrict__ key) {
+    const int id = blockIdx.x * blockDim.x + threadIdx.x;
+    const int cells = s->cells;
+    if (id >= n) return;
+    if (id >= cells) {
+        if (cells == 0 && id == 0) {  // no cell: the root leaf holds all bodies
+            const int ng = (n + gsize - 1) / gsize;
+            for (int k = 0; k < ng; ++k)
+                t.groups[k] = make_int2(k * gsize, min(n, (k + 1) * gsize) - 1);
+        }
+        return;
+    }
+    const int2 rg = t.range[id];
+    const int4 ch = t.child[id];
+    const int refs[4] = {ch.x, ch.y, ch.z, ch.w};
+    int ca[4], cb[4], nc = 0;
+    bool leaf[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int r = refs[q];
+        if (r == INT_MIN) break;
+        leaf[q] = r < 0;
+        if (r >= 0) {
+            const int2 cr = t.range[r];
+            ca[q] = cr.x;
+            cb[q] = cr.y;
+        } else {
+            ca[q] = ~r;
+            cb[q] = t.leaf_last[ca[q]];
+        }
+        nc = q + 1;
+    }
+    cell_groups<true>(rg, id == s->root, nc, ca, cb, leaf, gsize, fill, bt, key,
+                      t.groups + t.gbase[id]);
 }
 
 // Root reference of each universe: the cell whose body range is exactly the
@@ -1184,21 +1210,19 @@ void launch_batch_roots(nb_ctx* c) {
 void launch_groups(nb_ctx* c) {
     const int n = (int)c->n;
     const int sblocks = (int)blocks_for(n, kScanTile);
-    c->launches += 5;
+    c->launches += 4;
     const int gsize = split_group_size(c);
     // plain SPLIT fills groups to gsize bodies across sibling cells (fuller
     // warps, measured 2.6% off the walk at 4M with slightly lower errors); the
-    // learned correction keeps groups of whole cells, whose residuals it fits
+    // learned correction keeps groups of whole cells, whose residuals it fits.
+    // The linking pass counted every cell's groups; scan, then write them.
     const int fill = (c->p.flags & NB_FLAG_LEARNED) ? 0 : 1;
-    const uint64_t* key = c->sort.key[0];
-    tree_groups<false><<<blocks_for(n, kThreads), kThreads, 0, c->stream>>>(n, gsize, fill, c->tree,
-                                                                            c->scal, c->batch, key);
     scan_reduce<<<sblocks, kThreads, 0, c->stream>>>(c->tree.gcount, n, c->scan.block_sums);
     scan_block_sums<<<1, kThreads, 0, c->stream>>>(c->scan.block_sums, sblocks, &c->scal->groups);
     scan_apply<<<sblocks, kThreads, 0, c->stream>>>(c->tree.gcount, n, c->scan.block_sums,
                                                      c->tree.gbase, nullptr);
-    tree_groups<true><<<blocks_for(n, kThreads), kThreads, 0, c->stream>>>(n, gsize, fill, c->tree,
-                                                                           c->scal, c->batch, key);
+    tree_groups_write<<<blocks_for(n, kThreads), kThreads, 0, c->stream>>>(
+        n, gsize, fill, c->tree, c->scal, c->batch, c->sort.key[0]);
 }
 
 // SPLIT without quadrupoles takes its monopoles from prefix sums over the
@@ -1244,13 +1268,17 @@ void launch_tree(nb_ctx* c, const BodyBuffers& b) {
     scan_apply<<<sblocks, kThreads, 0, c->stream>>>(t.flag, n, c->scan.block_sums, t.cell_of,
                                                      t.rep_of);
     cudaMemsetAsync(&c->scal->nstart, 0, sizeof(int32_t), c->stream);
+    // SPLIT: the cells count their target groups as they link
+    const int gsize = c->p.mode == NB_MODE_SPLIT ? split_group_size(c) : 0;
+    const int fill = (c->p.flags & NB_FLAG_LEARNED) ? 0 : 1;
     if (mono)
         tree_link<true><<<blocks_for(n, kThreads), kThreads, 0, c->stream>>>(
-            key, t.lcp8, n, b.pos, b.mass, t, c->scal, t.prefix, c->batch, split_accept_scale(c));
+            key, t.lcp8, n, b.pos, b.mass, t, c->scal, t.prefix, c->batch, split_accept_scale(c),
+            gsize, fill);
     else
         tree_link<false><<<blocks_for(n, kThreads), kThreads, 0, c->stream>>>(
-            key, t.lcp8, n, b.pos, b.mass, t, c->scal, nullptr, c->batch, 0.f);
-    tree_trivial_root<<<1, 1, 0, c->stream>>>(b.pos, b.mass, n, t, c->scal);
+            key, t.lcp8, n, b.pos, b.mass, t, c->scal, nullptr, c->batch, 0.f, gsize, fill);
+    tree_trivial_root<<<1, 1, 0, c->stream>>>(b.pos, b.mass, n, t, c->scal, gsize);
 }
 
 void launch_features(nb_ctx* c, const BodyBuffers& b) {
