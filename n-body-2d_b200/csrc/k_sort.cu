@@ -739,11 +739,18 @@ tie_mark(const uint64_t* __restrict__ key, int64_t n, DeviceScalars* __restrict_
     if (passes >= 8) return;
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     const int sh = 64 - 8 * passes;
+    const int lane = threadIdx.x & 31;
+    // each key is read once; the neighbours come from the next and previous
+    // lanes (the row's end lanes read theirs)
+    const uint64_t ki = i < n ? key[i] : 0ull;
+    uint64_t kn = __shfl_down_sync(kFull, ki, 1), kp = __shfl_up_sync(kFull, ki, 1);
+    if (lane == 31 && i + 1 < n) kn = key[i + 1];
+    if (lane == 0 && i > 0 && i < n) kp = key[i - 1];
     bool start = false;
     int64_t e = i;
     if (i + 1 < n) {
-        const uint64_t top = key[i] >> sh;
-        start = (key[i + 1] >> sh) == top && (i == 0 || (key[i - 1] >> sh) != top);
+        const uint64_t top = ki >> sh;
+        start = (kn >> sh) == top && (i == 0 || (kp >> sh) != top);
         if (start) {  // last key of the group: galloping search
             int64_t step = 1, good = i + 1;
             while (good + step < n && (key[good + step] >> sh) == top) {
@@ -761,7 +768,6 @@ tie_mark(const uint64_t* __restrict__ key, int64_t n, DeviceScalars* __restrict_
     const unsigned size = (unsigned)(e - i + 1);
     const bool is_small = start && size <= 32, is_big = start && size > 32;
     const unsigned ms = __ballot_sync(kFull, is_small), mb = __ballot_sync(kFull, is_big);
-    const int lane = threadIdx.x & 31;
     unsigned b0 = 0, b1 = 0;
     if (lane == 0) {
         if (ms) b0 = atomicAdd(&s->tie_count[0], __popc(ms));

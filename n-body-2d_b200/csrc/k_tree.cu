@@ -334,16 +334,18 @@ __device__ __forceinline__ int warp_inclusive(int v) {
     return v;
 }
 
+template <int kBlock = kThreads>
 __device__ int block_exclusive(int v, int* wsum, int* total) {
+    static_assert(kBlock % 32 == 0 && kBlock <= 1024, "one warp scans the warp sums");
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int inc = warp_inclusive(v);
     if (lane == 31) wsum[warp] = inc;
     __syncthreads();
     if (warp == 0) {
-        const int w = lane < kThreads / 32 ? wsum[lane] : 0;
+        const int w = lane < kBlock / 32 ? wsum[lane] : 0;
         const int winc = warp_inclusive(w);
-        if (lane < kThreads / 32) wsum[lane] = winc - w;
-        if (lane == kThreads / 32 - 1 && total) *total = winc;
+        if (lane < kBlock / 32) wsum[lane] = winc - w;
+        if (lane == kBlock / 32 - 1 && total) *total = winc;
     }
     __syncthreads();
     const int r = wsum[warp] + inc - v;
@@ -370,15 +372,18 @@ scan_reduce(const int32_t* __restrict__ in, int n, int32_t* __restrict__ block_s
     if (threadIdx.x == 0) block_sums[blockIdx.x] = total;
 }
 
-__global__ void __launch_bounds__(kThreads)
+// One block of kSumsThreads: the block sums of 4M entries (2,048) take two
+// rounds instead of eight.
+constexpr int kSumsThreads = 1024;
+__global__ void __launch_bounds__(kSumsThreads)
 scan_block_sums(int32_t* __restrict__ block_sums, int blocks, int32_t* __restrict__ total_out) {
-    __shared__ int wsum[kThreads / 32];
+    __shared__ int wsum[kSumsThreads / 32];
     __shared__ int total;
     int carry = 0;
-    for (int b = 0; b < blocks; b += kThreads) {
+    for (int b = 0; b < blocks; b += kSumsThreads) {
         const int t = b + threadIdx.x;
         const int v = t < blocks ? block_sums[t] : 0;
-        const int ex = block_exclusive(v, wsum, &total);
+        const int ex = block_exclusive<kSumsThreads>(v, wsum, &total);
         if (t < blocks) block_sums[t] = carry + ex;
         carry += total;
         __syncthreads();
@@ -1218,7 +1223,7 @@ void launch_groups(nb_ctx* c) {
     // The linking pass counted every cell's groups; scan, then write them.
     const int fill = (c->p.flags & NB_FLAG_LEARNED) ? 0 : 1;
     scan_reduce<<<sblocks, kThreads, 0, c->stream>>>(c->tree.gcount, n, c->scan.block_sums);
-    scan_block_sums<<<1, kThreads, 0, c->stream>>>(c->scan.block_sums, sblocks, &c->scal->groups);
+    scan_block_sums<<<1, kSumsThreads, 0, c->stream>>>(c->scan.block_sums, sblocks, &c->scal->groups);
     scan_apply<<<sblocks, kThreads, 0, c->stream>>>(c->tree.gcount, n, c->scan.block_sums,
                                                      c->tree.gbase, nullptr);
     tree_groups_write<<<blocks_for(n, kThreads), kThreads, 0, c->stream>>>(
@@ -1264,7 +1269,7 @@ void launch_tree(nb_ctx* c, const BodyBuffers& b) {
                                                  t.flag, t.bnd);
     const int sblocks = (int)blocks_for(n, kScanTile);
     scan_reduce<<<sblocks, kThreads, 0, c->stream>>>(t.flag, n, c->scan.block_sums);
-    scan_block_sums<<<1, kThreads, 0, c->stream>>>(c->scan.block_sums, sblocks, &c->scal->cells);
+    scan_block_sums<<<1, kSumsThreads, 0, c->stream>>>(c->scan.block_sums, sblocks, &c->scal->cells);
     scan_apply<<<sblocks, kThreads, 0, c->stream>>>(t.flag, n, c->scan.block_sums, t.cell_of,
                                                      t.rep_of);
     cudaMemsetAsync(&c->scal->nstart, 0, sizeof(int32_t), c->stream);
