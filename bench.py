@@ -338,7 +338,11 @@ def gpu_baseline(nb, device: int) -> dict:
         rec["ratio_split_vs_reference"] = split["value"] / ref["value"]
     # the reference's own step ends with a download of every body (CU:632-646):
     # both sides again with that copy in every step, on the host clock
-    ref_dl = _ref_gpu_record(_ref_gpu_timed(m, p, v, 0.5, 5, download=True), 262144)
+    ref_dl = _ref_gpu_record(_ref_gpu_timed(m, p, v, 0.5, 5, download=True), 262144,
+                             how="the reference's CUDA kernels (BarnesHutCuda.cu, unmodified) under "
+                                 "the harness driver, each step ending with the scatter to original "
+                                 "order and the copy of all positions and velocities to host memory "
+                                 "(CU:498-506, 632-646); host clock over K steps")
     dl = {"reference": ref_dl,
           "ours_fp64": _stepped_with_download(nb, mk(nb.NB_MODE_FP64), m, p, v, 3, 20),
           "ours_split": _stepped_with_download(nb, mk(nb.NB_MODE_SPLIT), m, p, v, 3, 20)}
@@ -437,12 +441,12 @@ def _ref_gpu_timed(m, p, v, theta: float, steps: int, download: bool = False) ->
         return {"unavailable": f"reference GPU harness failed: {type(e).__name__}: {e}"[:300]}
 
 
-def _ref_gpu_record(r: dict, n: int) -> dict:
+def _ref_gpu_record(r: dict, n: int, how: str = REF_GPU_HOW) -> dict:
     if "seconds_per_step" not in r:
         return r
     return {"value": n / r["seconds_per_step"], "unit": "body-steps/s",
             "ms_per_step": r["seconds_per_step"] * 1e3, "max_stack": r["max_stack"],
-            "how": REF_GPU_HOW}
+            "how": how}
 
 
 def reference_gpu_records(args, m, p, v) -> dict:
