@@ -139,6 +139,9 @@ bbox_kernel(const double2* __restrict__ pos, int64_t n, double* __restrict__ par
         s->box[3] = by1;
         s->center[0] = 0.5 * (bx0 + bx1);
         s->center[1] = 0.5 * (by0 + by1);
+        // the Morton kernel's scale factors (CU:122-123), divided once here
+        s->inv_wh[0] = 1.0 / (bx1 - bx0);
+        s->inv_wh[1] = 1.0 / (by1 - by0);
         // CU:717 root width_sq, then CU:216 child_wsq = parent * 0.25 per level.
         const double w = bx1 - bx0;
         double wsq = w * w;
@@ -175,9 +178,8 @@ __global__ void morton_kernel(const double2* __restrict__ pos, int64_t n,
     const bool odd = s->sort_passes & 1;
     uint64_t* __restrict__ key = odd ? key1 : key0;
     uint32_t* __restrict__ val = odd ? val1 : val0;
-    const double x0 = s->box[0], x1 = s->box[1], y0 = s->box[2], y1 = s->box[3];
-    const double inv_w = 1.0 / (x1 - x0);
-    const double inv_h = 1.0 / (y1 - y0);
+    const double x0 = s->box[0], y0 = s->box[2];
+    const double inv_w = s->inv_wh[0], inv_h = s->inv_wh[1];
     const double2 p = __ldg(pos + i);
     const double nx = (p.x - x0) * inv_w;
     const double ny = (p.y - y0) * inv_h;

@@ -33,6 +33,7 @@ constexpr unsigned kErrUpload = 8u;     // nb_upload_async rejected its bodies
 struct DeviceScalars {
     double box[4];            // squared root box: x_min, x_max, y_min, y_max
     double center[2];         // box centre: origin of the FP32 coordinates
+    double inv_wh[2];         // 1 / (x_max - x_min), 1 / (y_max - y_min): the Morton scaling
     double wsq[kMaxLevel + 1];// squared cell width per level (root * 0.25^L)
     int32_t root;             // >= 0 cell id, < 0 leaf ~first_body
     int32_t cells;            // internal cells of the current tree
