@@ -52,12 +52,15 @@ PHASE_BYTES_PER_BODY = {"bbox+morton": 16 + 28, "sort": 8 + 8 * 24, "gather": 88
 
 def phase_bytes(passes: int, mono_prefix: bool) -> dict:
     """Algorithmic bytes per body of each HBM phase.  SPLIT monopoles take the
-    prefix sums before the tree and the cell records in the linking pass, so
-    their moments bytes belong to the tree phase and the moments phase is
-    empty."""
+    prefix sums in their own phase before the tree (24 bytes read and 32
+    written per body) and the cell records in the linking pass (about 24
+    bytes per body: 40 per cell at 0.6 cells per body), so the moments phase
+    is empty."""
     out = dict(PHASE_BYTES_PER_BODY, sort=sort_bytes(passes))
     if mono_prefix:
-        out["tree"] += out.pop("moments")
+        out.pop("moments")
+        out["prefix"] = 56
+        out["tree"] += 24
     return out
 
 

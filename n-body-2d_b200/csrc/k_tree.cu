@@ -1244,10 +1244,10 @@ static float split_accept_scale(const nb_ctx* c) {
                : 0.f;
 }
 
-void launch_tree(nb_ctx* c, const BodyBuffers& b) {
+void launch_prefix_sums(nb_ctx* c, const BodyBuffers& b) {
+    if (!mono_prefix(c)) return;
     const int n = (int)c->n;
-    const bool mono = mono_prefix(c);
-    if (mono) {  // the prefix sums need only the sorted bodies
+    {  // the prefix sums need only the sorted bodies
         const int ptiles = (int)blocks_for(n, kScanTile);
         c->launches += 3;
         prefix_reduce<<<ptiles, kThreads, 0, c->stream>>>(b.pos, b.mass, n, c->scal, c->batch,
@@ -1257,6 +1257,12 @@ void launch_tree(nb_ctx* c, const BodyBuffers& b) {
                                                          c->tree.prefix_tiles, ptiles,
                                                          c->tree.prefix);
     }
+}
+
+void launch_tree(nb_ctx* c, const BodyBuffers& b, bool prefix_done) {
+    const int n = (int)c->n;
+    const bool mono = mono_prefix(c);
+    if (mono && !prefix_done) launch_prefix_sums(c, b);
     const uint64_t* key = c->sort.key[0];
     Tree& t = c->tree;
     const int tiles = (int)blocks_for(n, kAnsvTile);

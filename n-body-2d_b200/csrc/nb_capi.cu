@@ -232,7 +232,7 @@ void drop_graphs(nb_ctx* c) {
 
 // "drift": the FP64 drift kernel; in learned mode the correction kernel, which
 // also kicks and drifts (plain SPLIT fuses both into the force kernel).
-const char* const kPhaseNames[nb::kPhases] = {"bbox+morton", "sort", "gather", "tree",
+const char* const kPhaseNames[nb::kPhases] = {"bbox+morton", "sort", "gather", "prefix", "tree",
                                               "moments", "groups", "force", "drift"};
 
 // Enqueues one step reading the state from buf[parity]; leaves it in the
@@ -251,10 +251,10 @@ void enqueue_step(nb_ctx* c, int parity, bool integrate, bool store_acc, bool ti
     cudaMemsetAsync(&c->scal->cell_terms, 0, 3 * sizeof(unsigned long long), c->stream);
     if (c->p.mode == NB_MODE_ALLPAIRS) {
         // AllPairsSim: drift into the other buffer, then the all-pairs kick there
-        for (int k = 1; k < 7; ++k) mark(k);
+        for (int k = 1; k < 8; ++k) mark(k);
         nb::launch_allpairs_step(c, A, B, integrate, store_acc);
-        mark(7);
         mark(8);
+        mark(9);
         return;
     }
     nb::launch_bbox(c, A.pos);
@@ -265,9 +265,11 @@ void enqueue_step(nb_ctx* c, int parity, bool integrate, bool store_acc, bool ti
     const bool split = c->p.mode == NB_MODE_SPLIT;
     nb::launch_gather(c, A, B, split ? c->tree.body4 : nullptr);
     mark(3);
-    nb::launch_tree(c, B);
-    nb::launch_batch_roots(c);
+    nb::launch_prefix_sums(c, B);  // SPLIT monopoles only
     mark(4);
+    nb::launch_tree(c, B, true);
+    nb::launch_batch_roots(c);
+    mark(5);
     // the target groups need only the tree: they are built on the side stream
     // while the moments run (two branches of the captured graph)
     if (split) {
@@ -280,9 +282,9 @@ void enqueue_step(nb_ctx* c, int parity, bool integrate, bool store_acc, bool ti
         cudaEventRecord(c->join_ev, c->side_stream);
     }
     nb::launch_moments(c, B, split);
-    mark(5);
-    if (split) cudaStreamWaitEvent(c->stream, c->join_ev, 0);
     mark(6);
+    if (split) cudaStreamWaitEvent(c->stream, c->join_ev, 0);
+    mark(7);
     if (split && (c->p.flags & NB_FLAG_LEARNED)) {
         // the features need only the monopoles, and only the correction reads
         // them: they are built on the side stream while the walk runs
@@ -294,18 +296,18 @@ void enqueue_step(nb_ctx* c, int parity, bool integrate, bool store_acc, bool ti
         c->stream = main_stream;
         cudaEventRecord(c->feat_join_ev, c->side_stream);
         nb::launch_force_split(c, B, integrate, store_acc);  // FP32 accelerations + band lists
-        mark(7);
+        mark(8);
         cudaStreamWaitEvent(c->stream, c->feat_join_ev, 0);
         nb::launch_mlp_correct(c, B, integrate, store_acc);  // learned term, kick, drift
     } else if (split) {
         nb::launch_force_split(c, B, integrate, store_acc);  // kick and drift fused
-        mark(7);
+        mark(8);
     } else {
         nb::launch_force_fp64(c, B, integrate, store_acc);
-        mark(7);
+        mark(8);
         if (integrate) nb::launch_drift(c, B);
     }
-    mark(8);
+    mark(9);
 }
 
 int capture_graph(nb_ctx* c, int parity) {

@@ -19,7 +19,7 @@ constexpr int kSortThreads = 256;
 constexpr int kSortTile = kSortTileItems * kSortThreads;  // 3072 keys
 constexpr int kAnsvTile = 2048;   // boundaries per tile of the tree build's level scans
 constexpr int kAnsvLevels = 32;   // table width per tile: levels 0..30 and one spare
-constexpr int kPhases = 8;        // morton, sort, gather, tree, moments, groups, force, drift
+constexpr int kPhases = 9;        // morton, sort, gather, prefix, tree, moments, groups, force, drift
 constexpr float kThetaBand = 0.5f; // learned mode: the default plain walk the MLP stands in for
 constexpr int kBandPerBody = 16;   // learned mode: band-list capacity per body of a group
 
@@ -266,7 +266,10 @@ void launch_batch_roots(nb_ctx* c);   // per-universe root cells after the tree 
 void launch_sort(nb_ctx* c);
 unsigned sort_timeout_probe(cudaStream_t st);                                   // result in key[0]/val[0]
 void launch_gather(nb_ctx* c, const BodyBuffers& src, const BodyBuffers& dst, float4* body4);
-void launch_tree(nb_ctx* c, const BodyBuffers& b);
+// SPLIT monopoles: the prefix sums over the sorted bodies (nothing in other
+// modes); launch_tree runs them itself unless prefix_done.
+void launch_prefix_sums(nb_ctx* c, const BodyBuffers& b);
+void launch_tree(nb_ctx* c, const BodyBuffers& b, bool prefix_done = false);
 void launch_moments(nb_ctx* c, const BodyBuffers& b, bool split);
 // learned mode: second and third moments and the BF16 feature records
 void launch_features(nb_ctx* c, const BodyBuffers& b);
