@@ -129,6 +129,60 @@ def test_tree_invariants(nbp):
     assert (t["level"] >= 0).all() and (t["level"] < 30).all()
 
 
+def _cells_from_codes(codes):
+    """The compressed quadtree's cells from sorted codes, built on the host
+    with a plain stack: boundary i (bodies i, i + 1) has level c_i = shared
+    leading 2-bit digits (capped at 30); the cell a boundary below 30
+    separates spans the bodies between the nearest smaller levels on either
+    side, and its first separator creates it.  Returns {(first, last, level)}."""
+    codes = codes.astype(np.uint64)
+    x = codes[:-1] ^ codes[1:]
+    bitlen = np.zeros(x.shape, dtype=np.int64)
+    for k in range(64):
+        bitlen += ((x >> np.uint64(k)) > 0).astype(np.int64)
+    c = np.minimum((64 - bitlen) // 2, 30)
+    n, m = len(codes), len(c)
+    left_lt, left_le, right_lt = np.full(m, -1), np.full(m, -1), np.full(m, n - 1)
+    stack = []
+    for i in range(m):  # nearest smaller (and smaller-or-equal) on the left
+        while stack and c[stack[-1]] > c[i]:
+            stack.pop()
+        left_le[i] = stack[-1] if stack else -1
+        j = len(stack) - 1
+        while j >= 0 and c[stack[j]] >= c[i]:
+            j -= 1
+        left_lt[i] = stack[j] if j >= 0 else -1
+        stack.append(i)
+    stack = []
+    for i in range(m - 1, -1, -1):  # nearest smaller on the right
+        while stack and c[stack[-1]] >= c[i]:
+            stack.pop()
+        right_lt[i] = stack[-1] if stack else n - 1
+        stack.append(i)
+    return {(int(left_lt[i] + 1), int(right_lt[i]), int(c[i])) for i in range(m)
+            if c[i] < 30 and left_le[i] == left_lt[i]}
+
+
+@pytest.mark.parametrize("n", [2047, 2048, 2049, 6145, 40000])
+def test_tree_cells_across_tiles(nbp, n):
+    """The device build works on tiles of 2,048 boundaries with per-tile
+    tables for what lies beyond a tile; its cells (body range and level)
+    must equal a plain host construction, including at tile edges and with
+    level-30 leaves (coincident bodies)."""
+    m, p, v = nbp.universes.colliding_discs(n + (n & 1), 2)
+    m, p, v = m[:n], p[:n].copy(), v[:n]
+    p[100:140] = p[100]          # a multi-body leaf
+    p[n // 2:n // 2 + 5] = p[n // 2]
+    with ctx_for(nbp, m, p, v) as ctx:
+        ctx.accelerations()
+        t = ctx.debug_tree()
+        codes, order, _ = ctx.debug_morton()
+    assert np.array_equal(order, np.arange(n))   # the state is already in code order
+    got = set(zip(t["first"].tolist(), t["last"].tolist(), t["level"].tolist()))
+    assert len(got) == len(t["first"])
+    assert got == _cells_from_codes(codes)
+
+
 def test_single_body_and_coincident_bodies(nbp, orc):
     with ctx_for(nbp, np.ones(1), np.zeros((1, 2)), np.ones((1, 2))) as ctx:
         assert np.array_equal(ctx.accelerations(), np.zeros((1, 2)))
